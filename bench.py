@@ -1,0 +1,342 @@
+"""Compaction throughput benchmark (one JSON line on rank 0).
+
+Workload: the L1->L2 compaction at size (1 L1 table of 2 MiB over 32 L2 tables
+of 2 MiB, Zipf(0.99) keys of 8-64 bytes, lognormal values, 3 snapshots, 5%
+deletion markers, L3 grandparents over half the key range), synthetic and
+seeded.  One step = one compaction job through the engine's C ABI.
+
+* value: MiB of input compacted per second with the input tables already in
+  HBM and the outputs left in HBM (lc_job_desc.inputs_on_device /
+  outputs_on_device); L2 is flushed between steps.
+* e2e: the same job through lc_compact with the tables in pinned host memory:
+  the host->device copy of the inputs and the device->host copy of every
+  output file are inside each step.
+* roofline: the slowest of the three bandwidth-bound kernels (decode, merge,
+  data-block encode), timed live with CUDA events on the job's own stream,
+  against the measured HBM copy bandwidth.
+* cpu_baseline: the reference's own CPU DoCompactionWork on one host core.
+
+--impl reference times the reference's CPU compaction on all usable host
+cores (one job per thread) on the same workload instead.
+
+Multi-GPU (torchrun): every rank compacts its own job stream on its own GPU
+(replicas; no collective on the data path); value sums all ranks' input bytes
+over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "compaction MB/s in->out (byte-exact); p50/p99 job latency, batched vs plain"
+UNIT = "MiB/s"
+WORKLOAD = "l1_l2_at_size"
+MiB = float(1 << 20)
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="luda", choices=["luda", "reference"])
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--cpu-seconds", type=float, default=10.0,
+                   help="bound on the CPU baseline sample")
+    return p.parse_args()
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def make_job(scale: float, seed: int):
+    from luda_b200 import workloads
+    return workloads.l1_l2_at_size(seed=seed, scale=scale)
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.has_ref():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU build (oracle/_ref) not present"}))
+        return
+    job = make_job(args.scale, 1)
+    job.materialize(lambda e, o: oracle.build_table(e, o, "ref"))
+    mib = job.input_bytes() / MiB
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(avail // (8 * job.input_bytes()))))
+    except Exception:
+        pass
+    cores = min(cores, 64)
+    for _ in range(args.warmup):
+        oracle.ref_compact_parallel(job, cores)
+    secs = []
+    for _ in range(args.steps):
+        secs.append(oracle.ref_compact_parallel(job, cores))
+    total = sum(secs)
+    value = args.steps * cores * mib / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "input_mib": mib, "jobs_per_step": cores,
+                   "scale": args.scale},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent copies of the {mib:.1f} MiB job per step "
+                                   f"(reference CPU DoCompactionWork, one DB per thread)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline(job, bound_s):
+    import oracle
+    kind = "reference" if oracle.has_ref() else "port"
+    mib = job.input_bytes() / MiB
+    secs = []
+    t_end = time.perf_counter() + bound_s
+    while time.perf_counter() < t_end and len(secs) < 50:
+        if kind == "reference":
+            _, s = oracle.ref_compact_timed(job)
+        else:
+            _, s = oracle.oracle_compact_timed(job)
+        secs.append(s)
+    med = float(np.median(secs))
+    return {"value": mib / med, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{len(secs)} runs of the full {mib:.1f} MiB job, median "
+                      f"DoCompactionWork time {med * 1e3:.1f} ms"}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    from luda_b200.engine import Engine
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    job = make_job(args.scale, 1 + 1000 * rank)
+    eng = Engine(local, phase_timing=True)
+    # input tables built by the engine's own flush encoder
+    job.materialize(lambda e, o: eng.build_table(e, o))
+    tables = job.input_tables()
+    in_bytes = job.input_bytes()
+    offs, total = [], 0
+    for f in tables:
+        offs.append(total)
+        total += (len(f.data) + 15) // 16 * 16
+    dev_in = torch.zeros(total + 16, dtype=torch.uint8, device="cuda")
+    for f, o in zip(tables, offs):
+        dev_in[o:o + len(f.data)] = torch.frombuffer(bytearray(f.data), dtype=torch.uint8).to("cuda")
+    ptrs = [dev_in.data_ptr() + o for o in offs]
+    # pinned host copies for the end-to-end leg
+    pinned = []
+    for f in tables:
+        t = torch.empty(len(f.data), dtype=torch.uint8).pin_memory()
+        t.copy_(torch.frombuffer(bytearray(f.data), dtype=torch.uint8))
+        pinned.append(t)
+    for f, t in zip(tables, pinned):
+        f.data = t.numpy()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    # consistency of the two paths (untimed): same file sizes
+    host_res = eng.compact(job)
+    dev_res = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+    assert dev_res.bytes_out == host_res.bytes_out and len(dev_res.files) == len(host_res.files)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+    barrier()
+    torch.cuda.synchronize()
+    ms_steps, phases, launches = [], [], 0
+    bytes_out = 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms_steps.append(e0.elapsed_time(e1))
+            phases.append(r.phase_ms)
+            launches += r.kernel_launches
+            bytes_out = r.bytes_out
+    barrier()
+    torch.cuda.synchronize()
+    total_ms = float(sum(ms_steps))
+
+    # end to end through host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        eng.compact(job)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = eng.compact(job)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = float(sum(e2e_ms))
+    d2h = r.bytes_out
+
+    # max over ranks
+    if dist is not None:
+        t = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+        b = torch.tensor([float(in_bytes)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(b)
+        all_in = float(b[0])
+    else:
+        all_in = float(in_bytes)
+    value = args.steps * all_in / MiB / (total_ms / 1e3)
+    e2e_value = args.steps * all_in / MiB / (e2e_total / 1e3)
+
+    # roofline: algorithmic bytes of the three bandwidth-bound kernels
+    n_in = r.entries_in
+    k_in = r.key_bytes_in
+    n_keep = r.entries_out
+    alg = {
+        "decode": in_bytes + k_in + 16 * n_in,
+        "merge": k_in + 16 * n_in + 4 * n_in,
+        "encode_blocks": r.key_bytes_out + r.value_bytes_out + bytes_out,
+    }
+    mean_ph = {k: float(np.mean([p[k] for p in phases])) for k in phases[0]}
+    dominant = max(alg, key=lambda k: mean_ph[k])
+    peak, peak_kind = measured_peak()
+    achieved = alg[dominant] / (mean_ph[dominant] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "algorithmic_bytes": alg[dominant],
+                "phase_ms": mean_ph,
+                "per_kernel_gbs": {k: alg[k] / (mean_ph[k] / 1e3) / 1e9 for k in alg
+                                   if mean_ph[k] > 0}}
+
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            try:
+                cpu = cpu_baseline(job, args.cpu_seconds)
+            except Exception as ex:  # the baseline is reported, never required
+                cpu = {"error": str(ex)}
+        lat = np.array(ms_steps)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": WORKLOAD, "input_mib": in_bytes / MiB,
+                       "output_mib": bytes_out / MiB, "entries_in": n_in, "entries_out": n_keep,
+                       "output_files": len(r.files), "parallelism": f"replicas{world}",
+                       "l2": "flushed between steps (256 MiB write)", "scale": args.scale},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99))},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+/*
+ * luda_b200 -- B200 (sm_100a) LSM compaction engine, C ABI.
+ *
+ * This is the boundary a LevelDB host calls in place of the body of
+ * DBImpl::DoCompactionWork (reference: db/db_impl.cc:1060 for the CPU version
+ * and db/db_impl.cc:1229 for LUDA's GPU version).  The version set, MANIFEST
+ * edits, file numbering and file I/O stay in the host; the engine receives the
+ * bytes of the input tables plus the few pieces of version state the
+ * compaction loop reads, and returns the bytes of the output tables, which are
+ * byte-identical to what the reference's CPU DoCompactionWork would write.
+ *
+ * All entry points are extern "C", take plain pointers and sizes, never throw,
+ * and return an lc_status.  Nothing here is thread-safe unless stated.
+ */
+#ifndef LUDA_B200_H_
+#define LUDA_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference returns leveldb::Status; LC_ERR_CORRUPT maps to
+ * Status::Corruption, LC_ERR_INVALID_ARG to Status::InvalidArgument and the
+ * rest to Status::IOError in the host shim. */
+typedef enum {
+  LC_OK = 0,
+  LC_ERR_INVALID_ARG = 1, /* bad descriptor, option or handle */
+  LC_ERR_CORRUPT = 2,     /* an input table failed a format check */
+  LC_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  LC_ERR_NO_MEMORY = 4,   /* device or host allocation failed */
+  LC_ERR_BUDGET = 5,      /* job larger than the engine's device budget */
+  LC_ERR_TIMEOUT = 6,     /* lc_job_wait timed out, or a device wait gave up */
+  LC_ERR_UNSUPPORTED = 7, /* input beyond an engine limit (e.g. >= 4 GiB) */
+  LC_ERR_SHUTDOWN = 8     /* engine is being destroyed */
+} lc_status;
+
+typedef struct lc_engine lc_engine;
+typedef struct lc_job lc_job;
+
+typedef struct {
+  int32_t device;               /* CUDA device ordinal */
+  uint64_t device_budget_bytes; /* admission budget; 0 = 40 GiB */
+  int32_t max_inflight_jobs;    /* jobs on the device at once; 0 = 4 */
+  uint32_t flags;               /* LC_FLAG_* */
+} lc_config;
+
+/* lc_config.flags: record CUDA events around each phase of every job on the
+ * job's own stream and report the device time per phase in lc_job_out. */
+#define LC_FLAG_PHASE_TIMING 1u
+
+/* One input SSTable (the bytes of a file at level L or L+1). */
+typedef struct {
+  const uint8_t* data; /* host pointer, or device pointer if inputs_on_device */
+  uint64_t size;       /* FileMetaData::file_size */
+} lc_table;
+
+/* A file at a level >= L+2, by key range (FileMetaData, db/version_edit.h:18). */
+typedef struct {
+  const uint8_t* smallest; /* internal key, host memory */
+  uint32_t smallest_len;
+  const uint8_t* largest; /* internal key, host memory */
+  uint32_t largest_len;
+  uint64_t file_size;
+  int32_t level;
+} lc_file_range;
+
+/* The Options fields that shape output bytes (include/leveldb/options.h). */
+typedef struct {
+  uint32_t block_size;       /* Options::block_size */
+  uint32_t restart_interval; /* Options::block_restart_interval */
+  int32_t bits_per_key;      /* NewBloomFilterPolicy(bits_per_key); <= 0: no filter */
+  uint64_t max_file_size;    /* Compaction::MaxOutputFileSize() */
+} lc_table_options;
+
+/* One compaction.  Replaces the CompactionState* argument of
+ * DBImpl::DoCompactionWork (db/db_impl.cc:1060): the tables are those of
+ * Compaction::inputs_[0] and inputs_[1] (db/version_set.h:380) in the order
+ * VersionSet::MakeInputIterator makes merge children (db/version_set.cc:
+ * 1237-1268): one child ("run") per level-0 file, one run per level >= 1
+ * holding that level's files in key order. */
+typedef struct {
+  int32_t level;            /* Compaction::level() */
+  int32_t n_tables;         /* all input tables, run-major */
+  const lc_table* tables;
+  int32_t n_runs;           /* merge children */
+  const int32_t* run_table_count; /* tables per run, sums to n_tables */
+  int32_t n_grandparents;   /* Compaction::grandparents_ (db/version_set.cc:1446) */
+  const lc_file_range* grandparents;
+  int32_t n_base_files;     /* every file at levels >= L+2, by level then key,
+                               for Compaction::IsBaseLevelForKey (:1535) */
+  const lc_file_range* base_files;
+  uint64_t smallest_snapshot; /* CompactionState::smallest_snapshot (db/db_impl.cc:1073) */
+  lc_table_options options;
+  int32_t inputs_on_device; /* 1: lc_table.data are device pointers on the engine's device */
+  int32_t outputs_on_device;/* 1: leave output bytes on the device (lc_job_out.data is a
+                               device pointer); 0: copy them to host memory */
+} lc_job_desc;
+
+/* Output of one compaction: what DoCompactionWork records in
+ * CompactionState::outputs (db/db_impl.cc:197-201) plus the file bytes.  The
+ * host assigns file numbers and writes the files.  All pointers stay valid
+ * until lc_job_release. */
+typedef struct {
+  int32_t n_files;
+  const uint8_t* data;          /* all output files back to back */
+  const uint64_t* file_offset;  /* n_files, offset of file i in data */
+  const uint64_t* file_size;    /* n_files */
+  const uint64_t* file_entries; /* n_files, TableBuilder::NumEntries() */
+  const uint8_t* key_bytes;     /* smallest/largest internal keys, packed */
+  const uint64_t* smallest_offset; /* n_files + 0: key i at key_bytes[off, off+len) */
+  const uint32_t* smallest_len;
+  const uint64_t* largest_offset;
+  const uint32_t* largest_len;
+  uint64_t bytes_in;    /* sum of input table sizes (CompactionStats::bytes_read) */
+  uint64_t bytes_out;   /* sum of output sizes (CompactionStats::bytes_written) */
+  uint64_t entries_in;  /* entries read */
+  uint64_t entries_out; /* entries written */
+  double device_ms;     /* device time of the job, first copy to last (CUDA events) */
+  uint32_t kernel_launches; /* kernels the job launched */
+  uint32_t n_phases;        /* > 0 with LC_FLAG_PHASE_TIMING */
+  const char* const* phase_name;
+  const float* phase_ms;    /* device time per phase */
+  uint64_t key_bytes_in;    /* decoded internal-key bytes (input) */
+  uint64_t value_bytes_out; /* value bytes written */
+  uint64_t key_bytes_out;   /* internal-key bytes of the survivors */
+} lc_job_out;
+
+/* Engine lifetime.  An engine owns one CUDA device, its streams, a stream-
+ * ordered device memory pool and a set of worker threads. */
+lc_status lc_engine_create(const lc_config* cfg, lc_engine** out);
+void lc_engine_destroy(lc_engine* e);
+
+/* Asynchronous jobs (thread-safe).  lc_job_submit copies the descriptor (not
+ * the table bytes: host table buffers must stay valid until lc_job_wait
+ * returns) and admits the job against the device budget; jobs beyond the
+ * in-flight limit queue on the host.  lc_job_wait blocks until the job is done
+ * or timeout_ns passes (< 0: forever). */
+lc_status lc_job_submit(lc_engine* e, const lc_job_desc* desc, lc_job** out);
+lc_status lc_job_wait(lc_job* j, int64_t timeout_ns);
+lc_status lc_job_result(lc_job* j, lc_job_out* out);
+void lc_job_release(lc_job* j);
+
+/* Synchronous compaction on the calling thread: the drop-in for one
+ * DoCompactionWork call.  *job_out must be released with lc_job_release. */
+lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_job** job_out);
+
+/* Flush encoder: one table from n sorted internal keys and values, the GPU
+ * counterpart of BuildTable's TableBuilder loop (db/builder.cc:17-60; LUDA's
+ * GPUWriteLevel0, db/db_impl.cc:86-181).  Keys/values are packed with n+1
+ * offsets, all in host memory (or device memory if on_device).  The table is
+ * returned like a one-file compaction output (no size split). */
+lc_status lc_build_table(lc_engine* e, const lc_table_options* opt, int64_t n,
+                         const uint8_t* keys, const uint64_t* key_offsets,
+                         const uint8_t* values, const uint64_t* value_offsets,
+                         int32_t on_device, lc_job_out* out, lc_job** job_out);
+
+/* Human-readable message for the last error on this engine (thread-local). */
+const char* lc_last_error(void);
+const char* lc_status_string(lc_status s);
+
+/* Library version. */
+const char* lc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUDA_B200_H_ */

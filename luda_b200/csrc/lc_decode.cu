@@ -1,0 +1,401 @@
+// Decode: input tables -> entries (keys reconstructed into a key arena, values
+// left in place).
+//
+// Follows the reference's table reader: Footer::DecodeFrom
+// (table/format.cc:42-62), the index block's block handles
+// (table/table.cc:38-111), and Block::Iter's entry parse (table/block.cc:
+// 170-190, 340-367).  The LUDA restart word (table/block_builder.cc:62-66,
+// 90-96) is (offset << 8) | entries in that restart run, so every restart run
+// is decoded independently: the run's first entry has no shared prefix, and
+// the run's entry count is known from the word before any entry is parsed.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "lc_device.cuh"
+#include "lc_kernels.h"
+
+namespace lc {
+
+namespace {
+
+constexpr uint32_t kMagicLo = 0x8b80fb57u;  // kTableMagicNumber (table/format.h:77)
+constexpr uint32_t kMagicHi = 0xdb477524u;
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_excl(T v, T* total) {
+  const int lane = threadIdx.x & 31;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T u = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += u;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+// Locates the index block of a table; false if the footer is invalid.
+__device__ bool parse_footer(const uint8_t* t, uint64_t n, uint64_t* i_off, uint64_t* i_size) {
+  if (n < kFooter) return false;
+  const uint8_t* f = t + n - kFooter;
+  if (ld_le32(f + 40) != kMagicLo || ld_le32(f + 44) != kMagicHi) return false;
+  uint64_t m_off, m_size;
+  const uint8_t* p = f;
+  const uint8_t* lim = f + 40;
+  if (!(p = get_varint64(p, lim, &m_off))) return false;
+  if (!(p = get_varint64(p, lim, &m_size))) return false;
+  if (!(p = get_varint64(p, lim, i_off))) return false;
+  if (!(p = get_varint64(p, lim, i_size))) return false;
+  if (*i_off > n || *i_size < 4 || *i_size + kTrailer > n - *i_off) return false;
+  return true;
+}
+
+// Parses one entry header at p (bounded by lim).  Returns the key-delta
+// pointer or nullptr.
+__device__ __forceinline__ const uint8_t* entry_header(const uint8_t* p, const uint8_t* lim,
+                                                       uint32_t* shared, uint32_t* non_shared,
+                                                       uint32_t* vlen) {
+  if (lim - p < 3) return nullptr;
+  uint32_t a = p[0], b = p[1], c = p[2];
+  if ((a | b | c) < 128) {
+    *shared = a;
+    *non_shared = b;
+    *vlen = c;
+    p += 3;
+  } else {
+    if (!(p = get_varint32(p, lim, shared))) return nullptr;
+    if (!(p = get_varint32(p, lim, non_shared))) return nullptr;
+    if (!(p = get_varint32(p, lim, vlen))) return nullptr;
+  }
+  if ((uint64_t)(lim - p) < (uint64_t)*non_shared + *vlen) return nullptr;
+  return p;
+}
+
+__global__ void k_table_index_count(JobDev J) {
+  const uint32_t t = blockIdx.x;
+  const TableDesc T = J.tables[t];
+  const uint8_t* base = J.in + T.off;
+  __shared__ uint64_t s_ioff, s_isize;
+  __shared__ uint32_t s_nr, s_ok;
+  __shared__ uint32_t s_part[32];
+  if (threadIdx.x == 0) {
+    uint64_t io = 0, is = 0;
+    bool ok = parse_footer(base, T.size, &io, &is);
+    uint32_t nr = 0;
+    if (ok) {
+      nr = ld_le32(base + io + is - 4);
+      if ((uint64_t)nr * 4 + 4 > is) ok = false;
+    }
+    if (!ok) set_error(J.ctr, kErrBadFooter, t);
+    s_ioff = io;
+    s_isize = is;
+    s_nr = nr;
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) {
+    if (threadIdx.x == 0) J.tbl_nblocks[t] = 0;
+    return;
+  }
+  const uint8_t* ra = base + s_ioff + s_isize - 4 - 4ull * s_nr;
+  uint32_t sum = 0;
+  for (uint32_t r = threadIdx.x; r < s_nr; r += blockDim.x) sum += ld_le32(ra + 4ull * r) & 0xff;
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) s += s_part[w];
+    J.tbl_nblocks[t] = s;
+  }
+}
+
+__global__ void k_table_index_entries(JobDev J) {
+  const uint32_t t = blockIdx.x;
+  const TableDesc T = J.tables[t];
+  const uint8_t* base = J.in + T.off;
+  uint64_t io, is;
+  if (!parse_footer(base, T.size, &io, &is)) return;  // error already recorded
+  const uint32_t nr = ld_le32(base + io + is - 4);
+  if ((uint64_t)nr * 4 + 4 > is) return;
+  const uint8_t* idx = base + io;
+  const uint64_t ra_off = is - 4 - 4ull * nr;
+  const uint8_t* ra = idx + ra_off;
+  const uint64_t out_base = J.tbl_block_base[t];
+  const uint64_t out_end = J.tbl_block_base[t + 1];
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base_r = 0; base_r < nr; base_r += blockDim.x) {
+    const uint32_t r = base_r + threadIdx.x;
+    uint32_t w = r < nr ? ld_le32(ra + 4ull * r) : 0;
+    uint32_t cnt = w & 0xff;
+    // block-wide exclusive scan of cnt
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t tot;
+    uint32_t ex = warp_excl(cnt, &tot);
+    if (lane == 0) s_warp[wid] = tot;
+    __syncthreads();
+    uint32_t before = s_carry;
+    for (int k = 0; k < wid; k++) before += s_warp[k];
+    uint32_t all = 0;
+    for (int k = 0; k < (int)((blockDim.x + 31) / 32); k++) all += s_warp[k];
+    ex += before;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += all;
+    if (r < nr) {
+      uint64_t start = w >> 8;
+      uint64_t end = (r + 1 < nr) ? (ld_le32(ra + 4ull * (r + 1)) >> 8) : ra_off;
+      bool ok = start <= end && end <= ra_off;
+      const uint8_t* p = idx + start;
+      const uint8_t* lim = idx + end;
+      for (uint32_t k = 0; ok && k < cnt; k++) {
+        uint32_t sh, ns, vl;
+        const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
+        if (!q) {
+          ok = false;
+          break;
+        }
+        q += ns;
+        uint64_t b_off, b_size;
+        const uint8_t* h = q;
+        if (!(h = get_varint64(h, q + vl, &b_off)) || !(h = get_varint64(h, q + vl, &b_size))) {
+          ok = false;
+          break;
+        }
+        if (b_off > T.size || b_size + kTrailer > T.size - b_off) {
+          ok = false;
+          break;
+        }
+        const uint64_t o = out_base + ex + k;
+        if (o >= out_end) {
+          ok = false;
+          break;
+        }
+        J.blk_off[o] = T.off + b_off;
+        J.blk_size[o] = (uint32_t)b_size;
+        J.blk_run[o] = T.run;
+        p = q + vl;
+      }
+      if (ok && p != lim) ok = false;
+      if (!ok) set_error(J.ctr, kErrBadIndex, t);
+    }
+    __syncthreads();
+  }
+}
+
+// Walks the entries of one restart run without writing them: counts key bytes
+// and validates every header against the run's bounds.
+__device__ __forceinline__ bool walk_run(const uint8_t* p, const uint8_t* lim, uint32_t cnt,
+                                         uint64_t* kbytes, uint32_t* maxk, bool* short_key) {
+  uint32_t prev = 0;
+  uint64_t kb = 0;
+  for (uint32_t k = 0; k < cnt; k++) {
+    uint32_t sh, ns, vl;
+    const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
+    if (!q) return false;
+    if ((k == 0 && sh != 0) || sh > prev) return false;
+    uint32_t kl = sh + ns;
+    if (kl < 8) *short_key = true;
+    kb += kl;
+    *maxk = max(*maxk, kl);
+    prev = kl;
+    p = q + ns + vl;
+  }
+  *kbytes = kb;
+  return p == lim;
+}
+
+struct BlockView {
+  const uint8_t* p;
+  uint64_t ra;  // offset of the restart array (end of entries)
+  uint32_t nr;
+  bool ok;
+};
+
+__device__ __forceinline__ BlockView block_view(const JobDev& J, uint64_t b) {
+  BlockView v;
+  v.p = J.in + J.blk_off[b];
+  const uint32_t size = J.blk_size[b];
+  v.ok = size >= 4;
+  v.nr = v.ok ? ld_le32(v.p + size - 4) : 0;
+  if (v.ok && (uint64_t)v.nr * 4 + 4 > size) v.ok = false;
+  v.ra = v.ok ? size - 4 - 4ull * v.nr : 0;
+  return v;
+}
+
+__device__ __forceinline__ void run_bounds(const BlockView& v, uint32_t r, uint64_t* start,
+                                           uint64_t* end, uint32_t* cnt) {
+  const uint32_t w = ld_le32(v.p + v.ra + 4ull * r);
+  *cnt = w & 0xff;
+  *start = w >> 8;
+  *end = (r + 1 < v.nr) ? (ld_le32(v.p + v.ra + 4ull * (r + 1)) >> 8) : v.ra;
+}
+
+__device__ void block_count_one(const JobDev& J, uint64_t b, uint32_t lane) {
+  BlockView v = block_view(J, b);
+  uint64_t ent = 0, kb = 0;
+  uint32_t maxk = 0;
+  bool ok = v.ok, short_key = false;
+  for (uint32_t r = lane; ok && r < v.nr; r += 32) {
+    uint64_t s, e;
+    uint32_t cnt;
+    run_bounds(v, r, &s, &e, &cnt);
+    if (s > e || e > v.ra) {
+      ok = false;
+      break;
+    }
+    uint64_t rk = 0;
+    if (!walk_run(v.p + s, v.p + e, cnt, &rk, &maxk, &short_key)) {
+      ok = false;
+      break;
+    }
+    ent += cnt;
+    kb += rk;
+  }
+  const bool all_ok = __all_sync(0xffffffffu, ok);
+  const bool any_short = __any_sync(0xffffffffu, short_key);
+  ent = warp_sum(ent);
+  kb = warp_sum(kb);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+  if (lane == 0) {
+    if (!all_ok) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
+    else if (any_short) set_error(J.ctr, kErrShortKey, (uint32_t)b);
+    J.blk_nent[b] = all_ok ? (uint32_t)ent : 0;
+    J.blk_kbytes[b] = all_ok ? kb : 0;
+    atomicMax(&J.ctr->max_klen, maxk);
+  }
+}
+
+__global__ void k_block_count(JobDev J) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nblk = J.ctr->n_blocks_in;
+  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk;
+       b += stride)
+    block_count_one(J, b, lane);
+}
+
+__global__ void k_run_bounds(JobDev J) {
+  // one thread: entries of merge child r start at the first block of its
+  // first table
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t next_run = 0;
+  for (uint32_t t = 0; t < J.n_tables; t++) {
+    while (next_run <= J.tables[t].run) {
+      J.run_entry_begin_w[next_run] = J.blk_ent_base[J.tbl_block_base[t]];
+      next_run++;
+    }
+  }
+  while (next_run <= J.n_runs) {
+    J.run_entry_begin_w[next_run] = J.ctr->n_entries_in;
+    next_run++;
+  }
+}
+
+__global__ void k_block_decode(JobDev J) {
+  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (b >= J.ctr->n_blocks_in) return;
+  if (J.ctr->error) return;
+  BlockView v = block_view(J, b);
+  uint64_t ent_carry = J.blk_ent_base[b];
+  uint64_t key_carry = J.blk_key_base[b];
+  for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    uint64_t s = 0, e = 0, rk = 0;
+    uint32_t cnt = 0, maxk = 0;
+    bool sk = false;
+    if (r < v.nr) {
+      run_bounds(v, r, &s, &e, &cnt);
+      walk_run(v.p + s, v.p + e, cnt, &rk, &maxk, &sk);
+    }
+    uint64_t cnt_tot, kb_tot;
+    uint64_t ent = warp_excl<uint64_t>(cnt, &cnt_tot) + ent_carry;
+    uint64_t kpos = warp_excl<uint64_t>(rk, &kb_tot) + key_carry;
+    ent_carry += cnt_tot;
+    key_carry += kb_tot;
+    if (r < v.nr) {
+      const uint8_t* p = v.p + s;
+      const uint8_t* lim = v.p + e;
+      uint64_t prev = kpos;
+      for (uint32_t k = 0; k < cnt; k++) {
+        uint32_t sh, ns, vl;
+        const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
+        if (!q) break;
+        const uint32_t kl = sh + ns;
+        if (kpos + kl > J.cap_key_bytes || ent >= J.cap_entries) {
+          set_error(J.ctr, kErrArenaOverflow, (uint32_t)b);
+          return;
+        }
+        uint8_t* dst = J.keys + kpos;
+        for (uint32_t i = 0; i < sh; i++) dst[i] = J.keys[prev + i];
+        for (uint32_t i = 0; i < ns; i++) dst[sh + i] = q[i];
+        J.e_koff[ent] = (uint32_t)kpos;
+        J.e_klen[ent] = kl;
+        J.e_voff[ent] = (uint32_t)((q + ns) - J.in);
+        J.e_vlen[ent] = vl;
+        J.e_pfx[ent] = user_prefix(dst, kl);
+        prev = kpos;
+        kpos += kl;
+        ent++;
+        p = q + ns + vl;
+      }
+    }
+  }
+}
+
+__global__ void k_entries_from_offsets(JobDev J, const uint64_t* koffs, const uint64_t* voffs,
+                                       uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t ko = koffs[i], kl = koffs[i + 1] - ko;
+  if (kl < 8) {
+    set_error(J.ctr, kErrShortKey, (uint32_t)i);
+    return;
+  }
+  J.e_koff[i] = (uint32_t)ko;
+  J.e_klen[i] = (uint32_t)kl;
+  J.e_voff[i] = (uint32_t)voffs[i];
+  J.e_vlen[i] = (uint32_t)(voffs[i + 1] - voffs[i]);
+  J.e_pfx[i] = user_prefix(J.keys + ko, (uint32_t)kl);
+  J.k_ids[i] = (uint32_t)i;
+}
+
+}  // namespace
+
+void launch_table_index_count(const JobDev& J, cudaStream_t st) {
+  note_launch(), k_table_index_count<<<J.n_tables, 128, 0, st>>>(J);
+}
+void launch_table_index_entries(const JobDev& J, cudaStream_t st) {
+  note_launch(), k_table_index_entries<<<J.n_tables, 128, 0, st>>>(J);
+}
+void launch_block_count(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
+  // grid-stride over the device-side block count: at most 148 SMs x 16 CTAs
+  uint64_t ctas = (std::max<uint64_t>(n_blocks_cap, 1) * 32 + 255) / 256;
+  ctas = std::min<uint64_t>(ctas, 148 * 16);
+  note_launch(), k_block_count<<<(unsigned)ctas, 256, 0, st>>>(J);
+}
+void launch_run_bounds(const JobDev& J, cudaStream_t st) { note_launch(), k_run_bounds<<<1, 32, 0, st>>>(J); }
+void launch_block_decode(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
+  uint64_t warps = n_blocks_cap ? n_blocks_cap : 1;
+  note_launch(), k_block_decode<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(J);
+}
+void launch_entries_from_offsets(const JobDev& J, const uint64_t* koffs, const uint64_t* voffs,
+                                 uint64_t n, cudaStream_t st) {
+  if (n == 0) return;
+  note_launch(), k_entries_from_offsets<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, koffs, voffs, n);
+}
+
+}  // namespace lc

@@ -1,0 +1,243 @@
+// Device-side codecs and comparisons for the LevelDB table format.
+//
+// Restated from the reference's host code: varint/fixed codecs
+// (util/coding.cc:9-192), the internal-key order (db/dbformat.cc:51-67), the
+// bloom hash (util/hash.cc:22-51) and CRC32C (util/crc32c.cc:276; reflected
+// Castagnoli polynomial 0x82F63B78 with pre/post inversion).  The CRC is
+// computed from a 256-entry table built from the polynomial at kernel start and
+// combined across lanes with multiplication by x^(8n) mod P in GF(2)[x].
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lc_job.h"
+
+namespace lc {
+
+constexpr uint32_t kCrcPoly = 0x82F63B78u;
+constexpr uint64_t kSeekTag = (((1ull << 56) - 1) << 8) | 1ull;  // PackSequenceAndType(kMax, kTypeValue)
+constexpr uint32_t kFilterBaseLg = 11;                             // table/filter_block.cc:14
+constexpr uint32_t kTrailer = 5;                                   // type byte + crc
+constexpr uint32_t kFooter = 48;                                   // table/format.h:61
+
+__device__ __forceinline__ uint32_t ld_le32(const uint8_t* p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+__device__ __forceinline__ uint64_t ld_le64(const uint8_t* p) {
+  return (uint64_t)ld_le32(p) | ((uint64_t)ld_le32(p + 4) << 32);
+}
+__device__ __forceinline__ void st_le32(uint8_t* p, uint32_t v) {
+  p[0] = (uint8_t)v;
+  p[1] = (uint8_t)(v >> 8);
+  p[2] = (uint8_t)(v >> 16);
+  p[3] = (uint8_t)(v >> 24);
+}
+
+// LEB128 decode bounded by `lim`; nullptr on truncation or overlong input.
+__device__ __forceinline__ const uint8_t* get_varint32(const uint8_t* p, const uint8_t* lim,
+                                                       uint32_t* v) {
+  uint32_t r = 0;
+  for (uint32_t shift = 0; shift <= 28 && p < lim; shift += 7) {
+    uint32_t b = *p++;
+    if (b & 128) {
+      r |= (b & 127) << shift;
+    } else {
+      *v = r | (b << shift);
+      return p;
+    }
+  }
+  return nullptr;
+}
+__device__ __forceinline__ const uint8_t* get_varint64(const uint8_t* p, const uint8_t* lim,
+                                                       uint64_t* v) {
+  uint64_t r = 0;
+  for (uint32_t shift = 0; shift <= 63 && p < lim; shift += 7) {
+    uint64_t b = *p++;
+    if (b & 128) {
+      r |= (b & 127) << shift;
+    } else {
+      *v = r | (b << shift);
+      return p;
+    }
+  }
+  return nullptr;
+}
+__host__ __device__ __forceinline__ uint32_t varint_len(uint64_t v) {
+  uint32_t n = 1;
+  while (v >= 128) {
+    v >>= 7;
+    n++;
+  }
+  return n;
+}
+__device__ __forceinline__ uint8_t* put_varint(uint8_t* p, uint64_t v) {
+  while (v >= 128) {
+    *p++ = (uint8_t)(v | 128);
+    v >>= 7;
+  }
+  *p++ = (uint8_t)v;
+  return p;
+}
+
+// Bytewise comparison (Slice::compare): memcmp, then length.
+__device__ __forceinline__ int bytes_cmp(const uint8_t* a, uint32_t al, const uint8_t* b,
+                                         uint32_t bl) {
+  uint32_t m = al < bl ? al : bl;
+  for (uint32_t i = 0; i < m; i++) {
+    if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+  }
+  return al < bl ? -1 : (al > bl ? 1 : 0);
+}
+
+// InternalKeyComparator::Compare (db/dbformat.cc:51-67).
+__device__ __forceinline__ int ikey_cmp(const uint8_t* a, uint32_t al, const uint8_t* b,
+                                        uint32_t bl) {
+  int r = bytes_cmp(a, al - 8, b, bl - 8);
+  if (r == 0) {
+    uint64_t an = ld_le64(a + al - 8), bn = ld_le64(b + bl - 8);
+    r = an > bn ? -1 : (an < bn ? 1 : 0);
+  }
+  return r;
+}
+
+// Big-endian value of the first 8 user-key bytes, zero padded: equal prefixes
+// say nothing, different prefixes order the keys.
+__device__ __forceinline__ uint64_t user_prefix(const uint8_t* k, uint32_t klen) {
+  uint32_t u = klen - 8;
+  uint64_t v = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) v = (v << 8) | (uint64_t)((uint32_t)i < u ? k[i] : 0);
+  return v;
+}
+
+// Compare two decoded entries by internal key.
+__device__ __forceinline__ int entry_cmp(const JobDev& J, uint32_t a, uint32_t b) {
+  uint64_t pa = J.e_pfx[a], pb = J.e_pfx[b];
+  if (pa != pb) return pa < pb ? -1 : 1;
+  return ikey_cmp(J.keys + J.e_koff[a], J.e_klen[a], J.keys + J.e_koff[b], J.e_klen[b]);
+}
+
+// Same user key?
+__device__ __forceinline__ bool same_user_key(const JobDev& J, uint32_t a, uint32_t b) {
+  if (J.e_pfx[a] != J.e_pfx[b]) return false;
+  uint32_t al = J.e_klen[a] - 8, bl = J.e_klen[b] - 8;
+  if (al != bl) return false;
+  const uint8_t* x = J.keys + J.e_koff[a];
+  const uint8_t* y = J.keys + J.e_koff[b];
+  for (uint32_t i = 0; i < al; i++)
+    if (x[i] != y[i]) return false;
+  return true;
+}
+
+// util/hash.cc:22-51.
+__device__ __forceinline__ uint32_t leveldb_hash(const uint8_t* data, uint32_t n, uint32_t seed) {
+  const uint32_t m = 0xc6a4a793u;
+  const uint8_t* limit = data + n;
+  uint32_t h = seed ^ (n * m);
+  while (data + 4 <= limit) {
+    h += ld_le32(data);
+    data += 4;
+    h *= m;
+    h ^= (h >> 16);
+  }
+  switch (limit - data) {
+    case 3:
+      h += (uint32_t)data[2] << 16;
+      [[fallthrough]];
+    case 2:
+      h += (uint32_t)data[1] << 8;
+      [[fallthrough]];
+    case 1:
+      h += data[0];
+      h *= m;
+      h ^= (h >> 24);
+      break;
+  }
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// CRC32C
+
+// Fills a 256-entry byte table in shared memory (call with all threads, then
+// __syncthreads()).
+__device__ __forceinline__ void crc_table_init(uint32_t* tab) {
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = i;
+#pragma unroll
+    for (int k = 0; k < 8; k++) c = (c & 1) ? (c >> 1) ^ kCrcPoly : (c >> 1);
+    tab[i] = c;
+  }
+}
+
+// Raw CRC register update (no inversion) over n bytes.
+__device__ __forceinline__ uint32_t crc_raw(const uint32_t* tab, uint32_t c, const uint8_t* p,
+                                            uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) c = tab[(c ^ p[i]) & 0xff] ^ (c >> 8);
+  return c;
+}
+
+// a * b mod P in the reflected representation (bit 31 = x^0).
+__host__ __device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
+  uint32_t p = 0;
+  for (int i = 0; i < 32; i++) {
+    if (a & 0x80000000u) p ^= b;
+    a <<= 1;
+    b = (b & 1) ? (b >> 1) ^ kCrcPoly : (b >> 1);
+  }
+  return p;
+}
+
+// x^(8n) mod P: table lookup for small n, square-and-multiply from the table
+// entries x^(8*2^k) beyond it.
+__device__ __forceinline__ uint32_t crc_xpow8(const JobDev& J, uint64_t n) {
+  const uint64_t N = J.crc_xpow_n;
+  if (n < N) return J.crc_xpow[n];
+  // n = q*N + r:  x^(8n) = (x^(8N))^q * x^(8r), the power by squaring.
+  uint32_t r = J.crc_xpow[n % N];
+  uint64_t q = n / N;
+  uint32_t base = gf2_mulmod(J.crc_xpow[N - 1], J.crc_xpow[1]);  // x^(8N)
+  while (q) {
+    if (q & 1) r = gf2_mulmod(r, base);
+    base = gf2_mulmod(base, base);
+    q >>= 1;
+  }
+  return r;
+}
+
+// shift(c, n): the raw CRC register after feeding n zero bytes.
+__device__ __forceinline__ uint32_t crc_shift(const JobDev& J, uint32_t c, uint64_t n) {
+  return gf2_mulmod(crc_xpow8(J, n), c);
+}
+
+// Masked CRC32C of contents followed by a zero type byte: the block trailer
+// of table/table_builder.cc:186-189, computed cooperatively by one warp over
+// `n` bytes at `p` (the type byte is appended implicitly).
+__device__ __forceinline__ uint32_t warp_block_crc(const JobDev& J, const uint32_t* tab,
+                                                   const uint8_t* p, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t total = n + 1;  // contents + type byte 0
+  uint32_t seg = (total + 31) / 32;
+  uint32_t b = lane * seg;
+  uint32_t e = min(total, b + seg);
+  uint32_t c = 0;
+  for (uint32_t i = b; i < e; i++) {
+    uint8_t byte = i < n ? p[i] : 0;
+    c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
+  }
+  // shift each lane's raw CRC by the bytes after its segment, xor together
+  uint32_t after = total > e ? total - e : 0;
+  uint32_t v = (b < total) ? crc_shift(J, c, after) : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  // init 0xffffffff contributes shift(~0, total); final inversion
+  uint32_t full = v ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+  return ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
+}
+
+// Error reporting: the first error code wins.
+__device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t detail) {
+  if (atomicCAS(&c->error, 0u, code) == 0u) c->error_detail = detail;
+}
+
+}  // namespace lc

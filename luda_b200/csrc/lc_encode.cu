@@ -1,0 +1,649 @@
+// Encode: survivors -> output tables, byte-identical to the reference's
+// TableBuilder driven by DoCompactionWork.
+//
+// Reference behaviour reproduced here:
+// * BlockBuilder (table/block_builder.cc:56-114): prefix compression against
+//   the previous key of the block, a restart every `restart_interval` entries,
+//   LUDA restart words (offset << 8) | run length, size estimate
+//   buffer + 4 * restarts + 4.
+// * TableBuilder::Add / Flush (table/table_builder.cc:94-140): a block is
+//   flushed as soon as the estimate reaches block_size after an add.
+// * DoCompactionWork's output split (db/db_impl.cc:1105-1111, 1174-1180): a
+//   file ends once its flushed bytes (blocks + 5-byte trailers) reach
+//   max_file_size, or before the first survivor at or after a grandparent cut.
+// * Index block (table_builder.cc:101-108, 228-234): restart interval 1, one
+//   entry per block keyed by FindShortestSeparator / FindShortSuccessor
+//   (db/dbformat.cc:69-101, util/comparator.cc:29-64).
+// * Filter block (table/filter_block.cc:21-76, util/bloom.cc:28-54): one
+//   bloom filter per 2 KiB of data-block start offsets over the user keys of
+//   the blocks that start there; empty filters for skipped indices.
+// * Metaindex, footer (table_builder.cc:213-252, table/format.cc:31-40) and
+//   masked CRC32C trailers (table_builder.cc:178-195).
+//
+// Block boundaries form a chain: where the next block starts depends on where
+// this one started (restart positions and the prefix-compression reset).  Each
+// survivor s gets next(s), the start of the following block if a block began
+// at s.  The chain from survivor 0 is resolved in three steps: per chunk of
+// survivors, a table of exits for every possible entry point (pointer chasing
+// in shared memory); one thread composing the tables across chunks; and a
+// per-chunk chase from the resolved entry point that marks block starts.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lc_device.cuh"
+#include "lc_kernels.h"
+
+namespace lc {
+
+namespace {
+
+constexpr uint32_t kNoSep = 0xffffffffu;
+__constant__ char kFilterName[] = "filter.leveldb.BuiltinBloomFilter2";
+constexpr uint32_t kFilterNameLen = 34;
+
+template <typename T>
+__device__ __forceinline__ T warp_excl(T v, T* total) {
+  const int lane = threadIdx.x & 31;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T u = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += u;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__device__ __forceinline__ uint32_t bloom_bytes(uint64_t n, int bpk) {
+  uint64_t bits = n * (uint64_t)bpk;
+  if (bits < 64) bits = 64;
+  return (uint32_t)((bits + 7) / 8);
+}
+
+__device__ __forceinline__ const uint8_t* kept_key(const JobDev& J, uint64_t k, uint32_t* len) {
+  const uint32_t id = J.k_ids[k];
+  *len = J.e_klen[id];
+  return J.keys + J.e_koff[id];
+}
+
+__global__ void k_sizes(JobDev J) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = k < J.ctr->n_kept;
+  uint32_t kl = 0, vl = 0;
+  if (valid) {
+    const uint8_t* key = kept_key(J, k, &kl);
+    vl = J.e_vlen[J.k_ids[k]];
+    uint32_t shared = 0;
+    if (k > 0) {
+      uint32_t pl;
+      const uint8_t* pk = kept_key(J, k - 1, &pl);
+      const uint32_t m = min(kl, pl);
+      while (shared < m && pk[shared] == key[shared]) shared++;
+    }
+    J.k_a[k] = 1 + varint_len(kl) + varint_len(vl) + kl + vl;
+    J.k_b[k] = varint_len(shared) + varint_len(kl - shared) + varint_len(vl) + (kl - shared) + vl;
+    J.k_shared[k] = shared;
+  }
+  // survivor byte totals, one atomic per warp
+  unsigned long long kb = kl, vb = vl;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    kb += __shfl_xor_sync(0xffffffffu, kb, o);
+    vb += __shfl_xor_sync(0xffffffffu, vb, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (kb | vb)) {
+    atomicAdd((unsigned long long*)&J.ctr->kept_key_bytes, kb);
+    atomicAdd((unsigned long long*)&J.ctr->kept_value_bytes, vb);
+  }
+}
+
+__global__ void k_next(JobDev J) {
+  const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t n = J.ctr->n_kept;
+  if (s >= n) return;
+  const uint32_t R = J.restart_interval;
+  const uint64_t bs = J.block_size;
+  uint64_t buf = 0;
+  uint64_t e = s;
+  uint32_t j = 0;
+  uint64_t nxt;
+  while (true) {
+    if (e >= n) {
+      nxt = n;
+      break;
+    }
+    if (j > 0 && J.k_forced[e]) {
+      nxt = e;
+      break;
+    }
+    buf += (j % R == 0) ? J.k_a[e] : J.k_b[e];
+    const uint64_t est = buf + 4ull * (1 + j / R) + 4;
+    if (est >= bs) {
+      nxt = e + 1;
+      break;
+    }
+    j++;
+    e++;
+  }
+  J.k_next[s] = (uint32_t)nxt;
+  atomicMax(&J.ctr->max_jump, (uint32_t)(nxt - s));
+}
+
+// Per chunk: exits of the chain for every entry point in the first `window`
+// survivors of the chunk.
+__global__ void k_chain_tables(JobDev J) {
+  extern __shared__ uint32_t s_next[];
+  const uint64_t n = J.ctr->n_kept;
+  const uint32_t C = J.chunk;
+  const uint64_t c0 = (uint64_t)blockIdx.x * C;
+  if (c0 >= n) return;
+  const uint64_t c1 = min(n, c0 + C);
+  const uint32_t W = J.ctr->max_jump;
+  if (W > C) return;  // resolved sequentially instead
+  for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < W; i += blockDim.x) {
+    uint64_t e = c0 + i;
+    while (e < c1) e = s_next[e - c0];
+    J.chunk_table[(uint64_t)blockIdx.x * C + i] = (uint32_t)e;
+  }
+}
+
+__global__ void k_chain_resolve(JobDev J) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint64_t n = J.ctr->n_kept;
+  const uint32_t C = J.chunk;
+  const uint32_t W = J.ctr->max_jump;
+  if (n == 0) return;
+  if (W > C) {
+    // blocks longer than a chunk: walk the whole chain
+    uint64_t e = 0;
+    while (e < n) {
+      J.k_bstart[e] = 1;
+      e = J.k_next[e];
+    }
+    return;
+  }
+  const uint64_t M = (n + C - 1) / C;
+  uint64_t e = 0;
+  for (uint64_t c = 0; c < M; c++) {
+    J.chunk_entry[c] = (uint32_t)e;
+    const uint64_t c0 = c * C;
+    if (e < n) e = J.chunk_table[c * C + (e - c0)];
+  }
+}
+
+__global__ void k_chain_mark(JobDev J) {
+  extern __shared__ uint32_t s_next[];
+  const uint64_t n = J.ctr->n_kept;
+  const uint32_t C = J.chunk;
+  if (J.ctr->max_jump > C) return;
+  const uint64_t c0 = (uint64_t)blockIdx.x * C;
+  if (c0 >= n) return;
+  const uint64_t c1 = min(n, c0 + C);
+  for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t e = J.chunk_entry[blockIdx.x];
+    while (e < c1) {
+      J.k_bstart[e] = 1;
+      e = s_next[e - c0];
+    }
+  }
+}
+
+__global__ void k_block_list(JobDev J) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t n = J.ctr->n_kept;
+  if (k == 0) J.b_first[J.k_block[n]] = (uint32_t)n;
+  if (k < n && J.k_bstart[k]) J.b_first[J.k_block[k]] = (uint32_t)k;
+}
+
+__global__ void k_block_sizes(JobDev J, uint32_t* tmp32) {
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= J.ctr->n_blocks_out) return;
+  const uint32_t R = J.restart_interval;
+  const uint64_t s = J.b_first[b], e = J.b_first[b + 1];
+  uint64_t sum = 0;
+  for (uint64_t j = 0; j < e - s; j++) sum += (j % R == 0) ? J.k_a[s + j] : J.k_b[s + j];
+  const uint64_t nrest = (e - s + R - 1) / R;
+  const uint32_t size = (uint32_t)(sum + 4 * nrest + 4);
+  J.b_size[b] = size;
+  tmp32[b] = size + kTrailer;
+}
+
+// Output files: size cuts at block ends, grandparent cuts at forced blocks.
+__global__ void k_files(JobDev J) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint64_t nb = J.ctr->n_blocks_out;
+  const uint64_t nk = J.ctr->n_kept;
+  const uint32_t nt = J.ctr->n_triggers;
+  uint32_t f = 0, tp = 0;
+  uint64_t b = 0;
+  while (b < nb) {
+    const uint64_t start = b;
+    uint64_t next_forced = nb;
+    while (tp < nt) {
+      const uint32_t kp = J.kept_pos[J.triggers[tp]];
+      if (kp >= nk) {
+        tp = nt;
+        break;
+      }
+      const uint64_t fb = J.k_block[kp];
+      if (fb <= start) {
+        tp++;
+        continue;
+      }
+      next_forced = fb;
+      break;
+    }
+    const uint64_t cum0 = J.b_cum[start];
+    const uint64_t target =
+        J.max_file_size > ~0ull - cum0 ? ~0ull : cum0 + J.max_file_size;  // saturating
+    uint64_t sc;
+    if (J.b_cum[nb] < target) {
+      sc = nb - 1;
+    } else {
+      uint64_t lo = start, hi = nb - 1;
+      while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (J.b_cum[mid + 1] >= target) hi = mid;
+        else lo = mid + 1;
+      }
+      sc = lo;
+    }
+    const uint64_t end = min(sc, next_forced - 1);
+    if (f >= J.cap_files) {
+      set_error(J.ctr, kErrLimit, 2);
+      break;
+    }
+    FileOut& F = J.files[f];
+    F.first_block = (uint32_t)start;
+    F.end_block = (uint32_t)(end + 1);
+    F.first_kept = J.b_first[start];
+    F.end_kept = J.b_first[end + 1];
+    f++;
+    b = end + 1;
+  }
+  J.ctr->n_files = f;
+}
+
+__device__ __forceinline__ uint32_t file_of_block(const JobDev& J, uint64_t b) {
+  uint32_t lo = 0, hi = J.ctr->n_files;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (J.files[mid].first_block <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_block_layout(JobDev J) {
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= J.ctr->n_blocks_out) return;
+  const uint32_t f = file_of_block(J, b);
+  const uint32_t fb0 = J.files[f].first_block, fb1 = J.files[f].end_block;
+  const uint64_t base = J.b_cum[fb0];
+  const uint64_t off = J.b_cum[b] - base;
+  J.b_file[b] = f;
+  J.b_off[b] = off;
+  // filter group: blocks of this file whose start offsets share off >> 11
+  uint32_t gbytes = 0, gkeys = 0;
+  if (J.bits_per_key > 0) {
+    const uint64_t j = off >> kFilterBaseLg;
+    const bool start = (b == fb0) || (((J.b_cum[b - 1] - base) >> kFilterBaseLg) != j);
+    if (start) {
+      uint64_t n = 0;
+      for (uint64_t bb = b; bb < fb1 && ((J.b_cum[bb] - base) >> kFilterBaseLg) == j; bb++)
+        n += J.b_first[bb + 1] - J.b_first[bb];
+      gkeys = (uint32_t)n;
+      gbytes = bloom_bytes(n, J.bits_per_key) + 1;
+    }
+  }
+  J.b_gbytes[b] = gbytes;
+  J.b_gkeys[b] = gkeys;
+  // index key for this block
+  uint32_t llen;
+  const uint8_t* lkey = kept_key(J, J.b_first[b + 1] - 1, &llen);
+  const uint32_t ulen = llen - 8;
+  uint32_t sep = kNoSep, ilen = llen;
+  if (b + 1 < fb1) {
+    uint32_t nlen;
+    const uint8_t* nkey = kept_key(J, J.b_first[b + 1], &nlen);
+    const uint32_t nul = nlen - 8;
+    const uint32_t m = min(ulen, nul);
+    uint32_t d = 0;
+    while (d < m && lkey[d] == nkey[d]) d++;
+    if (d < m) {
+      const uint32_t db = lkey[d];
+      if (db < 0xff && db + 1 < nkey[d] && d + 1 < ulen) {
+        sep = d;
+        ilen = d + 1 + 8;
+      }
+    }
+  } else {
+    uint32_t i = 0;
+    while (i < ulen && lkey[i] == 0xff) i++;
+    if (i < ulen && i + 1 < ulen) {
+      sep = i;
+      ilen = i + 1 + 8;
+    }
+  }
+  const uint32_t hl = varint_len(off) + varint_len(J.b_size[b]);
+  J.b_sep[b] = sep;
+  J.b_ilen[b] = ilen;
+  J.b_isize[b] = 1 + varint_len(ilen) + varint_len(hl) + ilen + hl;
+}
+
+__global__ void k_file_layout(JobDev J) {
+  const uint32_t nf = J.ctr->n_files;
+  for (uint32_t f = threadIdx.x; f < nf; f += blockDim.x) {
+    FileOut& F = J.files[f];
+    const uint32_t fb0 = F.first_block, fb1 = F.end_block;
+    const uint64_t D = J.b_cum[fb1] - J.b_cum[fb0];
+    F.data_bytes = D;
+    uint64_t meta_off;
+    if (J.bits_per_key > 0) {
+      const uint64_t o_last = J.b_cum[fb1 - 1] - J.b_cum[fb0];
+      const uint32_t nfl = (uint32_t)((D >> kFilterBaseLg) +
+                                      ((D >> kFilterBaseLg) == (o_last >> kFilterBaseLg) ? 1 : 0));
+      const uint64_t Ft = J.b_gcum[fb1] - J.b_gcum[fb0];
+      const uint64_t fsize = Ft + 4ull * nfl + 4 + 1;
+      F.filter_off = D;
+      F.filter_size = fsize;
+      F.n_filters = nfl;
+      meta_off = D + fsize + kTrailer;
+      F.meta_size = 3 + kFilterNameLen + varint_len(D) + varint_len(fsize) + 8;
+    } else {
+      F.filter_off = 0;
+      F.filter_size = 0;
+      F.n_filters = 0;
+      meta_off = D;
+      F.meta_size = 8;
+    }
+    F.meta_off = meta_off;
+    F.index_off = meta_off + F.meta_size + kTrailer;
+    F.index_size = (J.b_icum[fb1] - J.b_icum[fb0]) + 4ull * (fb1 - fb0) + 4;
+    F.size = F.index_off + F.index_size + kTrailer + kFooter;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t o = 0;
+    for (uint32_t f = 0; f < nf; f++) {
+      J.files[f].out_off = o;
+      o += J.files[f].size;
+    }
+    J.ctr->bytes_out = o;
+  }
+}
+
+// One warp per output data block.
+__global__ void k_encode_blocks(JobDev J) {
+  __shared__ uint32_t tab[256];
+  crc_table_init(tab);
+  __syncthreads();
+  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (b >= J.ctr->n_blocks_out) return;
+  const FileOut& F = J.files[J.b_file[b]];
+  uint8_t* dst = J.out + F.out_off + J.b_off[b];
+  const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
+  const uint32_t R = J.restart_interval;
+  const uint32_t bsz = J.b_size[b];
+  const uint64_t nrest = (n + R - 1) / R;
+  uint8_t* ra = dst + bsz - 4 * nrest - 4;
+  uint64_t carry = 0;
+  for (uint64_t j0 = 0; j0 < n; j0 += 32) {
+    const uint64_t j = j0 + lane;
+    const bool valid = j < n;
+    const bool restart = (j % R) == 0;
+    const uint64_t k = s + j;
+    const uint64_t size = valid ? (restart ? J.k_a[k] : J.k_b[k]) : 0;
+    uint64_t tot;
+    const uint64_t ex = warp_excl<uint64_t>(size, &tot) + carry;
+    carry += tot;
+    if (valid) {
+      const uint32_t id = J.k_ids[k];
+      const uint32_t kl = J.e_klen[id], vl = J.e_vlen[id];
+      const uint8_t* key = J.keys + J.e_koff[id];
+      const uint8_t* val = J.in + J.e_voff[id];
+      const uint32_t sh = restart ? 0 : J.k_shared[k];
+      uint8_t* p = dst + ex;
+      p = put_varint(p, sh);
+      p = put_varint(p, kl - sh);
+      p = put_varint(p, vl);
+      for (uint32_t i = sh; i < kl; i++) *p++ = key[i];
+      for (uint32_t i = 0; i < vl; i++) *p++ = val[i];
+      if (restart) {
+        const uint64_t rem = n - j;
+        const uint32_t cnt = (uint32_t)(rem < R ? rem : R);
+        st_le32(ra + 4 * (j / R), ((uint32_t)ex << 8) | cnt);
+      }
+    }
+  }
+  if (lane == 0) {
+    st_le32(dst + bsz - 4, (uint32_t)nrest);
+    dst[bsz] = 0;  // kNoCompression
+  }
+  __syncwarp();
+  const uint32_t crc = warp_block_crc(J, tab, dst, bsz);
+  if (lane == 0) st_le32(dst + bsz + 1, crc);
+}
+
+// One warp per filter group (at the group's first block).
+__global__ void k_encode_filters(JobDev J) {
+  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (b >= J.ctr->n_blocks_out || J.bits_per_key <= 0) return;
+  const FileOut& F = J.files[J.b_file[b]];
+  const uint32_t fb0 = F.first_block, fb1 = F.end_block;
+  uint8_t* fbase = J.out + F.out_off + F.filter_off;
+  const uint64_t Ft = J.b_gcum[fb1] - J.b_gcum[fb0];
+  const uint32_t gb = J.b_gbytes[b];
+  if (gb != 0) {
+    uint8_t* fdst = fbase + (J.b_gcum[b] - J.b_gcum[fb0]);
+    const uint32_t nbytes = gb - 1;
+    const uint64_t bits = (uint64_t)nbytes * 8;
+    for (uint32_t i = lane; i < nbytes; i += 32) fdst[i] = 0;
+    __syncwarp();
+    const uint64_t k0 = J.b_first[b];
+    const uint32_t nk = J.b_gkeys[b];
+    for (uint32_t i = lane; i < nk; i += 32) {
+      uint32_t kl;
+      const uint8_t* key = kept_key(J, k0 + i, &kl);
+      uint32_t h = leveldb_hash(key, kl - 8, 0xbc9f1d34u);
+      const uint32_t delta = (h >> 17) | (h << 15);
+      for (uint32_t q = 0; q < J.bloom_k; q++) {
+        const uint32_t bitpos = (uint32_t)(h % bits);
+        uint8_t* byte = fdst + (bitpos >> 3);
+        const uintptr_t a = reinterpret_cast<uintptr_t>(byte);
+        unsigned int* word = reinterpret_cast<unsigned int*>(a & ~uintptr_t(3));
+        atomicOr(word, 1u << ((a & 3) * 8 + (bitpos & 7)));
+        h += delta;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) fdst[nbytes] = (uint8_t)J.bloom_k;
+    // filter offsets of the empty indices before this group and of the group
+    const uint64_t jb = J.b_off[b] >> kFilterBaseLg;
+    const int64_t jprev = (b == fb0) ? -1 : (int64_t)(J.b_off[b - 1] >> kFilterBaseLg);
+    const uint32_t val = (uint32_t)(J.b_gcum[b] - J.b_gcum[fb0]);
+    for (int64_t jj = jprev + 1 + lane; jj <= (int64_t)jb; jj += 32)
+      st_le32(fbase + Ft + 4 * jj, val);
+  }
+}
+
+__global__ void k_encode_index(JobDev J) {
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= J.ctr->n_blocks_out) return;
+  const FileOut& F = J.files[J.b_file[b]];
+  const uint32_t fb0 = F.first_block, fb1 = F.end_block;
+  uint8_t* ib = J.out + F.out_off + F.index_off;
+  const uint64_t eoff = J.b_icum[b] - J.b_icum[fb0];
+  uint8_t* p = ib + eoff;
+  const uint32_t ilen = J.b_ilen[b], sep = J.b_sep[b];
+  const uint64_t off = J.b_off[b];
+  const uint32_t bsz = J.b_size[b];
+  *p++ = 0;
+  p = put_varint(p, ilen);
+  p = put_varint(p, varint_len(off) + varint_len(bsz));
+  uint32_t llen;
+  const uint8_t* lkey = kept_key(J, J.b_first[b + 1] - 1, &llen);
+  if (sep == kNoSep) {
+    for (uint32_t i = 0; i < ilen; i++) p[i] = lkey[i];
+  } else {
+    for (uint32_t i = 0; i < sep; i++) p[i] = lkey[i];
+    p[sep] = (uint8_t)(lkey[sep] + 1);
+    uint64_t t = kSeekTag;
+    for (int i = 0; i < 8; i++) p[sep + 1 + i] = (uint8_t)(t >> (8 * i));
+  }
+  p += ilen;
+  p = put_varint(p, off);
+  p = put_varint(p, bsz);
+  uint8_t* ra = ib + (J.b_icum[fb1] - J.b_icum[fb0]) + 4 * (b - fb0);
+  st_le32(ra, ((uint32_t)eoff << 8) | 1u);
+  if (b + 1 == fb1) st_le32(ra + 4, fb1 - fb0);
+}
+
+__global__ void k_encode_meta(JobDev J) {
+  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= J.ctr->n_files) return;
+  const FileOut& F = J.files[f];
+  uint8_t* base = J.out + F.out_off;
+  if (J.bits_per_key > 0) {
+    uint8_t* fb = base + F.filter_off;
+    const uint64_t Ft = J.b_gcum[F.end_block] - J.b_gcum[F.first_block];
+    const uint64_t jlast = J.b_off[F.end_block - 1] >> kFilterBaseLg;
+    for (uint64_t jj = jlast + 1; jj < F.n_filters; jj++) st_le32(fb + Ft + 4 * jj, (uint32_t)Ft);
+    st_le32(fb + Ft + 4ull * F.n_filters, (uint32_t)Ft);
+    fb[Ft + 4ull * F.n_filters + 4] = (uint8_t)kFilterBaseLg;
+    uint8_t* m = base + F.meta_off;
+    m[0] = 0;
+    m[1] = (uint8_t)kFilterNameLen;
+    m[2] = (uint8_t)(varint_len(F.filter_off) + varint_len(F.filter_size));
+    for (uint32_t i = 0; i < kFilterNameLen; i++) m[3 + i] = (uint8_t)kFilterName[i];
+    uint8_t* p = m + 3 + kFilterNameLen;
+    p = put_varint(p, F.filter_off);
+    p = put_varint(p, F.filter_size);
+    st_le32(p, 1u);  // restart word (0 << 8) | 1
+    st_le32(p + 4, 1u);
+  } else {
+    uint8_t* m = base + F.meta_off;
+    st_le32(m, 0u);
+    st_le32(m + 4, 1u);
+  }
+  uint8_t* foot = base + F.size - kFooter;
+  for (int i = 0; i < 40; i++) foot[i] = 0;
+  uint8_t* p = foot;
+  p = put_varint(p, F.meta_off);
+  p = put_varint(p, F.meta_size);
+  p = put_varint(p, F.index_off);
+  p = put_varint(p, F.index_size);
+  st_le32(foot + 40, 0x8b80fb57u);
+  st_le32(foot + 44, 0xdb477524u);
+}
+
+// Trailers of the filter, metaindex and index blocks: one CTA per block.
+__global__ void k_crc_regions(JobDev J) {
+  __shared__ uint32_t tab[256];
+  __shared__ uint32_t s_x[32];
+  crc_table_init(tab);
+  __syncthreads();
+  const uint32_t f = blockIdx.x / 3, which = blockIdx.x % 3;
+  if (f >= J.ctr->n_files) return;
+  if (which == 0 && J.bits_per_key <= 0) return;
+  const FileOut& F = J.files[f];
+  const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
+  const uint64_t len = which == 0 ? F.filter_size : (which == 1 ? F.meta_size : F.index_size);
+  uint8_t* p = J.out + F.out_off + off;
+  const uint64_t total = len + 1;
+  const uint64_t seg = (total + blockDim.x - 1) / blockDim.x;
+  const uint64_t b = (uint64_t)threadIdx.x * seg;
+  const uint64_t e = min(total, b + seg);
+  uint32_t c = 0;
+  for (uint64_t i = b; i < e; i++) {
+    const uint8_t byte = i < len ? p[i] : 0;
+    c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
+  }
+  uint32_t v = b < total ? crc_shift(J, c, total - e) : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s_x[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t x = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32; w++) x ^= s_x[w];
+    const uint32_t full = x ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+    p[len] = 0;
+    st_le32(p + len + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
+  }
+}
+
+__global__ void k_file_key_lens(JobDev J, uint32_t* lens) {
+  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= J.ctr->n_files) return;
+  uint32_t l0, l1;
+  kept_key(J, J.files[f].first_kept, &l0);
+  kept_key(J, J.files[f].end_kept - 1, &l1);
+  lens[2 * f] = l0;
+  lens[2 * f + 1] = l1;
+}
+
+__global__ void k_file_keys(JobDev J, uint8_t* out, const uint64_t* off) {
+  const uint32_t f = blockIdx.x;
+  if (f >= J.ctr->n_files) return;
+  for (int w = 0; w < 2; w++) {
+    uint32_t l;
+    const uint8_t* k = kept_key(J, w == 0 ? J.files[f].first_kept : J.files[f].end_kept - 1, &l);
+    uint8_t* d = out + off[2 * f + w];
+    for (uint32_t i = threadIdx.x; i < l; i += blockDim.x) d[i] = k[i];
+  }
+}
+
+inline unsigned grid_for(uint64_t n, unsigned per) { return (unsigned)((n + per - 1) / per) + (n == 0); }
+
+}  // namespace
+
+void launch_sizes(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
+  note_launch(), k_sizes<<<grid_for(n_cap, 256), 256, 0, st>>>(J);
+}
+void launch_next(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
+  note_launch(), k_next<<<grid_for(n_cap, 256), 256, 0, st>>>(J);
+}
+void launch_chain(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
+  const uint64_t chunks = (n_cap + J.chunk - 1) / J.chunk + 1;
+  const size_t smem = (size_t)J.chunk * sizeof(uint32_t);
+  note_launch(), k_chain_tables<<<(unsigned)chunks, 256, smem, st>>>(J);
+  note_launch(), k_chain_resolve<<<1, 32, 0, st>>>(J);
+  note_launch(), k_chain_mark<<<(unsigned)chunks, 128, smem, st>>>(J);
+}
+void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
+  note_launch(), k_block_list<<<grid_for(n_cap + 1, 256), 256, 0, st>>>(J);
+}
+void launch_block_sizes(const JobDev& J, uint32_t* tmp32, uint64_t nb_cap, cudaStream_t st) {
+  note_launch(), k_block_sizes<<<grid_for(nb_cap, 256), 256, 0, st>>>(J, tmp32);
+}
+void launch_files(const JobDev& J, cudaStream_t st) { note_launch(), k_files<<<1, 32, 0, st>>>(J); }
+void launch_block_layout(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
+  note_launch(), k_block_layout<<<grid_for(nb_cap, 256), 256, 0, st>>>(J);
+}
+void launch_file_layout(const JobDev& J, cudaStream_t st) { note_launch(), k_file_layout<<<1, 256, 0, st>>>(J); }
+void launch_encode_blocks(const JobDev& J, uint64_t nb, cudaStream_t st) {
+  if (nb) note_launch(), k_encode_blocks<<<grid_for(nb * 32, 256), 256, 0, st>>>(J);
+}
+void launch_encode_rest(const JobDev& J, uint64_t nb_cap, uint32_t n_files, cudaStream_t st) {
+  if (nb_cap == 0) return;
+  note_launch(), k_encode_filters<<<grid_for(nb_cap * 32, 256), 256, 0, st>>>(J);
+  note_launch(), k_encode_index<<<grid_for(nb_cap, 256), 256, 0, st>>>(J);
+  note_launch(), k_encode_meta<<<grid_for(n_files, 128), 128, 0, st>>>(J);
+  if (n_files) note_launch(), k_crc_regions<<<n_files * 3, 256, 0, st>>>(J);
+}
+void launch_file_key_lens(const JobDev& J, uint32_t n_files, uint32_t* lens, cudaStream_t st) {
+  note_launch(), k_file_key_lens<<<grid_for(n_files, 128), 128, 0, st>>>(J, lens);
+}
+void launch_file_keys(const JobDev& J, uint32_t n_files, uint8_t* key_out, const uint64_t* key_off,
+                      cudaStream_t st) {
+  if (n_files) note_launch(), k_file_keys<<<n_files, 64, 0, st>>>(J, key_out, key_off);
+}
+
+}  // namespace lc

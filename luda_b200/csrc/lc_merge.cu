@@ -1,0 +1,217 @@
+// Merge and drop: decoded runs -> survivors in output order.
+//
+// * Merge: the reference merges its children with MergingIterator
+//   (table/merger.cc:148, linear FindSmallest; on equal keys the earlier child
+//   wins).  Here the children are merged pairwise in rounds with merge path:
+//   each thread finds its output diagonal by binary search and merges a short
+//   stretch.  Ties go to the left (earlier) group, which keeps child order.
+// * Drop rule (db/db_impl.cc:1113-1147): an entry is hidden when the previous
+//   entry has the same user key and a sequence number <= smallest_snapshot;
+//   a deletion marker is dropped when its sequence number is <=
+//   smallest_snapshot and no file at a level >= L+2 covers its user key
+//   (Compaction::IsBaseLevelForKey, db/version_set.cc:1535-1554).  Keys whose
+//   type byte is not 0/1 (ParseInternalKey fails) are kept and reset the state.
+// * Grandparent cuts (Compaction::ShouldStopBefore, db/version_set.cc:
+//   1556-1579): evaluated for every merged key, dropped or not.  The number of
+//   grandparents whose largest key precedes each merged key is found by binary
+//   search; the cut positions are then a chain of threshold searches over the
+//   running overlap, which one thread resolves.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lc_device.cuh"
+#include "lc_kernels.h"
+
+namespace lc {
+
+namespace {
+
+constexpr int kMergeItems = 8;
+
+__global__ void k_iota(uint32_t* ids, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ids[i] = (uint32_t)i;
+}
+
+// Round with groups of `width` merge children; pairs (2p, 2p+1) merge.
+__global__ void k_merge_round(JobDev J, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                              uint32_t width) {
+  const uint64_t n = J.run_entry_begin[J.n_runs];
+  const uint64_t o0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kMergeItems;
+  if (o0 >= n) return;
+  const uint64_t o1 = min(n, o0 + kMergeItems);
+  uint64_t o = o0;
+  while (o < o1) {
+    // find the pair that owns output position o
+    uint32_t pair_runs = 2 * width;
+    uint32_t r0 = 0;
+    while (true) {
+      uint32_t r2 = min(r0 + pair_runs, J.n_runs);
+      if (o < J.run_entry_begin[r2]) break;
+      r0 = r2;
+    }
+    const uint32_t r1 = min(r0 + width, J.n_runs);
+    const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
+    const uint64_t a0 = J.run_entry_begin[r0], b0 = J.run_entry_begin[r1],
+                   b1 = J.run_entry_begin[r2];
+    const uint64_t na = b0 - a0, nb = b1 - b0;
+    const uint64_t stop = min(o1, b1);
+    if (nb == 0) {
+      for (; o < stop; o++) dst[o] = src[o];
+      continue;
+    }
+    const uint32_t* A = src + a0;
+    const uint32_t* B = src + b0;
+    const uint64_t d = o - a0;
+    uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (entry_cmp(J, A[mid], B[d - 1 - mid]) <= 0) lo = mid + 1;
+      else hi = mid;
+    }
+    uint64_t i = lo, j = d - lo;
+    for (; o < stop; o++) {
+      bool take_a = i < na && (j >= nb || entry_cmp(J, A[i], B[j]) <= 0);
+      dst[o] = take_a ? A[i++] : B[j++];
+    }
+  }
+}
+
+__device__ __forceinline__ bool is_base_level(const JobDev& J, const uint8_t* ukey, uint32_t ulen) {
+  for (uint32_t l = 0; l < J.n_base_levels; l++) {
+    uint32_t lo = J.base_level_begin[l], hi = J.base_level_begin[l + 1];
+    const uint32_t end = hi;
+    // first file whose largest user key >= ukey
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (bytes_cmp(ukey, ulen, J.base_keys + J.base_large_off[mid], J.base_large_len[mid]) > 0)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    if (lo < end &&
+        bytes_cmp(ukey, ulen, J.base_keys + J.base_small_off[lo], J.base_small_len[lo]) >= 0)
+      return false;
+  }
+  return true;
+}
+
+__global__ void k_drop(JobDev J, const uint32_t* __restrict__ ids) {
+  const uint64_t n = J.ctr->n_entries_in;
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const uint32_t id = ids[p];
+  const uint8_t* key = J.keys + J.e_koff[id];
+  const uint32_t klen = J.e_klen[id];
+  const uint64_t tag = ld_le64(key + klen - 8);
+  const uint32_t type = (uint32_t)(tag & 0xff);
+  const uint64_t seq = tag >> 8;
+  bool drop = false;
+  if (type <= 1) {
+    bool first = true;
+    uint64_t pseq = 0;
+    if (p > 0) {
+      const uint32_t pid = ids[p - 1];
+      const uint8_t* pkey = J.keys + J.e_koff[pid];
+      const uint64_t ptag = ld_le64(pkey + J.e_klen[pid] - 8);
+      if ((ptag & 0xff) <= 1 && same_user_key(J, pid, id)) {
+        first = false;
+        pseq = ptag >> 8;
+      }
+    }
+    if (!first && pseq <= J.smallest_snapshot) {
+      drop = true;
+    } else if (type == 0 && seq <= J.smallest_snapshot && is_base_level(J, key, klen - 8)) {
+      drop = true;
+    }
+  }
+  J.keep[p] = drop ? 0 : 1;
+  if (J.n_gp) {
+    // grandparents passed: count of g with key > largest[g]
+    uint32_t lo = 0, hi = J.n_gp;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi) >> 1;
+      const uint64_t go = J.gp_key_off[mid];
+      const uint32_t gl = (uint32_t)(J.gp_key_off[mid + 1] - go);
+      if (ikey_cmp(key, klen, J.gp_keys + go, gl) > 0) lo = mid + 1;
+      else hi = mid;
+    }
+    J.gp_idx[p] = lo;
+  }
+}
+
+__global__ void k_triggers(JobDev J) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint64_t n = J.ctr->n_entries_in;
+  uint32_t cnt = 0;
+  if (n > 0 && J.n_gp > 0) {
+    const uint64_t limit = (uint64_t)J.max_gp_overlap;
+    uint64_t base = J.gp_prefix[J.gp_idx[0]];
+    uint64_t t = 0;
+    while (t + 1 < n) {
+      if (J.gp_prefix[J.gp_idx[n - 1]] - base <= limit) break;
+      uint64_t lo = t + 1, hi = n - 1;
+      while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (J.gp_prefix[J.gp_idx[mid]] - base > limit) hi = mid;
+        else lo = mid + 1;
+      }
+      if (cnt >= J.cap_triggers) {
+        set_error(J.ctr, kErrLimit, 1);
+        break;
+      }
+      J.triggers[cnt++] = (uint32_t)lo;
+      base = J.gp_prefix[J.gp_idx[lo]];
+      t = lo;
+    }
+  }
+  J.ctr->n_triggers = cnt;
+}
+
+__global__ void k_kept_compact(JobDev J, const uint32_t* __restrict__ ids) {
+  const uint64_t n = J.ctr->n_entries_in;
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0) J.ctr->n_kept = J.kept_pos[n];
+  if (p < n && J.keep[p]) {
+    const uint32_t k = J.kept_pos[p];
+    J.k_ids[k] = ids[p];
+    J.k_forced[k] = 0;
+  }
+}
+
+__global__ void k_forced(JobDev J) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nk = J.kept_pos[J.ctr->n_entries_in];
+  if (i == 0 && nk > 0) J.k_forced[0] = 1;
+  if (i < J.ctr->n_triggers) {
+    const uint32_t kp = J.kept_pos[J.triggers[i]];
+    if (kp < nk) J.k_forced[kp] = 1;
+  }
+}
+
+}  // namespace
+
+void launch_iota(uint32_t* ids, uint64_t n, cudaStream_t st) {
+  if (n) note_launch(), k_iota<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ids, n);
+}
+
+void launch_merge_round(const JobDev& J, const uint32_t* src, uint32_t* dst, uint32_t width,
+                        uint64_t n, cudaStream_t st) {
+  const uint64_t threads = (n + kMergeItems - 1) / kMergeItems;
+  if (threads) note_launch(), k_merge_round<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(J, src, dst, width);
+}
+
+void launch_drop(const JobDev& J, uint64_t n, cudaStream_t st) {
+  if (n) note_launch(), k_drop<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, J.m_ids);
+}
+
+void launch_triggers(const JobDev& J, uint64_t n, cudaStream_t st) {
+  note_launch(), k_triggers<<<1, 32, 0, st>>>(J);
+}
+
+void launch_kept_compact(const JobDev& J, uint64_t n, cudaStream_t st) {
+  note_launch(), k_kept_compact<<<(unsigned)((n + 256) / 256), 256, 0, st>>>(J, J.m_ids);
+  note_launch(), k_forced<<<(J.cap_triggers + 255) / 256 + 1, 256, 0, st>>>(J);
+}
+
+}  // namespace lc

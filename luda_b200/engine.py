@@ -1,0 +1,317 @@
+"""ctypes binding of the engine's C ABI (``include/luda_b200.h``).
+
+``Engine.compact(job)`` is the Python-side counterpart of one
+``DBImpl::DoCompactionWork`` call (db/db_impl.cc:1060): it builds the
+descriptor from a :class:`luda_b200.job.CompactionJob` exactly as a patched
+LevelDB host would from its ``Compaction`` object, calls ``lc_compact`` and
+returns the output files with their smallest/largest internal keys.
+
+The shared library is required: if ``libluda_b200.so`` is missing or cannot be
+loaded the constructor raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .job import CompactionJob, Entries, TableOptions
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libluda_b200.so")
+
+_u8p = C.POINTER(C.c_uint8)
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+
+LC_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "corruption", 3: "cuda error", 4: "out of memory",
+          5: "over device budget", 6: "timeout", 7: "unsupported", 8: "shutting down"}
+
+
+class LcConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("device_budget_bytes", C.c_uint64),
+                ("max_inflight_jobs", C.c_int32), ("flags", C.c_uint32)]
+
+
+class LcTable(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_uint64)]
+
+
+class LcFileRange(C.Structure):
+    _fields_ = [("smallest", _u8p), ("smallest_len", C.c_uint32), ("largest", _u8p),
+                ("largest_len", C.c_uint32), ("file_size", C.c_uint64), ("level", C.c_int32)]
+
+
+class LcTableOptions(C.Structure):
+    _fields_ = [("block_size", C.c_uint32), ("restart_interval", C.c_uint32),
+                ("bits_per_key", C.c_int32), ("max_file_size", C.c_uint64)]
+
+
+class LcJobDesc(C.Structure):
+    _fields_ = [("level", C.c_int32), ("n_tables", C.c_int32), ("tables", C.POINTER(LcTable)),
+                ("n_runs", C.c_int32), ("run_table_count", C.POINTER(C.c_int32)),
+                ("n_grandparents", C.c_int32), ("grandparents", C.POINTER(LcFileRange)),
+                ("n_base_files", C.c_int32), ("base_files", C.POINTER(LcFileRange)),
+                ("smallest_snapshot", C.c_uint64), ("options", LcTableOptions),
+                ("inputs_on_device", C.c_int32), ("outputs_on_device", C.c_int32)]
+
+
+class LcJobOut(C.Structure):
+    _fields_ = [("n_files", C.c_int32), ("data", C.c_void_p), ("file_offset", _u64p),
+                ("file_size", _u64p), ("file_entries", _u64p), ("key_bytes", _u8p),
+                ("smallest_offset", _u64p), ("smallest_len", _u32p), ("largest_offset", _u64p),
+                ("largest_len", _u32p), ("bytes_in", C.c_uint64), ("bytes_out", C.c_uint64),
+                ("entries_in", C.c_uint64), ("entries_out", C.c_uint64), ("device_ms", C.c_double),
+                ("kernel_launches", C.c_uint32), ("n_phases", C.c_uint32),
+                ("phase_name", C.POINTER(C.c_char_p)), ("phase_ms", C.POINTER(C.c_float)),
+                ("key_bytes_in", C.c_uint64), ("value_bytes_out", C.c_uint64),
+                ("key_bytes_out", C.c_uint64)]
+
+LC_FLAG_PHASE_TIMING = 1
+
+
+EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wait",
+           "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
+           "lc_status_string", "lc_version"]
+
+
+class LcError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the engine library (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is not built; run luda_b200/build.py")
+    l = C.CDLL(path)
+    l.lc_engine_create.argtypes = [C.POINTER(LcConfig), C.POINTER(C.c_void_p)]
+    l.lc_engine_create.restype = C.c_int
+    l.lc_engine_destroy.argtypes = [C.c_void_p]
+    l.lc_engine_destroy.restype = None
+    l.lc_job_submit.argtypes = [C.c_void_p, C.POINTER(LcJobDesc), C.POINTER(C.c_void_p)]
+    l.lc_job_submit.restype = C.c_int
+    l.lc_job_wait.argtypes = [C.c_void_p, C.c_int64]
+    l.lc_job_wait.restype = C.c_int
+    l.lc_job_result.argtypes = [C.c_void_p, C.POINTER(LcJobOut)]
+    l.lc_job_result.restype = C.c_int
+    l.lc_job_release.argtypes = [C.c_void_p]
+    l.lc_job_release.restype = None
+    l.lc_compact.argtypes = [C.c_void_p, C.POINTER(LcJobDesc), C.POINTER(LcJobOut),
+                             C.POINTER(C.c_void_p)]
+    l.lc_compact.restype = C.c_int
+    l.lc_build_table.argtypes = [C.c_void_p, C.POINTER(LcTableOptions), C.c_int64, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                 C.POINTER(LcJobOut), C.POINTER(C.c_void_p)]
+    l.lc_build_table.restype = C.c_int
+    l.lc_last_error.argtypes = []
+    l.lc_last_error.restype = C.c_char_p
+    l.lc_status_string.argtypes = [C.c_int]
+    l.lc_status_string.restype = C.c_char_p
+    l.lc_version.argtypes = []
+    l.lc_version.restype = C.c_char_p
+    _lib = l
+    return l
+
+
+@dataclasses.dataclass
+class OutputFile:
+    data: bytes
+    smallest: bytes
+    largest: bytes
+    entries: int
+
+
+@dataclasses.dataclass
+class CompactionResult:
+    files: List[OutputFile]
+    bytes_in: int
+    bytes_out: int
+    entries_in: int
+    entries_out: int
+    device_ms: float
+    device_ptr: Optional[int] = None  # output base when left on the device
+    file_offsets: Optional[List[int]] = None
+    kernel_launches: int = 0
+    phase_ms: Optional[dict] = None
+    key_bytes_in: int = 0
+    value_bytes_out: int = 0
+    key_bytes_out: int = 0
+
+
+def _u8(b) -> np.ndarray:
+    if isinstance(b, np.ndarray):
+        return np.ascontiguousarray(b, dtype=np.uint8)
+    return np.frombuffer(bytes(b), np.uint8) if len(b) else np.zeros(1, np.uint8)
+
+
+class _Keep:
+    def __init__(self):
+        self.objs = []
+
+    def u8(self, b):
+        a = _u8(b)
+        self.objs.append(a)
+        return a.ctypes.data_as(_u8p)
+
+
+def table_options(o: TableOptions) -> LcTableOptions:
+    return LcTableOptions(o.block_size, o.restart_interval, o.bits_per_key, o.max_file_size)
+
+
+def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[int]] = None,
+              outputs_on_device: bool = False) -> LcJobDesc:
+    """The descriptor a patched DoCompactionWork would build from its
+    Compaction: runs in MakeInputIterator order, grandparents_, and every file
+    at levels >= L+2 for the base-level test."""
+    runs = job.runs()
+    tables = [f for r in runs for f in r]
+    t_arr = (LcTable * max(1, len(tables)))()
+    for i, f in enumerate(tables):
+        if device_tables is not None:
+            t_arr[i].data = device_tables[i]
+        else:
+            a = _u8(f.data)
+            keep.objs.append(a)
+            t_arr[i].data = a.ctypes.data
+        t_arr[i].size = len(f.data)
+    rc = (C.c_int32 * max(1, len(runs)))(*[len(r) for r in runs])
+
+    def ranges(fs):
+        arr = (LcFileRange * max(1, len(fs)))()
+        for i, f in enumerate(fs):
+            arr[i].smallest = keep.u8(f.smallest)
+            arr[i].smallest_len = len(f.smallest)
+            arr[i].largest = keep.u8(f.largest)
+            arr[i].largest_len = len(f.largest)
+            arr[i].file_size = f.file_size
+            arr[i].level = f.level
+        return arr
+
+    gp, base = job.grandparents(), job.base_files()
+    gpa, ba = ranges(gp), ranges(base)
+    keep.objs += [t_arr, rc, gpa, ba]
+    return LcJobDesc(job.level, len(tables), t_arr, len(runs), rc, len(gp), gpa, len(base), ba,
+                     job.smallest_snapshot(), table_options(job.options),
+                     1 if device_tables is not None else 0, 1 if outputs_on_device else 0)
+
+
+def _result(out: LcJobOut, on_device: bool) -> CompactionResult:
+    files = []
+    offs = []
+    for i in range(out.n_files):
+        off, size = out.file_offset[i], out.file_size[i]
+        offs.append(off)
+        data = b"" if on_device else C.string_at(out.data + off, size)
+        sm = C.string_at(C.addressof(out.key_bytes.contents) + out.smallest_offset[i],
+                         out.smallest_len[i])
+        lg = C.string_at(C.addressof(out.key_bytes.contents) + out.largest_offset[i],
+                         out.largest_len[i])
+        files.append(OutputFile(data, sm, lg, int(out.file_entries[i])))
+    phases = {out.phase_name[i].decode(): out.phase_ms[i] for i in range(out.n_phases)}
+    return CompactionResult(files, out.bytes_in, out.bytes_out, out.entries_in, out.entries_out,
+                            out.device_ms, out.data if on_device else None, offs,
+                            out.kernel_launches, phases or None, out.key_bytes_in,
+                            out.value_bytes_out, out.key_bytes_out)
+
+
+class Engine:
+    """One CUDA device's compaction engine (``lc_engine``)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_inflight: int = 4,
+                 phase_timing: bool = False):
+        self.lib = load_library()
+        cfg = LcConfig(device, budget_bytes, max_inflight,
+                       LC_FLAG_PHASE_TIMING if phase_timing else 0)
+        h = C.c_void_p()
+        st = self.lib.lc_engine_create(C.byref(cfg), C.byref(h))
+        if st != LC_OK:
+            raise LcError(st, self.lib.lc_last_error().decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lc_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st != LC_OK:
+            raise LcError(st, self.lib.lc_last_error().decode())
+
+    def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
+                outputs_on_device: bool = False) -> CompactionResult:
+        keep = _Keep()
+        d = make_desc(job, keep, device_tables, outputs_on_device)
+        out = LcJobOut()
+        jh = C.c_void_p()
+        self._check(self.lib.lc_compact(self.h, C.byref(d), C.byref(out), C.byref(jh)))
+        try:
+            return _result(out, outputs_on_device)
+        finally:
+            self.lib.lc_job_release(jh)
+
+    def submit(self, job: CompactionJob) -> "AsyncJob":
+        keep = _Keep()
+        d = make_desc(job, keep)
+        jh = C.c_void_p()
+        self._check(self.lib.lc_job_submit(self.h, C.byref(d), C.byref(jh)))
+        return AsyncJob(self, jh, keep)
+
+    def build_table(self, entries: Entries, options: TableOptions) -> bytes:
+        keys = _u8(entries.keys)
+        vals = _u8(entries.vals)
+        ko = np.ascontiguousarray(entries.koffs, np.uint64)
+        vo = np.ascontiguousarray(entries.voffs, np.uint64)
+        opt = table_options(options)
+        out = LcJobOut()
+        jh = C.c_void_p()
+        self._check(self.lib.lc_build_table(self.h, C.byref(opt), entries.n, keys.ctypes.data,
+                                            ko.ctypes.data, vals.ctypes.data, vo.ctypes.data, 0,
+                                            C.byref(out), C.byref(jh)))
+        try:
+            assert out.n_files == 1
+            return C.string_at(out.data + out.file_offset[0], out.file_size[0])
+        finally:
+            self.lib.lc_job_release(jh)
+
+
+class AsyncJob:
+    def __init__(self, eng: Engine, h, keep):
+        self.eng, self.h, self.keep = eng, h, keep
+
+    def wait(self, timeout_s: float = -1.0) -> CompactionResult:
+        lib = self.eng.lib
+        st = lib.lc_job_wait(self.h, int(timeout_s * 1e9) if timeout_s >= 0 else -1)
+        if st == 6:
+            raise TimeoutError("job not finished")
+        try:
+            self.eng._check(st)
+            out = LcJobOut()
+            self.eng._check(lib.lc_job_result(self.h, C.byref(out)))
+            return _result(out, False)
+        finally:
+            lib.lc_job_release(self.h)
+            self.h = None

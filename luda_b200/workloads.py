@@ -216,7 +216,7 @@ def l1_l2_at_size(seed: int = 1, scale: float = 1.0, n_l2_tables: int = 32,
                   n_l3_files: int = 160) -> CompactionJob:
     rng = np.random.default_rng(seed)
     table_bytes = int((2 << 20) * scale)
-    est_entry = 36 + 8 + 180 + 3
+    est_entry = 44 + 205 + 4  # mean internal key + mean clipped value + header
     n_l2 = max(16, n_l2_tables * table_bytes // est_entry)
     n_l1 = max(8, table_bytes // est_entry)
     # L2 ids: distinct Zipf draws in draw order; ~3% get a second version.
