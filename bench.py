@@ -230,13 +230,15 @@ def main():
     host_res = eng.compact(job)
     dev_res = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
     assert dev_res.bytes_out == host_res.bytes_out and len(dev_res.files) == len(host_res.files)
+    host_res.release()
+    dev_res.release()
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
     for _ in range(args.warmup):
-        eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+        eng.compact(job, device_tables=ptrs, outputs_on_device=True).release()
     barrier()
     torch.cuda.synchronize()
     ms_steps, phases, launches = [], [], 0
@@ -251,6 +253,7 @@ def main():
             r = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
             e1.record()
             torch.cuda.synchronize()
+            r.release()
             ms_steps.append(e0.elapsed_time(e1))
             phases.append(r.phase_ms)
             launches += r.kernel_launches
@@ -261,7 +264,7 @@ def main():
 
     # end to end through host buffers
     for _ in range(max(1, args.warmup // 2)):
-        eng.compact(job)
+        eng.compact(job).release()
     e2e_ms = []
     for _ in range(args.steps):
         flush.zero_()
@@ -269,6 +272,7 @@ def main():
         t0 = time.perf_counter()
         r = eng.compact(job)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        r.release()
     e2e_total = float(sum(e2e_ms))
     d2h = r.bytes_out
 

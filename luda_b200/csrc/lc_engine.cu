@@ -989,8 +989,9 @@ void lc_job_release(lc_job* j) {
   if (!j) return;
   if (j->h_out) j->eng->pinned.give(j->h_out, j->h_out_cap);
   if (j->d_out) {
+    // the job has completed; return the output to the stream-ordered pool
     cudaSetDevice(j->eng->device);
-    cudaFree(j->d_out);
+    cudaFreeAsync(j->d_out, 0);
   }
   delete j;
 }

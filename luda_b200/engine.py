@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import os
+import weakref
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -127,7 +128,7 @@ def load_library(path: str = LIB_PATH):
 
 @dataclasses.dataclass
 class OutputFile:
-    data: bytes
+    data: object  # bytes-like view of the file (zero copy while the result lives)
     smallest: bytes
     largest: bytes
     entries: int
@@ -148,6 +149,34 @@ class CompactionResult:
     key_bytes_in: int = 0
     value_bytes_out: int = 0
     key_bytes_out: int = 0
+    _handle: object = None
+
+    def release(self):
+        """Frees the job's output buffers (host pinned or device)."""
+        if self._handle is not None:
+            self._handle.release()
+            self._handle = None
+
+    def file_bytes(self) -> List[bytes]:
+        return [bytes(f.data) for f in self.files]
+
+
+class _JobHandle:
+    def __init__(self, lib, h, eng=None):
+        self.lib, self.h = lib, h
+        if eng is not None:
+            eng._live.add(self)
+
+    def release(self):
+        if self.h is not None:
+            self.lib.lc_job_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 def _u8(b) -> np.ndarray:
@@ -210,10 +239,13 @@ def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[
 def _result(out: LcJobOut, on_device: bool) -> CompactionResult:
     files = []
     offs = []
+    whole = None
+    if not on_device and out.bytes_out:
+        whole = np.ctypeslib.as_array(C.cast(out.data, _u8p), shape=(out.bytes_out,))
     for i in range(out.n_files):
         off, size = out.file_offset[i], out.file_size[i]
         offs.append(off)
-        data = b"" if on_device else C.string_at(out.data + off, size)
+        data = b"" if on_device else memoryview(whole[off:off + size])
         sm = C.string_at(C.addressof(out.key_bytes.contents) + out.smallest_offset[i],
                          out.smallest_len[i])
         lg = C.string_at(C.addressof(out.key_bytes.contents) + out.largest_offset[i],
@@ -239,9 +271,12 @@ class Engine:
         if st != LC_OK:
             raise LcError(st, self.lib.lc_last_error().decode())
         self.h = h
+        self._live = weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
+            for jh in list(self._live):
+                jh.release()
             self.lib.lc_engine_destroy(self.h)
             self.h = None
 
@@ -268,10 +303,9 @@ class Engine:
         out = LcJobOut()
         jh = C.c_void_p()
         self._check(self.lib.lc_compact(self.h, C.byref(d), C.byref(out), C.byref(jh)))
-        try:
-            return _result(out, outputs_on_device)
-        finally:
-            self.lib.lc_job_release(jh)
+        res = _result(out, outputs_on_device)
+        res._handle = _JobHandle(self.lib, jh, self)
+        return res
 
     def submit(self, job: CompactionJob) -> "AsyncJob":
         keep = _Keep()
@@ -311,7 +345,11 @@ class AsyncJob:
             self.eng._check(st)
             out = LcJobOut()
             self.eng._check(lib.lc_job_result(self.h, C.byref(out)))
-            return _result(out, False)
-        finally:
+        except Exception:
             lib.lc_job_release(self.h)
             self.h = None
+            raise
+        res = _result(out, False)
+        res._handle = _JobHandle(lib, self.h, self.eng)
+        self.h = None
+        return res

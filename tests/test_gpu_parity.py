@@ -52,7 +52,7 @@ def test_compaction_matches_reference(engine, built_jobs, case):
     assert len(res.files) == len(case["outputs"])
     for f, g in zip(res.files, case["outputs"]):
         assert len(f.data) == g["size"]
-        assert sha(f.data) == g["sha256"]
+        assert sha(bytes(f.data)) == g["sha256"]
         assert f.smallest.hex() == g["smallest"]
         assert f.largest.hex() == g["largest"]
     assert res.bytes_in == case["input_bytes"]
@@ -64,7 +64,7 @@ def test_compaction_matches_oracle(engine, built_jobs, case):
     job = built_jobs(case)
     res = engine.compact(job)
     ref = oracle.compact(job, "oracle")
-    assert [f.data for f in res.files] == [r[0] for r in ref]
+    assert res.file_bytes() == [r[0] for r in ref]
     assert [f.entries for f in res.files] == [len(oracle.read_table(r[0])) for r in ref]
 
 
@@ -92,11 +92,11 @@ def test_outputs_readable(engine, built_jobs):
     job = built_jobs(case)
     res = engine.compact(job)
     for f in res.files:
-        ents = oracle.read_table(f.data)
+        ents = oracle.read_table(bytes(f.data))
         assert len(ents) == f.entries
         assert ents[0][0] == f.smallest and ents[-1][0] == f.largest
         if oracle.has_ref():
-            assert oracle.read_table(f.data, "ref") == ents
+            assert oracle.read_table(bytes(f.data), "ref") == ents
 
 
 def test_device_resident_equals_host(engine, built_jobs):
@@ -123,7 +123,7 @@ def test_device_resident_equals_host(engine, built_jobs):
         err, = rt.cudaMemcpy(host_buf.ctypes.data, dev.device_ptr + dev.file_offsets[i], size,
                              rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
         assert err == rt.cudaError_t.cudaSuccess
-        assert host_buf.tobytes() == f.data
+        assert host_buf.tobytes() == bytes(f.data)
 
 
 def test_async_jobs_same_alone_and_in_mix(engine, built_jobs):
@@ -135,7 +135,7 @@ def test_async_jobs_same_alone_and_in_mix(engine, built_jobs):
     handles = [engine.submit(j) for j in jobs * 2]
     mixed = [h.wait() for h in handles]
     for a, m in zip(alone * 2, mixed):
-        assert [f.data for f in a.files] == [f.data for f in m.files]
+        assert a.file_bytes() == m.file_bytes()
 
 
 def _corrupt(job, fn):
@@ -174,4 +174,4 @@ def test_corrupt_input_reports_corruption(engine, kind):
     # the engine stays usable
     ok = workloads.plain_l0_l1(seed=8, scale=0.02)
     ok.materialize(lambda e, o: oracle.build_table(e, o, "oracle"))
-    assert [f.data for f in engine.compact(ok).files] == [x[0] for x in oracle.compact(ok)]
+    assert engine.compact(ok).file_bytes() == [x[0] for x in oracle.compact(ok)]
