@@ -157,6 +157,16 @@ lc_status lc_build_table(lc_engine* e, const lc_table_options* opt, int64_t n,
                          const uint8_t* values, const uint64_t* value_offsets,
                          int32_t on_device, lc_job_out* out, lc_job** job_out);
 
+/* Masked CRC32C of one buffer: crc32c::Mask(crc32c::Value(data, n))
+ * (util/crc32c.h:20-32), the value LevelDB stores in a block trailer
+ * (table/table_builder.cc:186-189) and that ReadBlock's verify_checksums path
+ * checks (table/format.cc:87-94).  Computed on the engine's device over many
+ * CTAs; data is host memory (copied in) or, with on_device, device memory.
+ * The result is written to *masked_crc (host memory).  Scratch comes from the
+ * engine's device memory pool. */
+lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_device,
+                    uint32_t* masked_crc);
+
 /* Human-readable message for the last error on this engine (thread-local). */
 const char* lc_last_error(void);
 const char* lc_status_string(lc_status s);

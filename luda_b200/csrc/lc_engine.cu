@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/luda_b200.h"
+#include "lc_crc_chunks.cuh"
 #include "lc_device.cuh"
 #include "lc_job.h"
 #include "lc_kernels.h"
@@ -1056,6 +1057,50 @@ lc_status lc_build_table(lc_engine* e, const lc_table_options* opt, int64_t n,
   fill_out(j, out);
   *job_out = j;
   return LC_OK;
+}
+
+lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_device,
+                    uint32_t* masked_crc) {
+  if (!e || !masked_crc || (n && !data)) return fail(LC_ERR_INVALID_ARG, "null argument");
+  cudaStream_t st = nullptr;
+  std::vector<void*> ptrs;
+  try {
+    CK(cudaSetDevice(e->device));
+    st = e->get_stream();
+    const uint8_t* d_data = data;
+    const uint32_t chunks = crc32c_chunk_count(n);
+    void* p = nullptr;
+    if (!on_device && n) {
+      CK(cudaMallocAsync(&p, n, st));
+      ptrs.push_back(p);
+      CK(cudaMemcpyAsync(p, data, n, cudaMemcpyHostToDevice, st));
+      d_data = (const uint8_t*)p;
+    }
+    // scratch: one register per chunk, the ticket counter, the result
+    CK(cudaMallocAsync(&p, ((size_t)chunks + 2) * sizeof(uint32_t), st));
+    ptrs.push_back(p);
+    uint32_t* partials = (uint32_t*)p;
+    uint32_t* counter = partials + chunks;
+    uint32_t* d_out = counter + 1;
+    CK(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st));
+    launch_crc32c_chunks(d_data, n, partials, counter, d_out, st);
+    CK(cudaGetLastError());
+    uint32_t h = 0;
+    CK(cudaMemcpyAsync(&h, d_out, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    for (void* q : ptrs) CK(cudaFreeAsync(q, st));
+    ptrs.clear();
+    CK(cudaStreamSynchronize(st));
+    e->put_stream(st);
+    *masked_crc = h;
+    return LC_OK;
+  } catch (const CudaError& ce) {
+    if (st) {
+      for (void* q : ptrs) cudaFreeAsync(q, st);
+      cudaStreamSynchronize(st);
+      e->put_stream(st);
+    }
+    return fail(LC_ERR_CUDA, std::string(ce.what) + ": " + cudaGetErrorString(ce.e));
+  }
 }
 
 }  // extern "C"

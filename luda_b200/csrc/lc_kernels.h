@@ -20,6 +20,10 @@ void scan_exclusive(const TI* in, TO* out, const uint64_t* n_dev, uint64_t n_cap
                     uint64_t* total_out, cudaStream_t st);
 uint64_t scan_scratch_elems(uint64_t n_cap);
 
+// lc_crc.cu -- masked CRC32C of one buffer; `counter` must be zero at launch
+void launch_crc32c_chunks(const uint8_t* data, uint64_t n, uint32_t* partials, uint32_t* counter,
+                          uint32_t* out, cudaStream_t st);
+
 // lc_decode.cu -- input tables -> decoded entries
 void launch_table_index_count(const JobDev& J, cudaStream_t st);
 void launch_table_index_entries(const JobDev& J, cudaStream_t st);

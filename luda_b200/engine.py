@@ -77,7 +77,7 @@ LC_FLAG_PHASE_TIMING = 1
 
 EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wait",
            "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
-           "lc_status_string", "lc_version"]
+           "lc_status_string", "lc_version", "lc_crc32c"]
 
 
 class LcError(RuntimeError):
@@ -120,6 +120,8 @@ def load_library(path: str = LIB_PATH):
     l.lc_last_error.restype = C.c_char_p
     l.lc_status_string.argtypes = [C.c_int]
     l.lc_status_string.restype = C.c_char_p
+    l.lc_crc32c.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(C.c_uint32)]
+    l.lc_crc32c.restype = C.c_int
     l.lc_version.argtypes = []
     l.lc_version.restype = C.c_char_p
     _lib = l
@@ -313,6 +315,17 @@ class Engine:
         jh = C.c_void_p()
         self._check(self.lib.lc_job_submit(self.h, C.byref(d), C.byref(jh)))
         return AsyncJob(self, jh, keep)
+
+    def crc32c(self, data=None, device_ptr: Optional[int] = None, n: int = 0) -> int:
+        """Masked CRC32C (LevelDB block-trailer form) of host bytes or of n
+        bytes at a device pointer."""
+        out = C.c_uint32()
+        if device_ptr is not None:
+            self._check(self.lib.lc_crc32c(self.h, device_ptr, n, 1, C.byref(out)))
+        else:
+            a = _u8(data)
+            self._check(self.lib.lc_crc32c(self.h, a.ctypes.data, len(data), 0, C.byref(out)))
+        return out.value
 
     def build_table(self, entries: Entries, options: TableOptions) -> bytes:
         keys = _u8(entries.keys)
