@@ -167,6 +167,28 @@ lc_status lc_build_table(lc_engine* e, const lc_table_options* opt, int64_t n,
 lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_device,
                     uint32_t* masked_crc);
 
+/* Allocation-free masked CRC32C.  No counterpart in the reference: it exists
+ * for hosts that cannot allocate device memory at the moment they need a
+ * checksum -- for example a host whose device memory is entirely owned by
+ * another allocator, or a path that must not take the device-wide
+ * synchronisation cudaMalloc/cudaFree imply.  It computes the same value as
+ * lc_crc32c, needs no engine, takes device pointers only (d_data: n input
+ * bytes; d_masked_crc: 4 output bytes), runs on `stream` (a cudaStream_t, or
+ * NULL for the default stream) and returns without waiting for the GPU.
+ *
+ * Scratch is one fixed static device array (about 64 KiB, held by every
+ * device that loads the library until the process exits), so n is limited to
+ * 1 GiB; larger buffers are rejected with LC_ERR_UNSUPPORTED before anything
+ * is launched.  Null pointers give LC_ERR_INVALID_ARG, runtime failures
+ * LC_ERR_CUDA.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  Every call clears the part of the array that must
+ * start at zero, but all calls share the array: calls that overlap on the GPU
+ * (on different streams, or from different threads) race, so serialise them,
+ * e.g. on one stream. */
+lc_status lc_crc32c_noalloc(const uint8_t* d_data, uint64_t n, uint32_t* d_masked_crc,
+                            void* stream);
+
 /* Human-readable message for the last error on this engine (thread-local). */
 const char* lc_last_error(void);
 const char* lc_status_string(lc_status s);

@@ -77,7 +77,7 @@ LC_FLAG_PHASE_TIMING = 1
 
 EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wait",
            "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
-           "lc_status_string", "lc_version", "lc_crc32c"]
+           "lc_status_string", "lc_version", "lc_crc32c", "lc_crc32c_noalloc"]
 
 
 class LcError(RuntimeError):
