@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "luda_b200.h")
 def declared_symbols():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(lc_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(lc_[a-z0-9_]+)\s*\(", src)))
 
 
 @pytest.fixture(scope="module")
