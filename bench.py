@@ -47,7 +47,7 @@ MiB = float(1 << 20)
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=400)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="luda", choices=["luda", "reference"])
     p.add_argument("--scale", type=float, default=1.0)
@@ -65,37 +65,41 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    """nvidia-smi samples (every 50 ms, written to a file) of SM clock and
+    throttle reasons; summary() keeps the samples taken while the timed region
+    ran (mark_start/mark_end)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
+        import tempfile
         self.device = device
-        self.samples = []
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+                 "--format=csv,noheader,nounits", "-lms", "50", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                self.samples.append(parts)
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -103,19 +107,39 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        import datetime
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 10:
+                        continue
+                    try:
+                        ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        continue
+                    rows.append((ts, parts))
+        except OSError:
+            pass
+        if self.t0 is not None:
+            win = [p for ts, p in rows if self.t0 - 0.06 <= ts <= (self.t1 or ts) + 0.06]
+        else:
+            win = [p for _, p in rows]
+        if not win:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"],
+                    "samples": 0, "samples_total": len(rows)}
+        sm = [float(p[2]) for p in win if p[2].replace(".", "").isdigit()]
+        mx = [float(p[3]) for p in win if p[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
-            for n, v in zip(names, s[5:9]):
+        for p in win:
+            for n, v in zip(names, p[6:10]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.samples)}
+                "samples": len(win)}
 
 
 def make_job(scale: float, seed: int):
@@ -202,7 +226,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     job = make_job(args.scale, 1 + 1000 * rank)
-    eng = Engine(local, phase_timing=True)
+    eng = Engine(local, phase_timing=True, max_inflight=4)
     # input tables built by the engine's own flush encoder
     job.materialize(lambda e, o: eng.build_table(e, o))
     tables = job.input_tables()
@@ -227,8 +251,10 @@ def main():
     torch.cuda.synchronize()
 
     # consistency of the two paths (untimed): same file sizes
-    host_res = eng.compact(job)
-    dev_res = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+    prep_dev = eng.prepare(job, device_tables=ptrs, outputs_on_device=True)
+    prep_host = eng.prepare(job)
+    host_res = eng.run(prep_host)
+    dev_res = eng.run(prep_dev)
     assert dev_res.bytes_out == host_res.bytes_out and len(dev_res.files) == len(host_res.files)
     host_res.release()
     dev_res.release()
@@ -238,19 +264,20 @@ def main():
             dist.barrier()
 
     for _ in range(args.warmup):
-        eng.compact(job, device_tables=ptrs, outputs_on_device=True).release()
+        eng.run(prep_dev).release()
     barrier()
     torch.cuda.synchronize()
     ms_steps, phases, launches = [], [], 0
     bytes_out = 0
     with ClockSampler(local) as clocks:
+        clocks.mark_start()
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            r = eng.compact(job, device_tables=ptrs, outputs_on_device=True)
+            r = eng.run(prep_dev)
             e1.record()
             torch.cuda.synchronize()
             r.release()
@@ -258,23 +285,42 @@ def main():
             phases.append(r.phase_ms)
             launches += r.kernel_launches
             bytes_out = r.bytes_out
+        clocks.mark_end()
     barrier()
     torch.cuda.synchronize()
     total_ms = float(sum(ms_steps))
 
-    # end to end through host buffers
+    # end to end through host buffers: K jobs through the asynchronous C ABI
+    # (lc_job_submit / lc_job_wait), at most `depth` in flight, so that one
+    # job's host<->device copies overlap another job's kernels.  Every job
+    # copies its own inputs in and its own outputs out.
+    depth = 3
     for _ in range(max(1, args.warmup // 2)):
-        eng.compact(job).release()
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = eng.compact(job)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        eng.run(prep_host).release()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    inflight, done = [], 0
+    submitted = 0
+    while done < args.steps:
+        while submitted < args.steps and len(inflight) < depth:
+            inflight.append(eng.submit_prepared(prep_host))
+            submitted += 1
+        r = inflight.pop(0).wait()
+        d2h = r.bytes_out
         r.release()
-    e2e_total = float(sum(e2e_ms))
-    d2h = r.bytes_out
+        done += 1
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_total = e0.elapsed_time(e1)
+    # the same, one job at a time (lc_compact), for reference
+    seq_ms = []
+    for _ in range(min(args.steps, 20)):
+        t0 = time.perf_counter()
+        r = eng.run(prep_host)
+        seq_ms.append((time.perf_counter() - t0) * 1e3)
+        r.release()
 
     # max over ranks
     if dist is not None:
@@ -311,7 +357,7 @@ def main():
 
     if rank == 0:
         cpu = None
-        if world == 1:
+        if world == 1 and args.cpu_seconds > 0:
             try:
                 cpu = cpu_baseline(job, args.cpu_seconds)
             except Exception as ex:  # the baseline is reported, never required
@@ -329,11 +375,15 @@ def main():
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps,
+                    "jobs_in_flight": depth,
+                    "sequential_ms_per_step": float(np.mean(seq_ms)),
+                    "sequential_value": in_bytes / MiB / (float(np.mean(seq_ms)) / 1e3)},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
+            "host": {"cpus": os.cpu_count()},
         }
         print(json.dumps(line))
     eng.close()

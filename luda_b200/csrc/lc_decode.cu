@@ -223,9 +223,11 @@ struct BlockView {
   bool ok;
 };
 
-__device__ __forceinline__ BlockView block_view(const JobDev& J, uint64_t b) {
+// View of data block b whose bytes are at `base` (a shared-memory stage or
+// the block in global memory).
+__device__ __forceinline__ BlockView block_view(const JobDev& J, uint64_t b, const uint8_t* base) {
   BlockView v;
-  v.p = J.in + J.blk_off[b];
+  v.p = base;
   const uint32_t size = J.blk_size[b];
   v.ok = size >= 4;
   v.nr = v.ok ? ld_le32(v.p + size - 4) : 0;
@@ -242,8 +244,52 @@ __device__ __forceinline__ void run_bounds(const BlockView& v, uint32_t r, uint6
   *end = (r + 1 < v.nr) ? (ld_le32(v.p + v.ra + 4ull * (r + 1)) >> 8) : v.ra;
 }
 
-__device__ void block_count_one(const JobDev& J, uint64_t b, uint32_t lane) {
-  BlockView v = block_view(J, b);
+// Per-warp shared memory of the staged decode kernels.
+constexpr uint32_t kDecWarps = 4;
+constexpr uint32_t kDecStage = 8448;    // data block bytes + 16-byte phase
+constexpr uint32_t kDecMaxEnt = 512;    // entries of one staged block
+constexpr uint32_t kDecKeyBuf = 4096 + 32;
+struct DecWarpSmem {
+  uint8_t stage[kDecStage];
+  uint8_t keybuf[kDecKeyBuf];
+  uint16_t dpos[kDecMaxEnt];  // key delta position in the stage
+  uint16_t sh[kDecMaxEnt];    // shared prefix
+  uint16_t kl[kDecMaxEnt];    // key length
+  uint16_t vl[kDecMaxEnt];    // value length
+};
+
+// Copies data block b into this warp's stage at the block's own 16-byte phase
+// with 16-byte loads; returns the staged pointer, or nullptr if it is too big.
+__device__ __forceinline__ const uint8_t* stage_block(const JobDev& J, uint64_t b, uint8_t* stage,
+                                                      uint32_t lane) {
+  const uint8_t* src = J.in + J.blk_off[b];
+  const uint32_t size = J.blk_size[b];
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uint32_t phase = (uint32_t)(a & 15);
+  if (size + phase + 16 > kDecStage) return nullptr;
+  const uintptr_t base = a - phase;
+  const uint32_t nch = (phase + size + 15) >> 4;
+  const uintptr_t lo = reinterpret_cast<uintptr_t>(J.in), hi = reinterpret_cast<uintptr_t>(J.in_end);
+  for (uint32_t c = lane; c < nch; c += 32) {
+    const uintptr_t q = base + 16ull * c;
+    if (q >= lo && q + 16 <= hi) {
+      cp_async16(stage + 16 * c, reinterpret_cast<const void*>(q));
+    } else {
+      uint32_t w[4] = {0, 0, 0, 0};
+      for (int i = 0; i < 16; i++) {
+        const uintptr_t x = q + i;
+        if (x >= a && x < a + size) w[i >> 2] |= (uint32_t)(*reinterpret_cast<const uint8_t*>(x)) << (8 * (i & 3));
+      }
+      *reinterpret_cast<uint4*>(stage + 16 * c) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+  cp_async_wait_all();
+  __syncwarp();
+  return stage + phase;
+}
+
+__device__ void block_count_one(const JobDev& J, uint64_t b, uint32_t lane, const uint8_t* base) {
+  BlockView v = block_view(J, b, base);
   uint64_t ent = 0, kb = 0;
   uint32_t maxk = 0;
   bool ok = v.ok, short_key = false;
@@ -278,13 +324,17 @@ __device__ void block_count_one(const JobDev& J, uint64_t b, uint32_t lane) {
   }
 }
 
-__global__ void k_block_count(JobDev J) {
-  const uint32_t lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kDecWarps * 32) k_block_count(JobDev J) {
+  extern __shared__ __align__(16) uint8_t dec_smem[];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
   const uint64_t nblk = J.ctr->n_blocks_in;
-  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk;
-       b += stride)
-    block_count_one(J, b, lane);
+  for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
+       b += (uint64_t)gridDim.x * kDecWarps) {
+    const uint8_t* st = stage_block(J, b, W.stage, lane);
+    block_count_one(J, b, lane, st ? st : J.in + J.blk_off[b]);
+    __syncwarp();
+  }
 }
 
 __global__ void k_run_bounds(JobDev J) {
@@ -304,12 +354,10 @@ __global__ void k_run_bounds(JobDev J) {
   }
 }
 
-__global__ void k_block_decode(JobDev J) {
-  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31;
-  if (b >= J.ctr->n_blocks_in) return;
-  if (J.ctr->error) return;
-  BlockView v = block_view(J, b);
+// Decode of one block straight from global memory, one lane per restart run:
+// the path for blocks that do not fit the shared-memory stage.
+__device__ void decode_direct(const JobDev& J, uint64_t b, uint32_t lane) {
+  BlockView v = block_view(J, b, J.in + J.blk_off[b]);
   uint64_t ent_carry = J.blk_ent_base[b];
   uint64_t key_carry = J.blk_key_base[b];
   for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
@@ -356,6 +404,132 @@ __global__ void k_block_decode(JobDev J) {
   }
 }
 
+// Decode of one staged block.  Lanes first walk the restart runs (one lane
+// per run, headers only) and record every entry's key-delta position, shared
+// prefix and lengths; then, 32 entries at a time, each lane rebuilds one key
+// in shared memory: the delta from its own entry, and the shared prefix from
+// the deltas of earlier entries of the same run (walking back until the
+// prefix is covered -- a restart entry has no shared prefix).  Keys leave in
+// 16-byte stores; descriptors are written one lane per entry.
+__device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const uint8_t* st,
+                              DecWarpSmem& W) {
+  BlockView v = block_view(J, b, st);
+  const uint32_t nent = J.blk_nent[b];
+  if (nent > kDecMaxEnt) return false;
+  // pass 1: headers of every entry, one lane per restart run
+  uint32_t carry = 0;
+  bool long_key = false;
+  for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    uint64_t s = 0, e = 0;
+    uint32_t cnt = 0;
+    if (r < v.nr) run_bounds(v, r, &s, &e, &cnt);
+    uint32_t tot;
+    const uint32_t e0 = warp_excl<uint32_t>(cnt, &tot) + carry;
+    carry += tot;
+    if (r < v.nr) {
+      const uint8_t* p = st + s;
+      const uint8_t* lim = st + e;
+      for (uint32_t k = 0; k < cnt; k++) {
+        uint32_t sh, ns, vl;
+        const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
+        if (!q) break;
+        const uint32_t idx = e0 + k;
+        if (idx < kDecMaxEnt) {
+          W.dpos[idx] = (uint16_t)(q - st);
+          W.sh[idx] = (uint16_t)sh;
+          W.kl[idx] = (uint16_t)(sh + ns);
+          W.vl[idx] = (uint16_t)vl;
+        }
+        if (sh + ns > 0xffff) long_key = true;
+        p = q + ns + vl;
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, long_key)) return false;
+  __syncwarp();
+  // pass 2: keys and descriptors, 32 entries at a time
+  const uint64_t ebase = J.blk_ent_base[b];
+  uint64_t kbase = J.blk_key_base[b];
+  const uint32_t voff0 = (uint32_t)J.blk_off[b];  // block offset in `in`
+  for (uint32_t g0 = 0; g0 < nent; g0 += 32) {
+    const uint32_t i = g0 + lane;
+    const bool valid = i < nent;
+    const uint32_t kl = valid ? W.kl[i] : 0;
+    uint32_t gk;
+    const uint32_t kofs = warp_excl<uint32_t>(kl, &gk);
+    uint8_t* gdst = J.keys + kbase;
+    const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
+    if (gk + kph + 16 > kDecKeyBuf) {
+      // keys of this group do not fit the buffer: write them directly
+      if (valid) {
+        uint8_t* d = gdst + kofs;
+        uint32_t m = W.sh[i];
+        for (uint32_t t = m; t < kl; t++) d[t] = st[W.dpos[i] + (t - m)];
+        for (int32_t j = (int32_t)i - 1; m > 0 && j >= 0; j--) {
+          const uint32_t lo = W.sh[j];
+          if (lo < m) {
+            for (uint32_t t = lo; t < m; t++) d[t] = st[W.dpos[j] + (t - lo)];
+            m = lo;
+          }
+        }
+      }
+    } else {
+      uint8_t* kb = W.keybuf + kph;
+      if (valid) {
+        uint8_t* d = kb + kofs;
+        uint32_t m = W.sh[i];
+        for (uint32_t t = m; t < kl; t++) d[t] = st[W.dpos[i] + (t - m)];
+        for (int32_t j = (int32_t)i - 1; m > 0 && j >= 0; j--) {
+          const uint32_t lo = W.sh[j];
+          if (lo < m) {
+            for (uint32_t t = lo; t < m; t++) d[t] = st[W.dpos[j] + (t - lo)];
+            m = lo;
+          }
+        }
+      }
+      __syncwarp();
+      // keys out: head bytes, 16-byte body, tail
+      const uint32_t head = (16 - kph) & 15;
+      const uint32_t h = head < gk ? head : gk;
+      if (lane < h) gdst[lane] = kb[lane];
+      const uint32_t body = (gk - h) & ~15u;
+      const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
+      uint4* dv = reinterpret_cast<uint4*>(gdst + h);
+      for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
+      const uint32_t t0 = h + body;
+      if (t0 + lane < gk) gdst[t0 + lane] = kb[t0 + lane];
+    }
+    if (valid) {
+      const uint64_t e = ebase + i;
+      const uint32_t ko = (uint32_t)(kbase + kofs);
+      J.e_koff[e] = ko;
+      J.e_klen[e] = kl;
+      J.e_voff[e] = voff0 + W.dpos[i] + (kl - W.sh[i]);
+      J.e_vlen[e] = W.vl[i];
+      const uint8_t* kp = (gk + kph + 16 > kDecKeyBuf) ? J.keys + ko : W.keybuf + kph + kofs;
+      J.e_pfx[e] = user_prefix(kp, kl);
+    }
+    kbase += gk;
+    __syncwarp();
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(JobDev J) {
+  extern __shared__ __align__(16) uint8_t dec_smem[];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
+  if (J.ctr->error) return;
+  const uint64_t nblk = J.ctr->n_blocks_in;
+  for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
+       b += (uint64_t)gridDim.x * kDecWarps) {
+    const uint8_t* st = stage_block(J, b, W.stage, lane);
+    if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
+    __syncwarp();
+  }
+}
+
 __global__ void k_entries_from_offsets(JobDev J, const uint64_t* koffs, const uint64_t* voffs,
                                        uint64_t n) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -381,16 +555,32 @@ void launch_table_index_count(const JobDev& J, cudaStream_t st) {
 void launch_table_index_entries(const JobDev& J, cudaStream_t st) {
   note_launch(), k_table_index_entries<<<J.n_tables, 128, 0, st>>>(J);
 }
+static void dec_smem_attr(const void* fn) {
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(kDecWarps * sizeof(DecWarpSmem)));
+}
+
 void launch_block_count(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
-  // grid-stride over the device-side block count: at most 148 SMs x 16 CTAs
-  uint64_t ctas = (std::max<uint64_t>(n_blocks_cap, 1) * 32 + 255) / 256;
-  ctas = std::min<uint64_t>(ctas, 148 * 16);
-  note_launch(), k_block_count<<<(unsigned)ctas, 256, 0, st>>>(J);
+  static bool attr = false;
+  if (!attr) {
+    dec_smem_attr((const void*)k_block_count);
+    attr = true;
+  }
+  // grid-stride over the device-side block count: 3 CTAs per SM x 8 waves
+  const uint64_t ctas =
+      std::min<uint64_t>((std::max<uint64_t>(n_blocks_cap, 1) + kDecWarps - 1) / kDecWarps, 148 * 3 * 8);
+  note_launch(), k_block_count<<<(unsigned)ctas, kDecWarps * 32, kDecWarps * sizeof(DecWarpSmem), st>>>(J);
 }
 void launch_run_bounds(const JobDev& J, cudaStream_t st) { note_launch(), k_run_bounds<<<1, 32, 0, st>>>(J); }
 void launch_block_decode(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
-  uint64_t warps = n_blocks_cap ? n_blocks_cap : 1;
-  note_launch(), k_block_decode<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(J);
+  static bool attr = false;
+  if (!attr) {
+    dec_smem_attr((const void*)k_block_decode);
+    attr = true;
+  }
+  const uint64_t ctas =
+      std::min<uint64_t>((std::max<uint64_t>(n_blocks_cap, 1) + kDecWarps - 1) / kDecWarps, 148 * 3 * 8);
+  note_launch(), k_block_decode<<<(unsigned)ctas, kDecWarps * 32, kDecWarps * sizeof(DecWarpSmem), st>>>(J);
 }
 void launch_entries_from_offsets(const JobDev& J, const uint64_t* koffs, const uint64_t* voffs,
                                  uint64_t n, cudaStream_t st) {

@@ -241,3 +241,76 @@ __device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t d
 }
 
 }  // namespace lc
+
+namespace lc {
+
+// ---------------------------------------------------------------------------
+// Asynchronous 16-byte global -> shared copies (cp.async, LDGSTS): many in
+// flight per warp without holding registers; completion by wait_all.
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Slicing-by-4 CRC32C tables in shared memory: tab4[k][x] is the register
+// update for byte x followed by k zero bytes (tab4[0] is the byte table).
+__device__ __forceinline__ void crc_tables4_init(uint32_t* tab4) {
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = i;
+#pragma unroll
+    for (int k = 0; k < 8; k++) c = (c & 1) ? (c >> 1) ^ kCrcPoly : (c >> 1);
+    tab4[i] = c;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+    uint32_t c = tab4[i];
+    for (int k = 1; k < 4; k++) {
+      c = (c >> 8) ^ tab4[c & 0xff];
+      tab4[256 * k + i] = c;
+    }
+  }
+}
+
+// Raw CRC register update over [p, p+n) in shared memory, four bytes per
+// step once p is word aligned.
+__device__ __forceinline__ uint32_t crc_raw4(const uint32_t* tab4, uint32_t c, const uint8_t* p,
+                                             uint32_t n) {
+  uint32_t i = 0;
+  while (i < n && (reinterpret_cast<uintptr_t>(p + i) & 3)) {
+    c = tab4[(c ^ p[i]) & 0xff] ^ (c >> 8);
+    i++;
+  }
+  for (; i + 4 <= n; i += 4) {
+    c ^= *reinterpret_cast<const uint32_t*>(p + i);
+    c = tab4[768 + (c & 0xff)] ^ tab4[512 + ((c >> 8) & 0xff)] ^ tab4[256 + ((c >> 16) & 0xff)] ^
+        tab4[c >> 24];
+  }
+  for (; i < n; i++) c = tab4[(c ^ p[i]) & 0xff] ^ (c >> 8);
+  return c;
+}
+
+// Masked block trailer CRC of n bytes in shared memory plus the zero type
+// byte, which the caller has stored at p[n].  One warp; each lane takes a
+// contiguous stretch whose length in words is odd (distinct banks).
+__device__ __forceinline__ uint32_t warp_block_crc_smem(const JobDev& J, const uint32_t* tab4,
+                                                        const uint8_t* p, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t total = n + 1;
+  uint32_t m = (total + 127) / 128;
+  m |= 1;
+  const uint32_t seg = 4 * m;
+  const uint32_t b0 = lane * seg;
+  const uint32_t e0 = min(total, b0 + seg);
+  const uint32_t c = b0 < e0 ? crc_raw4(tab4, 0, p + b0, e0 - b0) : 0;
+  uint32_t v = b0 < total ? crc_shift(J, c, total - e0) : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  const uint32_t full = v ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+  return ((full >> 15) | (full << 17)) + 0xa282ead8u;
+}
+
+}  // namespace lc

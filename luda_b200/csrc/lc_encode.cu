@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "lc_device.cuh"
 #include "lc_kernels.h"
 
@@ -150,13 +152,14 @@ __global__ void k_chain_tables(JobDev J) {
 }
 
 __global__ void k_chain_resolve(JobDev J) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  extern __shared__ uint32_t s_tab[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
   const uint32_t W = J.ctr->max_jump;
   if (n == 0) return;
   if (W > C) {
     // blocks longer than a chunk: walk the whole chain
+    if (threadIdx.x != 0) return;
     uint64_t e = 0;
     while (e < n) {
       J.k_bstart[e] = 1;
@@ -165,11 +168,19 @@ __global__ void k_chain_resolve(JobDev J) {
     return;
   }
   const uint64_t M = (n + C - 1) / C;
+  // the per-chunk tables fit in shared memory for most jobs: stage them
+  const bool staged = M * W <= J.chain_smem_words;
+  if (staged) {
+    for (uint64_t i = threadIdx.x; i < M * W; i += blockDim.x)
+      s_tab[i] = J.chunk_table[(i / W) * C + (i % W)];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   uint64_t e = 0;
   for (uint64_t c = 0; c < M; c++) {
     J.chunk_entry[c] = (uint32_t)e;
     const uint64_t c0 = c * C;
-    if (e < n) e = J.chunk_table[c * C + (e - c0)];
+    if (e < n) e = staged ? s_tab[c * W + (e - c0)] : J.chunk_table[c * C + (e - c0)];
   }
 }
 
@@ -213,57 +224,70 @@ __global__ void k_block_sizes(JobDev J, uint32_t* tmp32) {
 }
 
 // Output files: size cuts at block ends, grandparent cuts at forced blocks.
-__global__ void k_files(JobDev J) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Like the block chain, a file's end depends on where it starts: every block
+// b gets b_fnext[b], the first block of the next file if a file began at b (a
+// binary search for the size cut, and the next forced block); one thread then
+// walks the few file starts.
+
+// t_blocks[i] = output block that starts at grandparent cut i (ascending).
+__global__ void k_forced_blocks(JobDev J) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= J.ctr->n_triggers) return;
+  const uint64_t kp = J.kept_pos[J.triggers[i]];
+  J.t_blocks[i] = kp < J.ctr->n_kept ? J.k_block[kp] : (uint32_t)J.ctr->n_blocks_out;
+}
+
+__global__ void k_file_next(JobDev J) {
   const uint64_t nb = J.ctr->n_blocks_out;
-  const uint64_t nk = J.ctr->n_kept;
   const uint32_t nt = J.ctr->n_triggers;
-  uint32_t f = 0, tp = 0;
-  uint64_t b = 0;
-  while (b < nb) {
-    const uint64_t start = b;
-    uint64_t next_forced = nb;
-    while (tp < nt) {
-      const uint32_t kp = J.kept_pos[J.triggers[tp]];
-      if (kp >= nk) {
-        tp = nt;
-        break;
-      }
-      const uint64_t fb = J.k_block[kp];
-      if (fb <= start) {
-        tp++;
-        continue;
-      }
-      next_forced = fb;
-      break;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (uint64_t)gridDim.x * blockDim.x) {
+    // first forced block after b
+    uint32_t lo = 0, hi = nt;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (J.t_blocks[mid] <= b) lo = mid + 1;
+      else hi = mid;
     }
-    const uint64_t cum0 = J.b_cum[start];
+    const uint64_t next_forced = lo < nt ? J.t_blocks[lo] : nb;
+    // first block end where the file's flushed bytes reach max_file_size
+    const uint64_t cum0 = J.b_cum[b];
     const uint64_t target =
         J.max_file_size > ~0ull - cum0 ? ~0ull : cum0 + J.max_file_size;  // saturating
     uint64_t sc;
     if (J.b_cum[nb] < target) {
       sc = nb - 1;
     } else {
-      uint64_t lo = start, hi = nb - 1;
-      while (lo < hi) {
-        uint64_t mid = (lo + hi) >> 1;
-        if (J.b_cum[mid + 1] >= target) hi = mid;
-        else lo = mid + 1;
+      uint64_t l = b, h = nb - 1;
+      while (l < h) {
+        const uint64_t mid = (l + h) >> 1;
+        if (J.b_cum[mid + 1] >= target) h = mid;
+        else l = mid + 1;
       }
-      sc = lo;
+      sc = l;
     }
-    const uint64_t end = min(sc, next_forced - 1);
+    J.b_fnext[b] = (uint32_t)(min(sc, next_forced - 1) + 1);
+  }
+}
+
+__global__ void k_files(JobDev J) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint64_t nb = J.ctr->n_blocks_out;
+  uint32_t f = 0;
+  uint64_t b = 0;
+  while (b < nb) {
+    const uint64_t end = J.b_fnext[b];
     if (f >= J.cap_files) {
       set_error(J.ctr, kErrLimit, 2);
       break;
     }
     FileOut& F = J.files[f];
-    F.first_block = (uint32_t)start;
-    F.end_block = (uint32_t)(end + 1);
-    F.first_kept = J.b_first[start];
-    F.end_kept = J.b_first[end + 1];
+    F.first_block = (uint32_t)b;
+    F.end_block = (uint32_t)end;
+    F.first_kept = J.b_first[b];
+    F.end_kept = J.b_first[end];
     f++;
-    b = end + 1;
+    b = end;
   }
   J.ctr->n_files = f;
 }
@@ -374,19 +398,21 @@ __global__ void k_file_layout(JobDev J) {
       o += J.files[f].size;
     }
     J.ctr->bytes_out = o;
+    if (o > J.cap_out) set_error(J.ctr, kErrLimit, 3);
   }
 }
 
-// One warp per output data block.
-__global__ void k_encode_blocks(JobDev J) {
-  __shared__ uint32_t tab[256];
-  crc_table_init(tab);
-  __syncthreads();
-  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31;
-  if (b >= J.ctr->n_blocks_out) return;
-  const FileOut& F = J.files[J.b_file[b]];
-  uint8_t* dst = J.out + F.out_off + J.b_off[b];
+// One warp per output data block.  The block is assembled in this warp's
+// shared-memory stage at the same 16-byte phase as its destination, entries are
+// copied by four 8-lane groups with 16-byte loads, the CRC32C trailer is
+// computed from shared memory, and the block leaves with 16-byte stores.
+// Blocks larger than the stage are written straight to global memory.
+constexpr uint32_t kEncWarps = 4;
+constexpr uint32_t kEncStage = 8448;    // bytes per warp: 8 KiB blocks + phase + trailer
+constexpr uint32_t kEncScratch = 8192;  // bytes per warp: gathered 16-byte source chunks
+
+__device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab, uint64_t b,
+                                           uint8_t* dst, uint32_t lane) {
   const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
   const uint32_t R = J.restart_interval;
   const uint32_t bsz = J.b_size[b];
@@ -423,18 +449,194 @@ __global__ void k_encode_blocks(JobDev J) {
   }
   if (lane == 0) {
     st_le32(dst + bsz - 4, (uint32_t)nrest);
-    dst[bsz] = 0;  // kNoCompression
+    dst[bsz] = 0;
   }
   __syncwarp();
   const uint32_t crc = warp_block_crc(J, tab, dst, bsz);
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
+// Copies len bytes from global src to shared dst with the 8 lanes of one
+// group: 16-byte loads of the aligned chunks that cover src, bytes scattered
+// into place.  Chunks that would read past `limit` fall back to byte loads.
+__device__ __forceinline__ void group_copy(const uint8_t* src, uint32_t len, uint8_t* dst,
+                                           uint32_t sub, const uint8_t* limit) {
+  if (len == 0) return;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t base = a & ~uintptr_t(15);
+  const uint32_t lead = (uint32_t)(a - base);
+  const uint32_t nch = (lead + len + 15) >> 4;
+  for (uint32_t c = sub; c < nch; c += 8) {
+    const uint8_t* q = reinterpret_cast<const uint8_t*>(base + 16ull * c);
+    uint4 v;
+    if (q + 16 <= limit) {
+      v = *reinterpret_cast<const uint4*>(q);
+    } else {
+      uint32_t w[4] = {0, 0, 0, 0};
+      for (int i = 0; i < 16; i++)
+        if (q + i < limit) w[i >> 2] |= (uint32_t)q[i] << (8 * (i & 3));
+      v = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    const uint32_t o = 16 * c - lead;  // offset of chunk byte 0 in dst (may wrap)
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const uint32_t word = i < 4 ? v.x : (i < 8 ? v.y : (i < 12 ? v.z : v.w));
+      const uint32_t off = o + i;
+      if (off < len) dst[off] = (uint8_t)(word >> (8 * (i & 3)));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(JobDev J) {
+  extern __shared__ __align__(16) uint8_t enc_smem[];
+  uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
+  uint8_t* stages = enc_smem + 4096;
+  crc_tables4_init(tab4);
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t sub = lane & 7, grp = lane >> 3;
+  if (J.ctr->error) return;
+  const uint64_t nb = J.ctr->n_blocks_out;
+  const uint32_t R = J.restart_interval;
+  const uint8_t* in_limit = J.in_end;
+  const uint8_t* key_limit = J.keys + J.cap_key_bytes + 16;
+  uint8_t* stage = stages + warp * (kEncStage + kEncScratch);
+  uint8_t* scratch = stage + kEncStage;
+  for (uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp; b < nb;
+       b += (uint64_t)gridDim.x * kEncWarps) {
+    const FileOut& F = J.files[J.b_file[b]];
+    uint8_t* dst = J.out + F.out_off + J.b_off[b];
+    const uint32_t bsz = J.b_size[b];
+    const uint32_t phase = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+    if (bsz + kTrailer + phase > kEncStage) {
+      enc_direct(J, tab4, b, dst, lane);
+      continue;
+    }
+    uint8_t* st = stage + phase;
+    const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
+    const uint64_t nrest = (n + R - 1) / R;
+    const uint32_t rbase = bsz - 4 * (uint32_t)nrest - 4;
+    uint32_t carry = 0;
+    for (uint64_t j0 = 0; j0 < n; j0 += 32) {
+      const uint64_t j = j0 + lane;
+      const bool valid = j < n;
+      const bool restart = (j % R) == 0;
+      uint32_t size = 0, ksrc = 0, klen = 0, vsrc = 0, vlen = 0, hl = 0, sh = 0;
+      if (valid) {
+        const uint64_t k = s + j;
+        const uint32_t id = J.k_ids[k];
+        const uint32_t kl = J.e_klen[id];
+        vlen = J.e_vlen[id];
+        vsrc = J.e_voff[id];
+        sh = restart ? 0 : J.k_shared[k];
+        ksrc = J.e_koff[id] + sh;
+        klen = kl - sh;
+        size = restart ? J.k_a[k] : J.k_b[k];
+        hl = varint_len(sh) + varint_len(klen) + varint_len(vlen);
+      }
+      uint32_t tot;
+      const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
+      carry += tot;
+      if (valid) {
+        uint8_t* p = st + ex;
+        p = put_varint(p, sh);
+        p = put_varint(p, klen);
+        put_varint(p, vlen);
+        if (restart) {
+          const uint64_t rem = n - j;
+          const uint32_t cnt = (uint32_t)(rem < R ? rem : R);
+          st_le32(st + rbase + 4 * (uint32_t)(j / R), (ex << 8) | cnt);
+        }
+      }
+      const uint32_t cnt_here = (uint32_t)((n - j0) < 32 ? (n - j0) : 32);
+      // 16-byte chunks that cover this entry's key delta and value
+      const uintptr_t ka = reinterpret_cast<uintptr_t>(J.keys + ksrc) & ~uintptr_t(15);
+      const uint32_t klead = (uint32_t)(reinterpret_cast<uintptr_t>(J.keys + ksrc) - ka);
+      const uint32_t nk = klen ? (klead + klen + 15) >> 4 : 0;
+      const uintptr_t va = reinterpret_cast<uintptr_t>(J.in + vsrc) & ~uintptr_t(15);
+      const uint32_t vlead = (uint32_t)(reinterpret_cast<uintptr_t>(J.in + vsrc) - va);
+      const uint32_t nv = vlen ? (vlead + vlen + 15) >> 4 : 0;
+      uint32_t gchunks;
+      const uint32_t sc = warp_excl<uint32_t>(nk + nv, &gchunks);
+      if (gchunks * 16 <= kEncScratch) {
+        // gather every chunk of the group with asynchronous copies, wait once
+        for (uint32_t e = 0; e < cnt_here; e++) {
+          const uint32_t e_nk = __shfl_sync(0xffffffffu, nk, e);
+          const uint32_t e_n = e_nk + __shfl_sync(0xffffffffu, nv, e);
+          const uint32_t e_sc = __shfl_sync(0xffffffffu, sc, e);
+          const uintptr_t e_ka = __shfl_sync(0xffffffffu, (unsigned long long)ka, e);
+          const uintptr_t e_va = __shfl_sync(0xffffffffu, (unsigned long long)va, e);
+          for (uint32_t c = lane; c < e_n; c += 32) {
+            const uint8_t* src = reinterpret_cast<const uint8_t*>(
+                c < e_nk ? e_ka + 16ull * c : e_va + 16ull * (c - e_nk));
+            uint8_t* d = scratch + 16 * (e_sc + c);
+            const uint8_t* lim = c < e_nk ? key_limit : in_limit;
+            if (src + 16 <= lim) {
+              cp_async16(d, src);
+            } else {
+              for (int i = 0; i < 16; i++) d[i] = src + i < lim ? src[i] : 0;
+            }
+          }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        // shift the gathered bytes into place in the stage
+        for (uint32_t e = 0; e < cnt_here; e++) {
+          const uint32_t e_ex = __shfl_sync(0xffffffffu, ex + hl, e);
+          const uint32_t e_kl = __shfl_sync(0xffffffffu, klen, e);
+          const uint32_t e_vl = __shfl_sync(0xffffffffu, vlen, e);
+          const uint32_t e_ks = __shfl_sync(0xffffffffu, 16 * sc + klead, e);
+          const uint32_t e_vs = __shfl_sync(0xffffffffu, 16 * (sc + nk) + vlead, e);
+          for (uint32_t t = lane; t < e_kl; t += 32) st[e_ex + t] = scratch[e_ks + t];
+          for (uint32_t t = lane; t < e_vl; t += 32) st[e_ex + e_kl + t] = scratch[e_vs + t];
+        }
+        __syncwarp();
+      } else {
+        // large values: four entries at a time, one per 8-lane group
+        for (uint32_t e0 = 0; e0 < cnt_here; e0 += 4) {
+          const uint32_t q = e0 + grp;
+          const uint32_t q_ex = __shfl_sync(0xffffffffu, ex, q & 31);
+          const uint32_t q_hl = __shfl_sync(0xffffffffu, hl, q & 31);
+          const uint32_t q_ks = __shfl_sync(0xffffffffu, ksrc, q & 31);
+          const uint32_t q_kl = __shfl_sync(0xffffffffu, klen, q & 31);
+          const uint32_t q_vs = __shfl_sync(0xffffffffu, vsrc, q & 31);
+          const uint32_t q_vl = __shfl_sync(0xffffffffu, vlen, q & 31);
+          if (q < cnt_here) {
+            uint8_t* d = st + q_ex + q_hl;
+            group_copy(J.keys + q_ks, q_kl, d, sub, key_limit);
+            group_copy(J.in + q_vs, q_vl, d + q_kl, sub, in_limit);
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      st_le32(st + bsz - 4, (uint32_t)nrest);
+      st[bsz] = 0;  // kNoCompression
+    }
+    __syncwarp();
+    const uint32_t crc = warp_block_crc_smem(J, tab4, st, bsz);
+    if (lane == 0) st_le32(st + bsz + 1, crc);
+    __syncwarp();
+    // write out [0, bsz + 5): bytes up to the first 16-byte boundary, 16-byte
+    // stores, then the tail
+    {
+      const uint32_t total = bsz + kTrailer;
+      const uint32_t head = (16 - phase) & 15;
+      const uint32_t h = head < total ? head : total;
+      if (lane < h) dst[lane] = st[lane];
+      const uint32_t body = (total - h) & ~15u;
+      const uint4* srcv = reinterpret_cast<const uint4*>(st + h);
+      uint4* dstv = reinterpret_cast<uint4*>(dst + h);
+      for (uint32_t c = lane; c < body / 16; c += 32) dstv[c] = srcv[c];
+      const uint32_t t0 = h + body;
+      if (t0 + lane < total) dst[t0 + lane] = st[t0 + lane];
+    }
+    __syncwarp();
+  }
+}
+
 // One warp per filter group (at the group's first block).
-__global__ void k_encode_filters(JobDev J) {
-  const uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t lane = threadIdx.x & 31;
-  if (b >= J.ctr->n_blocks_out || J.bits_per_key <= 0) return;
+__device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b, uint32_t lane) {
   const FileOut& F = J.files[J.b_file[b]];
   const uint32_t fb0 = F.first_block, fb1 = F.end_block;
   uint8_t* fbase = J.out + F.out_off + F.filter_off;
@@ -473,9 +675,16 @@ __global__ void k_encode_filters(JobDev J) {
   }
 }
 
-__global__ void k_encode_index(JobDev J) {
-  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= J.ctr->n_blocks_out) return;
+__global__ void k_encode_filters(JobDev J) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (J.bits_per_key <= 0 || J.ctr->error) return;
+  const uint64_t nb = J.ctr->n_blocks_out;
+  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride)
+    encode_filter_group(J, b, lane);
+}
+
+__device__ __forceinline__ void encode_index_entry(const JobDev& J, uint64_t b) {
   const FileOut& F = J.files[J.b_file[b]];
   const uint32_t fb0 = F.first_block, fb1 = F.end_block;
   uint8_t* ib = J.out + F.out_off + F.index_off;
@@ -505,9 +714,17 @@ __global__ void k_encode_index(JobDev J) {
   if (b + 1 == fb1) st_le32(ra + 4, fb1 - fb0);
 }
 
+__global__ void k_encode_index(JobDev J) {
+  if (J.ctr->error) return;
+  const uint64_t nb = J.ctr->n_blocks_out;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (uint64_t)gridDim.x * blockDim.x)
+    encode_index_entry(J, b);
+}
+
 __global__ void k_encode_meta(JobDev J) {
   const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= J.ctr->n_files) return;
+  if (f >= J.ctr->n_files || J.ctr->error) return;
   const FileOut& F = J.files[f];
   uint8_t* base = J.out + F.out_off;
   if (J.bits_per_key > 0) {
@@ -550,7 +767,7 @@ __global__ void k_crc_regions(JobDev J) {
   crc_table_init(tab);
   __syncthreads();
   const uint32_t f = blockIdx.x / 3, which = blockIdx.x % 3;
-  if (f >= J.ctr->n_files) return;
+  if (f >= J.ctr->n_files || J.ctr->error) return;
   if (which == 0 && J.bits_per_key <= 0) return;
   const FileOut& F = J.files[f];
   const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
@@ -579,24 +796,46 @@ __global__ void k_crc_regions(JobDev J) {
   }
 }
 
-__global__ void k_file_key_lens(JobDev J, uint32_t* lens) {
-  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= J.ctr->n_files) return;
-  uint32_t l0, l1;
-  kept_key(J, J.files[f].first_kept, &l0);
-  kept_key(J, J.files[f].end_kept - 1, &l1);
-  lens[2 * f] = l0;
-  lens[2 * f + 1] = l1;
-}
-
-__global__ void k_file_keys(JobDev J, uint8_t* out, const uint64_t* off) {
-  const uint32_t f = blockIdx.x;
-  if (f >= J.ctr->n_files) return;
-  for (int w = 0; w < 2; w++) {
+// Smallest / largest internal key of every output file, packed: one CTA;
+// koff[2f], koff[2f+1] start file f's smallest and largest key.
+__global__ void k_file_keys(JobDev J, uint8_t* out, uint64_t* koff) {
+  __shared__ uint64_t s_warp[32];
+  __shared__ uint64_t s_carry;
+  const uint32_t nf = J.ctr->error ? 0 : J.ctr->n_files;
+  const uint32_t nk = 2 * nf;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  // lengths -> offsets (block-wide scan in chunks of blockDim)
+  for (uint32_t base = 0; base < nk; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    uint64_t l = 0;
+    if (i < nk) {
+      uint32_t kl;
+      kept_key(J, (i & 1) ? J.files[i >> 1].end_kept - 1 : J.files[i >> 1].first_kept, &kl);
+      l = kl;
+    }
+    uint64_t tot;
+    uint64_t ex = warp_excl<uint64_t>(l, &tot);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = tot;
+    __syncthreads();
+    uint64_t before = s_carry, all = 0;
+    for (uint32_t w = 0; w < blockDim.x / 32; w++) {
+      if (w < (threadIdx.x >> 5)) before += s_warp[w];
+      all += s_warp[w];
+    }
+    if (i < nk) koff[i] = before + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += all;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) koff[nk] = s_carry;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x >> 5; i < nk; i += blockDim.x >> 5) {
+    const uint32_t f = i >> 1;
     uint32_t l;
-    const uint8_t* k = kept_key(J, w == 0 ? J.files[f].first_kept : J.files[f].end_kept - 1, &l);
-    uint8_t* d = out + off[2 * f + w];
-    for (uint32_t i = threadIdx.x; i < l; i += blockDim.x) d[i] = k[i];
+    const uint8_t* k = kept_key(J, (i & 1) ? J.files[f].end_kept - 1 : J.files[f].first_kept, &l);
+    uint8_t* d = out + koff[i];
+    for (uint32_t t = threadIdx.x & 31; t < l; t += 32) d[t] = k[t];
   }
 }
 
@@ -614,7 +853,7 @@ void launch_chain(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
   const uint64_t chunks = (n_cap + J.chunk - 1) / J.chunk + 1;
   const size_t smem = (size_t)J.chunk * sizeof(uint32_t);
   note_launch(), k_chain_tables<<<(unsigned)chunks, 256, smem, st>>>(J);
-  note_launch(), k_chain_resolve<<<1, 32, 0, st>>>(J);
+  note_launch(), k_chain_resolve<<<1, 256, (size_t)J.chain_smem_words * 4, st>>>(J);
   note_launch(), k_chain_mark<<<(unsigned)chunks, 128, smem, st>>>(J);
 }
 void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
@@ -623,27 +862,38 @@ void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
 void launch_block_sizes(const JobDev& J, uint32_t* tmp32, uint64_t nb_cap, cudaStream_t st) {
   note_launch(), k_block_sizes<<<grid_for(nb_cap, 256), 256, 0, st>>>(J, tmp32);
 }
-void launch_files(const JobDev& J, cudaStream_t st) { note_launch(), k_files<<<1, 32, 0, st>>>(J); }
+void launch_files(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
+  note_launch(), k_forced_blocks<<<(J.cap_triggers + 255) / 256, 256, 0, st>>>(J);
+  note_launch(), k_file_next<<<(unsigned)std::min<uint64_t>(grid_for(nb_cap, 256), 148 * 16), 256, 0, st>>>(J);
+  note_launch(), k_files<<<1, 32, 0, st>>>(J);
+}
 void launch_block_layout(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
   note_launch(), k_block_layout<<<grid_for(nb_cap, 256), 256, 0, st>>>(J);
 }
 void launch_file_layout(const JobDev& J, cudaStream_t st) { note_launch(), k_file_layout<<<1, 256, 0, st>>>(J); }
-void launch_encode_blocks(const JobDev& J, uint64_t nb, cudaStream_t st) {
-  if (nb) note_launch(), k_encode_blocks<<<grid_for(nb * 32, 256), 256, 0, st>>>(J);
+void launch_encode_blocks(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
+  if (!nb_cap) return;
+  const size_t smem = 4096 + (size_t)kEncWarps * (kEncStage + kEncScratch);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  // grid-stride over the device-side block count: up to 3 CTAs per SM x 8 waves
+  const uint64_t ctas = std::min<uint64_t>((nb_cap + kEncWarps - 1) / kEncWarps, 148 * 3 * 8);
+  note_launch(), k_encode_blocks<<<(unsigned)ctas, kEncWarps * 32, smem, st>>>(J);
 }
-void launch_encode_rest(const JobDev& J, uint64_t nb_cap, uint32_t n_files, cudaStream_t st) {
+void launch_encode_rest(const JobDev& J, uint64_t nb_cap, uint32_t cap_files, cudaStream_t st) {
   if (nb_cap == 0) return;
-  note_launch(), k_encode_filters<<<grid_for(nb_cap * 32, 256), 256, 0, st>>>(J);
-  note_launch(), k_encode_index<<<grid_for(nb_cap, 256), 256, 0, st>>>(J);
-  note_launch(), k_encode_meta<<<grid_for(n_files, 128), 128, 0, st>>>(J);
-  if (n_files) note_launch(), k_crc_regions<<<n_files * 3, 256, 0, st>>>(J);
+  const uint64_t wctas = std::min<uint64_t>((nb_cap * 32 + 255) / 256, 148 * 16);
+  note_launch(), k_encode_filters<<<(unsigned)wctas, 256, 0, st>>>(J);
+  note_launch(), k_encode_index<<<(unsigned)std::min<uint64_t>(grid_for(nb_cap, 256), 148 * 16), 256, 0, st>>>(J);
+  note_launch(), k_encode_meta<<<grid_for(cap_files, 128), 128, 0, st>>>(J);
+  note_launch(), k_crc_regions<<<cap_files * 3, 256, 0, st>>>(J);
 }
-void launch_file_key_lens(const JobDev& J, uint32_t n_files, uint32_t* lens, cudaStream_t st) {
-  note_launch(), k_file_key_lens<<<grid_for(n_files, 128), 128, 0, st>>>(J, lens);
-}
-void launch_file_keys(const JobDev& J, uint32_t n_files, uint8_t* key_out, const uint64_t* key_off,
+void launch_file_keys(const JobDev& J, uint32_t cap_files, uint8_t* key_out, uint64_t* key_off,
                       cudaStream_t st) {
-  if (n_files) note_launch(), k_file_keys<<<n_files, 64, 0, st>>>(J, key_out, key_off);
+  note_launch(), k_file_keys<<<1, 256, 0, st>>>(J, key_out, key_off);
 }
 
 }  // namespace lc

@@ -174,23 +174,47 @@ struct lc_job {
 
 namespace {
 
-// Device allocations of one job, freed in stream order at the end.
+// Device allocations of one job: a bump allocator over a few large chunks of
+// the stream-ordered pool (one cudaMallocAsync per 64 MiB instead of one per
+// array), all freed in stream order at the end.  Sub-allocations are
+// 256-byte aligned and padded so that 16-byte vector loads may run past the
+// end of an array.
 struct DevAlloc {
+  static constexpr uint64_t kChunkBytes = 64ull << 20;
   cudaStream_t st;
   std::vector<void*> ptrs;
+  uint8_t* cur = nullptr;
+  uint64_t left = 0;
   explicit DevAlloc(cudaStream_t s) : st(s) {}
   template <typename T>
   T* get(uint64_t n) {
+    const uint64_t bytes = (std::max<uint64_t>(n, 1) * sizeof(T) + 16 + 255) & ~uint64_t(255);
+    if (bytes > left) {
+      const uint64_t c = std::max(bytes, kChunkBytes);
+      void* p = nullptr;
+      CK(cudaMallocAsync(&p, c, st));
+      ptrs.push_back(p);
+      cur = (uint8_t*)p;
+      left = c;
+    }
+    T* r = (T*)cur;
+    cur += bytes;
+    left -= bytes;
+    return r;
+  }
+  // a separate allocation (e.g. an output that outlives the job)
+  uint8_t* own(uint64_t bytes) {
     void* p = nullptr;
-    uint64_t bytes = std::max<uint64_t>(16, round16(n * sizeof(T)) + 16);
-    CK(cudaMallocAsync(&p, bytes, st));
+    CK(cudaMallocAsync(&p, std::max<uint64_t>(bytes, 16) + 64, st));
     ptrs.push_back(p);
-    return (T*)p;
+    return (uint8_t*)p;
   }
   void release(void* keep = nullptr) {
     for (void* p : ptrs)
       if (p != keep) cudaFreeAsync(p, st);
     ptrs.clear();
+    cur = nullptr;
+    left = 0;
   }
 };
 
@@ -274,7 +298,7 @@ uint32_t bloom_k(int bpk) {
 
 // Survivors (k_ids, counters n_kept / n_triggers set) -> encoded files.
 void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cudaStream_t st,
-                 PhaseTimer& T) {
+                 PhaseTimer& T, uint32_t max_klen) {
   J.k_a = A.get<uint32_t>(N);
   J.k_b = A.get<uint32_t>(N);
   J.k_shared = A.get<uint32_t>(N);
@@ -283,6 +307,7 @@ void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cu
   J.k_block = A.get<uint32_t>(N + 1);
   CK(cudaMemsetAsync(J.k_bstart, 0, N + 1, st));
   J.chunk = kChunk;
+  J.chain_smem_words = 12 * 1024;  // 48 KiB
   const uint64_t chunks = (N + kChunk - 1) / kChunk + 1;
   J.chunk_table = A.get<uint32_t>(chunks * kChunk);
   J.chunk_entry = A.get<uint32_t>(chunks);
@@ -306,7 +331,9 @@ void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cu
                                                          (8 * (J.in_size + J.cap_key_bytes) + N * 64) /
                                                              std::max<uint64_t>(1, J.max_file_size));
   J.files = A.get<FileOut>(J.cap_files);
-  launch_files(J, st);
+  J.b_fnext = A.get<uint32_t>(N);
+  J.t_blocks = A.get<uint32_t>(J.cap_triggers);
+  launch_files(J, N, st);
   J.b_file = A.get<uint32_t>(N);
   J.b_off = A.get<uint64_t>(N);
   J.b_isize = A.get<uint32_t>(N);
@@ -321,43 +348,40 @@ void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cu
                                      nullptr, st);
   scan_exclusive<uint32_t, uint64_t>(J.b_isize, J.b_icum, &J.ctr->n_blocks_out, N, scratch64,
                                      nullptr, st);
+  // Output capacity, bounded without waiting for the layout: every survivor
+  // costs at most its key, its value and 15 header bytes; every block at most
+  // 4 bytes of restart word per entry, 9 bytes of count and trailer, one index
+  // entry (key + 31) and a filter share; every file 256 bytes of metaindex,
+  // footer and trailers.  The layout kernel checks the real size against it.
+  const uint64_t bpk = j->opt.bits_per_key > 0 ? (uint64_t)j->opt.bits_per_key : 0;
+  J.cap_out = J.in_size + 2 * J.cap_key_bytes + N * (80 + max_klen + (bpk + 7) / 8) +
+              (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
+  J.out = A.own(J.cap_out);
   launch_file_layout(J, st);
   check_launch();
   T.mark(kPartition);
-  read_counters(hc, J.ctr, st);
-
+  launch_encode_blocks(J, N, st);
+  T.mark(kEncodeBlocks);
+  launch_encode_rest(J, N, J.cap_files, st);
+  T.mark(kEncodeMeta);
+  // smallest / largest key of every file, gathered on the device
+  const uint64_t key_cap = 2ull * J.cap_files * max_klen;
+  uint8_t* d_keys = A.get<uint8_t>(key_cap + 1);
+  uint64_t* d_koff = A.get<uint64_t>(2ull * J.cap_files + 1);
+  launch_file_keys(J, J.cap_files, d_keys, d_koff, st);
+  check_launch();
+  std::vector<FileOut> files(J.cap_files);
+  std::vector<uint64_t> koff(2ull * J.cap_files + 1);
+  j->key_bytes.resize(key_cap + 1);
+  CK(cudaMemcpyAsync(hc, J.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(files.data(), J.files, J.cap_files * sizeof(FileOut), cudaMemcpyDeviceToHost,
+                     st));
+  CK(cudaMemcpyAsync(koff.data(), d_koff, koff.size() * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(j->key_bytes.data(), d_keys, key_cap + 1, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  check_counters(*hc);
   const uint32_t nf = hc->n_files;
   const uint64_t nbytes = hc->bytes_out;
-  const uint64_t nb = hc->n_blocks_out;
-  J.out = A.get<uint8_t>(nbytes + 16);
-  J.cap_out = nbytes;
-  T.start();
-  launch_encode_blocks(J, nb, st);
-  T.mark(kEncodeBlocks);
-  launch_encode_rest(J, nb, nf, st);
-  T.mark(kEncodeMeta);
-  // smallest / largest key of every file
-  uint32_t* d_lens = A.get<uint32_t>(2 * (uint64_t)nf + 2);
-  launch_file_key_lens(J, nf, d_lens, st);
-  std::vector<uint32_t> lens(2 * (size_t)nf);
-  std::vector<FileOut> files(nf);
-  if (nf) {
-    CK(cudaMemcpyAsync(lens.data(), d_lens, lens.size() * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(files.data(), J.files, nf * sizeof(FileOut), cudaMemcpyDeviceToHost, st));
-  }
-  CK(cudaStreamSynchronize(st));
-  std::vector<uint64_t> koff(2 * (size_t)nf + 1, 0);
-  for (size_t i = 0; i < lens.size(); i++) koff[i + 1] = koff[i] + lens[i];
-  uint64_t* d_koff = A.get<uint64_t>(koff.size());
-  uint8_t* d_keys = A.get<uint8_t>(koff.back() + 1);
-  if (nf) {
-    CK(cudaMemcpyAsync(d_koff, koff.data(), koff.size() * 8, cudaMemcpyHostToDevice, st));
-    launch_file_keys(J, nf, d_keys, d_koff, st);
-  }
-  check_launch();
-  j->key_bytes.resize(koff.back());
-  if (koff.back())
-    CK(cudaMemcpyAsync(j->key_bytes.data(), d_keys, koff.back(), cudaMemcpyDeviceToHost, st));
   if (!j->outputs_on_device && nbytes) {
     j->h_out = j->eng->pinned.take(nbytes, &j->h_out_cap);
     if (!j->h_out) throw StatusError{LC_ERR_NO_MEMORY, "pinned host buffer"};
@@ -375,9 +399,9 @@ void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cu
     j->file_size[f] = files[f].size;
     j->file_entries[f] = files[f].end_kept - files[f].first_kept;
     j->small_off[f] = koff[2 * f];
-    j->small_len[f] = lens[2 * f];
+    j->small_len[f] = (uint32_t)(koff[2 * f + 1] - koff[2 * f]);
     j->large_off[f] = koff[2 * f + 1];
-    j->large_len[f] = lens[2 * f + 1];
+    j->large_len[f] = (uint32_t)(koff[2 * f + 2] - koff[2 * f + 1]);
   }
   T.mark(kDownload);
   j->bytes_out = nbytes;
@@ -461,6 +485,7 @@ void run_compaction(lc_job* j, cudaStream_t st) {
     }
     J.in = d_in;
     J.in_size = in_size;
+    J.in_end = d_in + in_size + (zero_copy ? 0 : 16);
     TableDesc* d_td = A.get<TableDesc>(nt);
     CK(cudaMemcpyAsync(d_td, td.data(), nt * sizeof(TableDesc), cudaMemcpyHostToDevice, st));
     J.tables = d_td;
@@ -604,13 +629,13 @@ void run_compaction(lc_job* j, cudaStream_t st) {
     J.k_forced = A.get<uint8_t>(N + 1);
     uint32_t* scratch32 = A.get<uint32_t>(scan_scratch_elems(N + 1));
     launch_drop(J, N, st);
-    launch_triggers(J, N, st);
+    launch_triggers(J, N, A.get<uint32_t>(J.n_gp + 1), st);
     scan_exclusive<uint8_t, uint32_t>(J.keep, J.kept_pos, &J.ctr->n_entries_in, N, scratch32,
                                       &J.ctr->n_kept, st);
     launch_kept_compact(J, N, st);
     check_launch();
     T.mark(kDrop);
-    encode_tail(j, J, A, N, &hc, st, T);
+    encode_tail(j, J, A, N, &hc, st, T, std::max<uint32_t>(hc.max_klen, 8));
     CK(cudaEventRecord(ev1, st));
     CK(cudaStreamSynchronize(st));
     float ms = 0;
@@ -670,6 +695,7 @@ void run_build(lc_job* j, cudaStream_t st) {
     CK(cudaMemcpyAsync(d_vo, j->bvoffs, (N + 1) * 8, kind, st));
     J.in = d_vals;
     J.in_size = vb;
+    J.in_end = d_vals + vb + 16;
     J.cap_key_bytes = kb;
     J.cap_entries = N;
     J.ctr = A.get<Counters>(1);
@@ -696,7 +722,20 @@ void run_build(lc_job* j, cudaStream_t st) {
     Counters hc;
     j->entries_in = N;
     j->key_bytes_in = kb;
-    encode_tail(j, J, A, N, &hc, st, T);
+    uint32_t max_klen = 8;
+    {
+      std::vector<uint64_t> hk;
+      const uint64_t* ko = j->bkoffs;
+      if (j->inputs_on_device) {
+        hk.resize(N + 1);
+        CK(cudaMemcpyAsync(hk.data(), j->bkoffs, (N + 1) * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ko = hk.data();
+      }
+      for (uint64_t i = 0; i < N; i++)
+        max_klen = std::max<uint32_t>(max_klen, (uint32_t)(ko[i + 1] - ko[i]));
+    }
+    encode_tail(j, J, A, N, &hc, st, T, max_klen);
     CK(cudaEventRecord(ev1, st));
     CK(cudaStreamSynchronize(st));
     float ms = 0;

@@ -83,6 +83,7 @@ struct JobDev {
   // input
   const uint8_t* in;
   uint64_t in_size;
+  const uint8_t* in_end;  // end of memory that may be read with 16-byte loads
   const TableDesc* tables;
   uint32_t n_tables;
   uint32_t n_runs;
@@ -152,6 +153,7 @@ struct JobDev {
   uint32_t* chunk_table;     // per chunk: exit for each window entry
   uint32_t* chunk_entry;     // per chunk: resolved entry point
   uint32_t window;           // table width
+  uint32_t chain_smem_words; // shared-memory words for staging the chunk tables
 
   // output blocks
   uint32_t* b_first;         // first kept entry of block (cap_blocks_out + 1)
@@ -168,6 +170,8 @@ struct JobDev {
   uint32_t* b_gbytes;        // filter group bytes (nonzero at group starts)
   uint64_t* b_gcum;          // prefix of b_gbytes
   uint32_t* b_gkeys;         // keys in the group (at group starts)
+  uint32_t* b_fnext;         // first block of the next file if a file starts here
+  uint32_t* t_blocks;        // output block starting at each grandparent cut
   uint64_t cap_blocks_out;
 
   // files

@@ -38,7 +38,7 @@ void launch_iota(uint32_t* ids, uint64_t n, cudaStream_t st);
 void launch_merge_round(const JobDev& J, const uint32_t* src, uint32_t* dst, uint32_t width,
                         uint64_t n, cudaStream_t st);
 void launch_drop(const JobDev& J, uint64_t n, cudaStream_t st);
-void launch_triggers(const JobDev& J, uint64_t n, cudaStream_t st);
+void launch_triggers(const JobDev& J, uint64_t n, uint32_t* gp_first, cudaStream_t st);
 void launch_kept_compact(const JobDev& J, uint64_t n, cudaStream_t st);
 
 // lc_encode.cu -- survivors -> output tables
@@ -47,13 +47,12 @@ void launch_next(const JobDev& J, uint64_t n_cap, cudaStream_t st);
 void launch_chain(const JobDev& J, uint64_t n_cap, cudaStream_t st);
 void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st);
 void launch_block_sizes(const JobDev& J, uint32_t* tmp32, uint64_t nb_cap, cudaStream_t st);
-void launch_files(const JobDev& J, cudaStream_t st);
+void launch_files(const JobDev& J, uint64_t nb_cap, cudaStream_t st);
 void launch_block_layout(const JobDev& J, uint64_t nb_cap, cudaStream_t st);
 void launch_file_layout(const JobDev& J, cudaStream_t st);
 void launch_encode_blocks(const JobDev& J, uint64_t nb, cudaStream_t st);
 void launch_encode_rest(const JobDev& J, uint64_t nb, uint32_t n_files, cudaStream_t st);
-void launch_file_keys(const JobDev& J, uint32_t n_files, uint8_t* key_out,
-                      const uint64_t* key_off, cudaStream_t st);
-void launch_file_key_lens(const JobDev& J, uint32_t n_files, uint32_t* lens, cudaStream_t st);
+void launch_file_keys(const JobDev& J, uint32_t cap_files, uint8_t* key_out, uint64_t* key_off,
+                      cudaStream_t st);
 
 }  // namespace lc

@@ -140,29 +140,64 @@ __global__ void k_drop(JobDev J, const uint32_t* __restrict__ ids) {
   }
 }
 
-__global__ void k_triggers(JobDev J) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// gp_first[g] = first merged position whose grandparent count reaches g
+// (gp_idx is non-decreasing along the merge order).
+__global__ void k_gp_first(JobDev J, uint32_t* gp_first) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > J.n_gp) return;
   const uint64_t n = J.ctr->n_entries_in;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (J.gp_idx[mid] >= g) hi = mid;
+    else lo = mid + 1;
+  }
+  gp_first[g] = (uint32_t)lo;
+}
+
+// The cut positions: after a cut at t (or from the first key), the next cut
+// is the first key whose running overlap exceeds the limit, i.e. the first
+// position whose grandparent count reaches the smallest g with
+// prefix[g] - prefix[gp_idx[t]] > limit.  Few cuts; one thread walks them
+// over shared-memory copies of the prefix and first-position arrays.
+__global__ void k_triggers(JobDev J, const uint32_t* gp_first, bool in_smem) {
+  extern __shared__ uint64_t s_tr[];
+  const uint64_t n = J.ctr->n_entries_in;
+  const uint32_t G = J.n_gp;
+  const uint64_t* pre = J.gp_prefix;
+  const uint32_t* first = gp_first;
+  if (in_smem) {  // G + 1 prefixes, then G + 1 first positions
+    uint32_t* s_first = reinterpret_cast<uint32_t*>(s_tr + G + 1);
+    for (uint32_t g = threadIdx.x; g <= G; g += blockDim.x) {
+      s_tr[g] = J.gp_prefix[g];
+      s_first[g] = gp_first[g];
+    }
+    pre = s_tr;
+    first = s_first;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   uint32_t cnt = 0;
-  if (n > 0 && J.n_gp > 0) {
+  if (n > 0 && G > 0) {
     const uint64_t limit = (uint64_t)J.max_gp_overlap;
-    uint64_t base = J.gp_prefix[J.gp_idx[0]];
-    uint64_t t = 0;
-    while (t + 1 < n) {
-      if (J.gp_prefix[J.gp_idx[n - 1]] - base <= limit) break;
-      uint64_t lo = t + 1, hi = n - 1;
+    uint32_t gb = J.gp_idx[0];
+    while (true) {
+      const uint64_t target = pre[gb] + limit;  // need prefix > target
+      uint32_t lo = gb + 1, hi = G + 1;
       while (lo < hi) {
-        uint64_t mid = (lo + hi) >> 1;
-        if (J.gp_prefix[J.gp_idx[mid]] - base > limit) hi = mid;
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pre[mid] > target) hi = mid;
         else lo = mid + 1;
       }
+      if (lo > G) break;
+      const uint64_t t = first[lo];
+      if (t >= n) break;
       if (cnt >= J.cap_triggers) {
         set_error(J.ctr, kErrLimit, 1);
         break;
       }
-      J.triggers[cnt++] = (uint32_t)lo;
-      base = J.gp_prefix[J.gp_idx[lo]];
-      t = lo;
+      J.triggers[cnt++] = (uint32_t)t;
+      gb = J.gp_idx[t];
     }
   }
   J.ctr->n_triggers = cnt;
@@ -205,8 +240,11 @@ void launch_drop(const JobDev& J, uint64_t n, cudaStream_t st) {
   if (n) note_launch(), k_drop<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, J.m_ids);
 }
 
-void launch_triggers(const JobDev& J, uint64_t n, cudaStream_t st) {
-  note_launch(), k_triggers<<<1, 32, 0, st>>>(J);
+void launch_triggers(const JobDev& J, uint64_t n, uint32_t* gp_first, cudaStream_t st) {
+  if (J.n_gp) note_launch(), k_gp_first<<<(J.n_gp + 1 + 255) / 256, 256, 0, st>>>(J, gp_first);
+  const size_t smem = (size_t)(J.n_gp + 1) * 12;
+  const bool in_smem = smem <= 48 * 1024;
+  note_launch(), k_triggers<<<1, 256, in_smem ? smem : 0, st>>>(J, gp_first, in_smem);
 }
 
 void launch_kept_compact(const JobDev& J, uint64_t n, cudaStream_t st) {

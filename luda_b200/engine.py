@@ -298,16 +298,29 @@ class Engine:
         if st != LC_OK:
             raise LcError(st, self.lib.lc_last_error().decode())
 
-    def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: bool = False) -> CompactionResult:
+    def prepare(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
+                outputs_on_device: bool = False) -> "PreparedJob":
+        """Builds the C descriptor once, for repeated runs of the same job."""
         keep = _Keep()
-        d = make_desc(job, keep, device_tables, outputs_on_device)
+        return PreparedJob(make_desc(job, keep, device_tables, outputs_on_device), keep,
+                           outputs_on_device)
+
+    def run(self, p: "PreparedJob") -> CompactionResult:
         out = LcJobOut()
         jh = C.c_void_p()
-        self._check(self.lib.lc_compact(self.h, C.byref(d), C.byref(out), C.byref(jh)))
-        res = _result(out, outputs_on_device)
+        self._check(self.lib.lc_compact(self.h, C.byref(p.desc), C.byref(out), C.byref(jh)))
+        res = _result(out, p.outputs_on_device)
         res._handle = _JobHandle(self.lib, jh, self)
         return res
+
+    def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
+                outputs_on_device: bool = False) -> CompactionResult:
+        return self.run(self.prepare(job, device_tables, outputs_on_device))
+
+    def submit_prepared(self, p: "PreparedJob") -> "AsyncJob":
+        jh = C.c_void_p()
+        self._check(self.lib.lc_job_submit(self.h, C.byref(p.desc), C.byref(jh)))
+        return AsyncJob(self, jh, p.keep)
 
     def submit(self, job: CompactionJob) -> "AsyncJob":
         keep = _Keep()
@@ -343,6 +356,13 @@ class Engine:
             return C.string_at(out.data + out.file_offset[0], out.file_size[0])
         finally:
             self.lib.lc_job_release(jh)
+
+
+@dataclasses.dataclass
+class PreparedJob:
+    desc: LcJobDesc
+    keep: object
+    outputs_on_device: bool
 
 
 class AsyncJob:
