@@ -43,13 +43,17 @@ typedef struct lc_job lc_job;
 typedef struct {
   int32_t device;               /* CUDA device ordinal */
   uint64_t device_budget_bytes; /* admission budget; 0 = 40 GiB */
-  int32_t max_inflight_jobs;    /* jobs on the device at once; 0 = 4 */
+  int32_t max_inflight_jobs;    /* worker threads, i.e. batches on the device at once; 0 = 4 */
   uint32_t flags;               /* LC_FLAG_* */
+  int32_t max_batch_jobs;       /* jobs one batch (one set of launches) may hold; 0 = 64 */
 } lc_config;
 
 /* lc_config.flags: record CUDA events around each phase of every job on the
  * job's own stream and report the device time per phase in lc_job_out. */
 #define LC_FLAG_PHASE_TIMING 1u
+/* lc_config.flags: launch every kernel directly instead of replaying captured
+ * CUDA graphs (same results; for debugging and for measuring the graphs). */
+#define LC_FLAG_NO_GRAPHS 2u
 
 /* One input SSTable (the bytes of a file at level L or L+1). */
 typedef struct {
@@ -146,6 +150,38 @@ void lc_job_release(lc_job* j);
 /* Synchronous compaction on the calling thread: the drop-in for one
  * DoCompactionWork call.  *job_out must be released with lc_job_release. */
 lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_job** job_out);
+
+/* Batched compaction (no counterpart in the reference, which runs one
+ * DoCompactionWork at a time).  Runs n independent compactions together:
+ * every kernel launch covers all jobs of a batch (up to max_batch_jobs; more
+ * are split into several batches), and the kernel sequence after the first
+ * host synchronisation is one captured CUDA graph, replayed for later batches
+ * of the same shape.  Each job's output is byte-identical to lc_compact on the
+ * same descriptor.  On return every jobs[i] is a finished handle (release each
+ * with lc_job_release): lc_job_wait returns its status at once and
+ * lc_job_result its output.  Returns LC_OK when every job succeeded, else the
+ * status of the first job that failed; argument errors create no handles. */
+lc_status lc_compact_batch(lc_engine* e, int32_t n, const lc_job_desc* descs, lc_job** jobs);
+
+/* Launch parameters the autotuner chooses (no counterpart in the reference). */
+typedef struct {
+  uint32_t ctas_per_job;  /* CTAs per job in the grid-stride kernels; 0 = from the sizes */
+  uint32_t merge_items;   /* merge-path outputs per thread, 1..32 */
+  uint32_t merge_threads; /* threads per merge CTA: 64..1024, a multiple of 32;
+                             the merge tile is merge_threads * merge_items outputs */
+} lc_tuning;
+
+lc_status lc_get_tuning(lc_engine* e, lc_tuning* out);
+/* Applies to batches that start after the call. */
+lc_status lc_set_tuning(lc_engine* e, const lc_tuning* t);
+
+/* Autotuner: runs the n jobs as batches under candidate settings (merge
+ * tile, items per thread, CTAs per job), `repeats` times each, keeps the one
+ * with the lowest median device time for the engine and writes it to
+ * *chosen.  The outputs are computed and discarded; the descriptors' inputs
+ * must stay valid for the call. */
+lc_status lc_autotune(lc_engine* e, int32_t n, const lc_job_desc* descs, int32_t repeats,
+                      lc_tuning* chosen);
 
 /* Flush encoder: one table from n sorted internal keys and values, the GPU
  * counterpart of BuildTable's TableBuilder loop (db/builder.cc:17-60; LUDA's

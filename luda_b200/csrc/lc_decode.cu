@@ -80,8 +80,10 @@ __device__ __forceinline__ const uint8_t* entry_header(const uint8_t* p, const u
   return p;
 }
 
-__global__ void k_table_index_count(JobDev J) {
+__global__ void k_table_index_count(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t t = blockIdx.x;
+  if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
   const uint8_t* base = J.in + T.off;
   __shared__ uint64_t s_ioff, s_isize;
@@ -119,8 +121,10 @@ __global__ void k_table_index_count(JobDev J) {
   }
 }
 
-__global__ void k_table_index_entries(JobDev J) {
+__global__ void k_table_index_entries(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t t = blockIdx.x;
+  if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
   const uint8_t* base = J.in + T.off;
   uint64_t io, is;
@@ -178,7 +182,7 @@ __global__ void k_table_index_entries(JobDev J) {
           break;
         }
         const uint64_t o = out_base + ex + k;
-        if (o >= out_end) {
+        if (o >= out_end || o >= J.cap_blocks_in) {
           ok = false;
           break;
         }
@@ -324,11 +328,14 @@ __device__ void block_count_one(const JobDev& J, uint64_t b, uint32_t lane, cons
   }
 }
 
-__global__ void __launch_bounds__(kDecWarps * 32) k_block_count(JobDev J) {
+__global__ void __launch_bounds__(kDecWarps * 32) k_block_count(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t dec_smem[];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
-  const uint64_t nblk = J.ctr->n_blocks_in;
+  // after a footer or index error some block handles were never written
+  if (J.ctr->error) return;
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
        b += (uint64_t)gridDim.x * kDecWarps) {
     const uint8_t* st = stage_block(J, b, W.stage, lane);
@@ -337,14 +344,17 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_count(JobDev J) {
   }
 }
 
-__global__ void k_run_bounds(JobDev J) {
+__global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   // one thread: entries of merge child r start at the first block of its
   // first table
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   uint32_t next_run = 0;
+  const bool bad = J.ctr->error != 0;  // the job fails; keep every read in bounds
   for (uint32_t t = 0; t < J.n_tables; t++) {
     while (next_run <= J.tables[t].run) {
-      J.run_entry_begin_w[next_run] = J.blk_ent_base[J.tbl_block_base[t]];
+      J.run_entry_begin_w[next_run] =
+          bad ? 0 : J.blk_ent_base[min(J.tbl_block_base[t], J.cap_blocks_in)];
       next_run++;
     }
   }
@@ -516,12 +526,13 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
   return true;
 }
 
-__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(JobDev J) {
+__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t dec_smem[];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
   if (J.ctr->error) return;
-  const uint64_t nblk = J.ctr->n_blocks_in;
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
        b += (uint64_t)gridDim.x * kDecWarps) {
     const uint8_t* st = stage_block(J, b, W.stage, lane);
@@ -530,62 +541,65 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(JobDev J) {
   }
 }
 
-__global__ void k_entries_from_offsets(JobDev J, const uint64_t* koffs, const uint64_t* voffs,
-                                       uint64_t n) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t ko = koffs[i], kl = koffs[i + 1] - ko;
-  if (kl < 8) {
-    set_error(J.ctr, kErrShortKey, (uint32_t)i);
-    return;
+__global__ void k_entries_from_offsets(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = J.cap_entries;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t ko = J.src_koffs[i], kl = J.src_koffs[i + 1] - ko;
+    if (kl < 8) {
+      set_error(J.ctr, kErrShortKey, (uint32_t)i);
+      continue;
+    }
+    J.e_koff[i] = (uint32_t)ko;
+    J.e_klen[i] = (uint32_t)kl;
+    J.e_voff[i] = (uint32_t)J.src_voffs[i];
+    J.e_vlen[i] = (uint32_t)(J.src_voffs[i + 1] - J.src_voffs[i]);
+    J.e_pfx[i] = user_prefix(J.keys + ko, (uint32_t)kl);
+    J.k_ids[i] = (uint32_t)i;
   }
-  J.e_koff[i] = (uint32_t)ko;
-  J.e_klen[i] = (uint32_t)kl;
-  J.e_voff[i] = (uint32_t)voffs[i];
-  J.e_vlen[i] = (uint32_t)(voffs[i + 1] - voffs[i]);
-  J.e_pfx[i] = user_prefix(J.keys + ko, (uint32_t)kl);
-  J.k_ids[i] = (uint32_t)i;
 }
 
 }  // namespace
 
-void launch_table_index_count(const JobDev& J, cudaStream_t st) {
-  note_launch(), k_table_index_count<<<J.n_tables, 128, 0, st>>>(J);
+void launch_table_index_count(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_table_index_count<<<dim3(bt.max_tables, bt.B), 128, 0, st>>>(bt.d);
 }
-void launch_table_index_entries(const JobDev& J, cudaStream_t st) {
-  note_launch(), k_table_index_entries<<<J.n_tables, 128, 0, st>>>(J);
+void launch_table_index_entries(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_table_index_entries<<<dim3(bt.max_tables, bt.B), 128, 0, st>>>(bt.d);
 }
+
 static void dec_smem_attr(const void* fn) {
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(kDecWarps * sizeof(DecWarpSmem)));
 }
 
-void launch_block_count(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    dec_smem_attr((const void*)k_block_count);
-    attr = true;
-  }
-  // grid-stride over the device-side block count: 3 CTAs per SM x 8 waves
-  const uint64_t ctas =
-      std::min<uint64_t>((std::max<uint64_t>(n_blocks_cap, 1) + kDecWarps - 1) / kDecWarps, 148 * 3 * 8);
-  note_launch(), k_block_count<<<(unsigned)ctas, kDecWarps * 32, kDecWarps * sizeof(DecWarpSmem), st>>>(J);
+static unsigned dec_ctas(const Batch& bt) {
+  // grid-stride over the device-side block count: 3 CTAs per SM x 8 waves in
+  // total, shared out among the jobs of the batch
+  const uint64_t cap = std::max<uint64_t>(1, bt.ctas_per_job ? bt.ctas_per_job : 148 * 3 * 8 / bt.B);
+  return grid_x(bt.max_blocks_in, kDecWarps, cap);
 }
-void launch_run_bounds(const JobDev& J, cudaStream_t st) { note_launch(), k_run_bounds<<<1, 32, 0, st>>>(J); }
-void launch_block_decode(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    dec_smem_attr((const void*)k_block_decode);
-    attr = true;
-  }
-  const uint64_t ctas =
-      std::min<uint64_t>((std::max<uint64_t>(n_blocks_cap, 1) + kDecWarps - 1) / kDecWarps, 148 * 3 * 8);
-  note_launch(), k_block_decode<<<(unsigned)ctas, kDecWarps * 32, kDecWarps * sizeof(DecWarpSmem), st>>>(J);
+
+void decode_kernel_attributes() {
+  dec_smem_attr((const void*)k_block_count);
+  dec_smem_attr((const void*)k_block_decode);
 }
-void launch_entries_from_offsets(const JobDev& J, const uint64_t* koffs, const uint64_t* voffs,
-                                 uint64_t n, cudaStream_t st) {
-  if (n == 0) return;
-  note_launch(), k_entries_from_offsets<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, koffs, voffs, n);
+
+void launch_block_count(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_count<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
+                                 kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
+}
+void launch_run_bounds(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_run_bounds<<<dim3(1, bt.B), 32, 0, st>>>(bt.d);
+}
+void launch_block_decode(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
+                                  kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
+}
+void launch_entries_from_offsets(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_entries_from_offsets<<<dim3(grid_x(bt.max_entries, 256, 148 * 8), bt.B), 256, 0,
+                                          st>>>(bt.d);
 }
 
 }  // namespace lc

@@ -68,13 +68,16 @@ __device__ __forceinline__ const uint8_t* kept_key(const JobDev& J, uint64_t k, 
   return J.keys + J.e_koff[id];
 }
 
-__global__ void k_sizes(JobDev J) {
-  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = k < J.ctr->n_kept;
-  uint32_t kl = 0, vl = 0;
-  if (valid) {
+__global__ void k_sizes(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = J.ctr->n_kept;
+  unsigned long long kb = 0, vb = 0;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * blockDim.x; k0 < n; k0 += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = k0 + threadIdx.x;
+    if (k >= n) continue;
+    uint32_t kl;
     const uint8_t* key = kept_key(J, k, &kl);
-    vl = J.e_vlen[J.k_ids[k]];
+    const uint32_t vl = J.e_vlen[J.k_ids[k]];
     uint32_t shared = 0;
     if (k > 0) {
       uint32_t pl;
@@ -85,9 +88,10 @@ __global__ void k_sizes(JobDev J) {
     J.k_a[k] = 1 + varint_len(kl) + varint_len(vl) + kl + vl;
     J.k_b[k] = varint_len(shared) + varint_len(kl - shared) + varint_len(vl) + (kl - shared) + vl;
     J.k_shared[k] = shared;
+    kb += kl;
+    vb += vl;
   }
   // survivor byte totals, one atomic per warp
-  unsigned long long kb = kl, vb = vl;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     kb += __shfl_xor_sync(0xffffffffu, kb, o);
@@ -99,10 +103,15 @@ __global__ void k_sizes(JobDev J) {
   }
 }
 
-__global__ void k_next(JobDev J) {
-  const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_zero_bstart(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = J.ctr->n_kept;
-  if (s >= n) return;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    J.k_bstart[i] = 0;
+}
+
+__device__ __forceinline__ void next_one(const JobDev& J, uint64_t s, uint64_t n) {
   const uint32_t R = J.restart_interval;
   const uint64_t bs = J.block_size;
   uint64_t buf = 0;
@@ -131,27 +140,40 @@ __global__ void k_next(JobDev J) {
   atomicMax(&J.ctr->max_jump, (uint32_t)(nxt - s));
 }
 
+__global__ void k_next(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = J.ctr->n_kept;
+  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+       s += (uint64_t)gridDim.x * blockDim.x)
+    next_one(J, s, n);
+}
+
+
 // Per chunk: exits of the chain for every entry point in the first `window`
 // survivors of the chunk.
-__global__ void k_chain_tables(JobDev J) {
+__global__ void k_chain_tables(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ uint32_t s_next[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
-  const uint64_t c0 = (uint64_t)blockIdx.x * C;
-  if (c0 >= n) return;
-  const uint64_t c1 = min(n, c0 + C);
   const uint32_t W = J.ctr->max_jump;
   if (W > C) return;  // resolved sequentially instead
-  for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < W; i += blockDim.x) {
-    uint64_t e = c0 + i;
-    while (e < c1) e = s_next[e - c0];
-    J.chunk_table[(uint64_t)blockIdx.x * C + i] = (uint32_t)e;
+  for (uint64_t c = blockIdx.x; c * C < n; c += gridDim.x) {
+    const uint64_t c0 = c * C;
+    const uint64_t c1 = min(n, c0 + C);
+    __syncthreads();
+    for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < W; i += blockDim.x) {
+      uint64_t e = c0 + i;
+      while (e < c1) e = s_next[e - c0];
+      J.chunk_table[c * C + i] = (uint32_t)e;
+    }
   }
 }
 
-__global__ void k_chain_resolve(JobDev J) {
+__global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ uint32_t s_tab[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
@@ -184,35 +206,40 @@ __global__ void k_chain_resolve(JobDev J) {
   }
 }
 
-__global__ void k_chain_mark(JobDev J) {
+__global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ uint32_t s_next[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
   if (J.ctr->max_jump > C) return;
-  const uint64_t c0 = (uint64_t)blockIdx.x * C;
-  if (c0 >= n) return;
-  const uint64_t c1 = min(n, c0 + C);
-  for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint64_t e = J.chunk_entry[blockIdx.x];
-    while (e < c1) {
-      J.k_bstart[e] = 1;
-      e = s_next[e - c0];
+  for (uint64_t c = blockIdx.x; c * C < n; c += gridDim.x) {
+    const uint64_t c0 = c * C;
+    const uint64_t c1 = min(n, c0 + C);
+    __syncthreads();
+    for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint64_t e = J.chunk_entry[c];
+      while (e < c1) {
+        J.k_bstart[e] = 1;
+        e = s_next[e - c0];
+      }
     }
   }
 }
 
-__global__ void k_block_list(JobDev J) {
-  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_block_list(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = J.ctr->n_kept;
-  if (k == 0) J.b_first[J.k_block[n]] = (uint32_t)n;
-  if (k < n && J.k_bstart[k]) J.b_first[J.k_block[k]] = (uint32_t)k;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= n;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    if (k == n) J.b_first[J.k_block[n]] = (uint32_t)n;
+    else if (J.k_bstart[k]) J.b_first[J.k_block[k]] = (uint32_t)k;
+  }
 }
 
-__global__ void k_block_sizes(JobDev J, uint32_t* tmp32) {
-  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= J.ctr->n_blocks_out) return;
+__device__ __forceinline__ void block_size_one(const JobDev& J, uint64_t b) {
+  uint32_t* tmp32 = J.tmp32;
   const uint32_t R = J.restart_interval;
   const uint64_t s = J.b_first[b], e = J.b_first[b + 1];
   uint64_t sum = 0;
@@ -223,6 +250,14 @@ __global__ void k_block_sizes(JobDev J, uint32_t* tmp32) {
   tmp32[b] = size + kTrailer;
 }
 
+__global__ void k_block_sizes(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t nb = J.ctr->n_blocks_out;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (uint64_t)gridDim.x * blockDim.x)
+    block_size_one(J, b);
+}
+
 // Output files: size cuts at block ends, grandparent cuts at forced blocks.
 // Like the block chain, a file's end depends on where it starts: every block
 // b gets b_fnext[b], the first block of the next file if a file began at b (a
@@ -230,14 +265,16 @@ __global__ void k_block_sizes(JobDev J, uint32_t* tmp32) {
 // walks the few file starts.
 
 // t_blocks[i] = output block that starts at grandparent cut i (ascending).
-__global__ void k_forced_blocks(JobDev J) {
+__global__ void k_forced_blocks(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= J.ctr->n_triggers) return;
   const uint64_t kp = J.kept_pos[J.triggers[i]];
   J.t_blocks[i] = kp < J.ctr->n_kept ? J.k_block[kp] : (uint32_t)J.ctr->n_blocks_out;
 }
 
-__global__ void k_file_next(JobDev J) {
+__global__ void k_file_next(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t nt = J.ctr->n_triggers;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
@@ -270,7 +307,8 @@ __global__ void k_file_next(JobDev J) {
   }
 }
 
-__global__ void k_files(JobDev J) {
+__global__ void k_files(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   uint32_t f = 0;
@@ -302,9 +340,17 @@ __device__ __forceinline__ uint32_t file_of_block(const JobDev& J, uint64_t b) {
   return lo;
 }
 
-__global__ void k_block_layout(JobDev J) {
-  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= J.ctr->n_blocks_out) return;
+__device__ void block_layout_one(const JobDev& J, uint64_t b);
+
+__global__ void k_block_layout(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t nb = J.ctr->n_blocks_out;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (uint64_t)gridDim.x * blockDim.x)
+    block_layout_one(J, b);
+}
+
+__device__ void block_layout_one(const JobDev& J, uint64_t b) {
   const uint32_t f = file_of_block(J, b);
   const uint32_t fb0 = J.files[f].first_block, fb1 = J.files[f].end_block;
   const uint64_t base = J.b_cum[fb0];
@@ -359,7 +405,8 @@ __global__ void k_block_layout(JobDev J) {
   J.b_isize[b] = 1 + varint_len(ilen) + varint_len(hl) + ilen + hl;
 }
 
-__global__ void k_file_layout(JobDev J) {
+__global__ void k_file_layout(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t nf = J.ctr->n_files;
   for (uint32_t f = threadIdx.x; f < nf; f += blockDim.x) {
     FileOut& F = J.files[f];
@@ -487,7 +534,8 @@ __device__ __forceinline__ void group_copy(const uint8_t* src, uint32_t len, uin
   }
 }
 
-__global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(JobDev J) {
+__global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t enc_smem[];
   uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
   uint8_t* stages = enc_smem + 4096;
@@ -675,7 +723,8 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
   }
 }
 
-__global__ void k_encode_filters(JobDev J) {
+__global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t lane = threadIdx.x & 31;
   if (J.bits_per_key <= 0 || J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
@@ -714,7 +763,8 @@ __device__ __forceinline__ void encode_index_entry(const JobDev& J, uint64_t b) 
   if (b + 1 == fb1) st_le32(ra + 4, fb1 - fb0);
 }
 
-__global__ void k_encode_index(JobDev J) {
+__global__ void k_encode_index(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
@@ -722,7 +772,8 @@ __global__ void k_encode_index(JobDev J) {
     encode_index_entry(J, b);
 }
 
-__global__ void k_encode_meta(JobDev J) {
+__global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= J.ctr->n_files || J.ctr->error) return;
   const FileOut& F = J.files[f];
@@ -761,7 +812,8 @@ __global__ void k_encode_meta(JobDev J) {
 }
 
 // Trailers of the filter, metaindex and index blocks: one CTA per block.
-__global__ void k_crc_regions(JobDev J) {
+__global__ void k_crc_regions(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t tab[256];
   __shared__ uint32_t s_x[32];
   crc_table_init(tab);
@@ -798,7 +850,10 @@ __global__ void k_crc_regions(JobDev J) {
 
 // Smallest / largest internal key of every output file, packed: one CTA;
 // koff[2f], koff[2f+1] start file f's smallest and largest key.
-__global__ void k_file_keys(JobDev J, uint8_t* out, uint64_t* koff) {
+__global__ void k_file_keys(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  uint8_t* out = J.fkeys;
+  uint64_t* koff = J.fkoff;
   __shared__ uint64_t s_warp[32];
   __shared__ uint64_t s_carry;
   const uint32_t nf = J.ctr->error ? 0 : J.ctr->n_files;
@@ -839,61 +894,76 @@ __global__ void k_file_keys(JobDev J, uint8_t* out, uint64_t* koff) {
   }
 }
 
-inline unsigned grid_for(uint64_t n, unsigned per) { return (unsigned)((n + per - 1) / per) + (n == 0); }
+inline unsigned per_job(const Batch& bt, unsigned total) {
+  return bt.ctas_per_job ? bt.ctas_per_job : std::max<unsigned>(1, total / bt.B);
+}
 
 }  // namespace
 
-void launch_sizes(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
-  note_launch(), k_sizes<<<grid_for(n_cap, 256), 256, 0, st>>>(J);
+void launch_zero_bstart(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_zero_bstart<<<dim3(grid_x(bt.max_entries + 1, 256, per_job(bt, 148 * 8)), bt.B),
+                                 256, 0, st>>>(bt.d);
 }
-void launch_next(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
-  note_launch(), k_next<<<grid_for(n_cap, 256), 256, 0, st>>>(J);
+void launch_sizes(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_sizes<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
+                           st>>>(bt.d);
 }
-void launch_chain(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
-  const uint64_t chunks = (n_cap + J.chunk - 1) / J.chunk + 1;
-  const size_t smem = (size_t)J.chunk * sizeof(uint32_t);
-  note_launch(), k_chain_tables<<<(unsigned)chunks, 256, smem, st>>>(J);
-  note_launch(), k_chain_resolve<<<1, 256, (size_t)J.chain_smem_words * 4, st>>>(J);
-  note_launch(), k_chain_mark<<<(unsigned)chunks, 128, smem, st>>>(J);
+void launch_next(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_next<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
+                          st>>>(bt.d);
 }
-void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st) {
-  note_launch(), k_block_list<<<grid_for(n_cap + 1, 256), 256, 0, st>>>(J);
+void launch_chain(const Batch& bt, cudaStream_t st) {
+  const uint64_t chunks = (bt.max_entries + bt.chunk - 1) / bt.chunk + 1;
+  const size_t smem = (size_t)bt.chunk * sizeof(uint32_t);
+  const unsigned g = (unsigned)std::min<uint64_t>(chunks, per_job(bt, 148 * 4));
+  note_launch(), k_chain_tables<<<dim3(g, bt.B), 256, smem, st>>>(bt.d);
+  note_launch(), k_chain_resolve<<<dim3(1, bt.B), 256, (size_t)bt.chain_smem_words * 4, st>>>(bt.d);
+  note_launch(), k_chain_mark<<<dim3(g, bt.B), 128, smem, st>>>(bt.d);
 }
-void launch_block_sizes(const JobDev& J, uint32_t* tmp32, uint64_t nb_cap, cudaStream_t st) {
-  note_launch(), k_block_sizes<<<grid_for(nb_cap, 256), 256, 0, st>>>(J, tmp32);
+void launch_block_list(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_list<<<dim3(grid_x(bt.max_entries + 1, 256, per_job(bt, 148 * 8)), bt.B), 256,
+                                0, st>>>(bt.d);
 }
-void launch_files(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
-  note_launch(), k_forced_blocks<<<(J.cap_triggers + 255) / 256, 256, 0, st>>>(J);
-  note_launch(), k_file_next<<<(unsigned)std::min<uint64_t>(grid_for(nb_cap, 256), 148 * 16), 256, 0, st>>>(J);
-  note_launch(), k_files<<<1, 32, 0, st>>>(J);
+void launch_block_sizes(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_sizes<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
+                                 0, st>>>(bt.d);
 }
-void launch_block_layout(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
-  note_launch(), k_block_layout<<<grid_for(nb_cap, 256), 256, 0, st>>>(J);
+void launch_files(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_forced_blocks<<<dim3((bt.max_cap_triggers + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_file_next<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
+                               st>>>(bt.d);
+  note_launch(), k_files<<<dim3(1, bt.B), 32, 0, st>>>(bt.d);
 }
-void launch_file_layout(const JobDev& J, cudaStream_t st) { note_launch(), k_file_layout<<<1, 256, 0, st>>>(J); }
-void launch_encode_blocks(const JobDev& J, uint64_t nb_cap, cudaStream_t st) {
-  if (!nb_cap) return;
-  const size_t smem = 4096 + (size_t)kEncWarps * (kEncStage + kEncScratch);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  // grid-stride over the device-side block count: up to 3 CTAs per SM x 8 waves
-  const uint64_t ctas = std::min<uint64_t>((nb_cap + kEncWarps - 1) / kEncWarps, 148 * 3 * 8);
-  note_launch(), k_encode_blocks<<<(unsigned)ctas, kEncWarps * 32, smem, st>>>(J);
+void launch_block_layout(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_layout<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
+                                  0, st>>>(bt.d);
 }
-void launch_encode_rest(const JobDev& J, uint64_t nb_cap, uint32_t cap_files, cudaStream_t st) {
-  if (nb_cap == 0) return;
-  const uint64_t wctas = std::min<uint64_t>((nb_cap * 32 + 255) / 256, 148 * 16);
-  note_launch(), k_encode_filters<<<(unsigned)wctas, 256, 0, st>>>(J);
-  note_launch(), k_encode_index<<<(unsigned)std::min<uint64_t>(grid_for(nb_cap, 256), 148 * 16), 256, 0, st>>>(J);
-  note_launch(), k_encode_meta<<<grid_for(cap_files, 128), 128, 0, st>>>(J);
-  note_launch(), k_crc_regions<<<cap_files * 3, 256, 0, st>>>(J);
+void launch_file_layout(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_file_layout<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
 }
-void launch_file_keys(const JobDev& J, uint32_t cap_files, uint8_t* key_out, uint64_t* key_off,
-                      cudaStream_t st) {
-  note_launch(), k_file_keys<<<1, 256, 0, st>>>(J, key_out, key_off);
+constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * (kEncStage + kEncScratch);
+
+void encode_kernel_attributes() {
+  cudaFuncSetAttribute(k_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEncSmem);
+}
+
+void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
+  const size_t smem = kEncSmem;
+  // grid-stride over the device-side block count: 3 CTAs per SM x 8 waves,
+  // shared out among the jobs
+  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 3 * 8)),
+                                        bt.B), kEncWarps * 32, smem, st>>>(bt.d);
+}
+void launch_encode_rest(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries * 32, 256, per_job(bt, 148 * 16)), bt.B),
+                                    256, 0, st>>>(bt.d);
+  note_launch(), k_encode_index<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 16)), bt.B), 256,
+                                  0, st>>>(bt.d);
+  note_launch(), k_encode_meta<<<dim3(grid_x(bt.max_cap_files, 128, 1 << 20), bt.B), 128, 0, st>>>(bt.d);
+  note_launch(), k_crc_regions<<<dim3(bt.max_cap_files * 3, bt.B), 256, 0, st>>>(bt.d);
+}
+void launch_file_keys(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_file_keys<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
 }
 
 }  // namespace lc

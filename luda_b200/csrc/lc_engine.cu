@@ -1,15 +1,19 @@
 // Host orchestration and the C ABI (include/luda_b200.h).
 //
-// One job runs as a sequence of kernels on one CUDA stream:
+// Jobs run in batches; a plain compaction is a batch of one.  Every kernel
+// launch covers all jobs of the batch (grid y = job), so a batch costs the
+// same number of launches and host synchronisations as one job:
 //   upload -> table/index parse -> block count -> [sync: entry and key totals]
 //   -> decode -> merge rounds -> drop rule + grandparent cuts -> survivors
-//   -> entry sizes -> block chain -> blocks -> files -> layout
-//   -> [sync: file count and output size] -> encode -> download -> [sync]
+//   -> entry sizes -> block chain -> blocks -> files -> layout -> encode
+//      (one captured CUDA graph, replayed for later batches of the same shape)
+//   -> [sync: file counts and output sizes] -> download -> [sync]
 // Device memory comes from the device's stream-ordered pool (cudaMallocAsync),
 // whose release threshold is raised so freed blocks are reused across jobs.
-// Asynchronous jobs are served by worker threads, one stream each; a job is
-// admitted only while the estimated device memory of the jobs in flight stays
-// under the engine's budget.
+// Asynchronous jobs are served by worker threads, each with its own stream,
+// descriptor array and graph cache; a worker takes every queued job that fits
+// the device budget as one batch, so jobs that arrive while a batch runs are
+// admitted into the next one (continuous batching).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -19,6 +23,8 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -95,7 +101,15 @@ struct PinnedCache {
   }
 };
 
+struct Tunables {
+  uint32_t ctas_per_job = 0;     // grid x of the grid-stride kernels (0: from the sizes)
+  uint32_t merge_items = 8;      // merge-path outputs per thread
+  uint32_t merge_threads = 256;  // threads per merge CTA
+};
+
 }  // namespace
+
+struct lc_slot;
 
 struct lc_engine {
   int device = 0;
@@ -111,26 +125,22 @@ struct lc_engine {
   std::vector<std::thread> workers;
   bool stop = false;
   uint64_t inflight_bytes = 0;
-  std::mutex stream_mu;
-  std::vector<cudaStream_t> free_streams;
-  cudaStream_t get_stream() {
-    {
-      std::lock_guard<std::mutex> g(stream_mu);
-      if (!free_streams.empty()) {
-        cudaStream_t s = free_streams.back();
-        free_streams.pop_back();
-        return s;
-      }
-    }
-    cudaStream_t s;
-    cudaSetDevice(device);
-    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    return s;
+  uint32_t max_batch = 64;
+  bool use_graphs = true;
+  std::mutex tun_mu;
+  Tunables tun;
+  // one slot per worker thread, then slots for synchronous calls (grown on
+  // demand, one per concurrent caller)
+  std::vector<std::unique_ptr<lc_slot>> slots;
+  std::mutex slot_mu;
+  std::vector<lc_slot*> free_slots;
+  lc_slot* take_slot();
+  void put_slot(lc_slot* s);
+  Tunables tuning() {
+    std::lock_guard<std::mutex> g(tun_mu);
+    return tun;
   }
-  void put_stream(cudaStream_t s) {
-    std::lock_guard<std::mutex> g(stream_mu);
-    free_streams.push_back(s);
-  }
+  ~lc_engine();
 };
 
 struct lc_job {
@@ -209,9 +219,9 @@ struct DevAlloc {
     ptrs.push_back(p);
     return (uint8_t*)p;
   }
-  void release(void* keep = nullptr) {
+  void release(const std::vector<void*>& keep) {
     for (void* p : ptrs)
-      if (p != keep) cudaFreeAsync(p, st);
+      if (std::find(keep.begin(), keep.end(), p) == keep.end()) cudaFreeAsync(p, st);
     ptrs.clear();
     cur = nullptr;
     left = 0;
@@ -232,22 +242,41 @@ const char* const kPhaseNames[kNumPhases] = {"upload", "parse", "decode", "merge
 
 struct PhaseTimer {
   bool on = false;
+  bool external = false;  // record as graph nodes while capturing
   cudaStream_t st = nullptr;
   std::vector<std::pair<int, cudaEvent_t>> evs;  // (phase ended here, or -1), in order
+  std::vector<bool> owned;
   PhaseTimer(bool enable, cudaStream_t s) : on(enable), st(s) {}
   ~PhaseTimer() {
-    for (auto& e : evs) cudaEventDestroy(e.second);
+    for (size_t i = 0; i < evs.size(); i++)
+      if (owned[i]) cudaEventDestroy(evs[i].second);
   }
   void record(int tag) {
     if (!on) return;
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
-    CK(cudaEventRecord(e, st));
+    if (external) CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+    else CK(cudaEventRecord(e, st));
     evs.emplace_back(tag, e);
+    owned.push_back(true);
   }
   // a phase runs from the previous recorded event to its mark
   void start() { record(-1); }
   void mark(int p) { record(p); }
+  // events recorded by a replayed graph (owned by the graph)
+  void borrow(const std::vector<std::pair<int, cudaEvent_t>>& g) {
+    for (auto& e : g) {
+      evs.push_back(e);
+      owned.push_back(false);
+    }
+  }
+  // hands the recorded events over (to a graph cache entry)
+  std::vector<std::pair<int, cudaEvent_t>> take() {
+    auto r = evs;
+    evs.clear();
+    owned.clear();
+    return r;
+  }
   void collect(std::vector<float>& out) {
     out.assign(kNumPhases, 0.f);
     if (!on) return;
@@ -297,120 +326,6 @@ uint32_t bloom_k(int bpk) {
 }
 
 // Survivors (k_ids, counters n_kept / n_triggers set) -> encoded files.
-void encode_tail(lc_job* j, JobDev& J, DevAlloc& A, uint64_t N, Counters* hc, cudaStream_t st,
-                 PhaseTimer& T, uint32_t max_klen) {
-  J.k_a = A.get<uint32_t>(N);
-  J.k_b = A.get<uint32_t>(N);
-  J.k_shared = A.get<uint32_t>(N);
-  J.k_next = A.get<uint32_t>(N);
-  J.k_bstart = A.get<uint8_t>(N + 1);
-  J.k_block = A.get<uint32_t>(N + 1);
-  CK(cudaMemsetAsync(J.k_bstart, 0, N + 1, st));
-  J.chunk = kChunk;
-  J.chain_smem_words = 12 * 1024;  // 48 KiB
-  const uint64_t chunks = (N + kChunk - 1) / kChunk + 1;
-  J.chunk_table = A.get<uint32_t>(chunks * kChunk);
-  J.chunk_entry = A.get<uint32_t>(chunks);
-  uint64_t* scratch64 = A.get<uint64_t>(scan_scratch_elems(N + 1));
-  uint32_t* scratch32 = A.get<uint32_t>(scan_scratch_elems(N + 1));
-
-  launch_sizes(J, N, st);
-  launch_next(J, N, st);
-  launch_chain(J, N, st);
-  scan_exclusive<uint8_t, uint32_t>(J.k_bstart, J.k_block, &J.ctr->n_kept, N, scratch32,
-                                    &J.ctr->n_blocks_out, st);
-  J.b_first = A.get<uint32_t>(N + 1);
-  launch_block_list(J, N, st);
-  J.b_size = A.get<uint32_t>(N);
-  uint32_t* tmp32 = A.get<uint32_t>(N);
-  J.b_cum = A.get<uint64_t>(N + 1);
-  launch_block_sizes(J, tmp32, N, st);
-  scan_exclusive<uint32_t, uint64_t>(tmp32, J.b_cum, &J.ctr->n_blocks_out, N, scratch64,
-                                     nullptr, st);
-  J.cap_files = (uint32_t)std::min<uint64_t>(N + 1, 64 + J.cap_triggers +
-                                                         (8 * (J.in_size + J.cap_key_bytes) + N * 64) /
-                                                             std::max<uint64_t>(1, J.max_file_size));
-  J.files = A.get<FileOut>(J.cap_files);
-  J.b_fnext = A.get<uint32_t>(N);
-  J.t_blocks = A.get<uint32_t>(J.cap_triggers);
-  launch_files(J, N, st);
-  J.b_file = A.get<uint32_t>(N);
-  J.b_off = A.get<uint64_t>(N);
-  J.b_isize = A.get<uint32_t>(N);
-  J.b_icum = A.get<uint64_t>(N + 1);
-  J.b_sep = A.get<uint32_t>(N);
-  J.b_ilen = A.get<uint32_t>(N);
-  J.b_gbytes = A.get<uint32_t>(N);
-  J.b_gcum = A.get<uint64_t>(N + 1);
-  J.b_gkeys = A.get<uint32_t>(N);
-  launch_block_layout(J, N, st);
-  scan_exclusive<uint32_t, uint64_t>(J.b_gbytes, J.b_gcum, &J.ctr->n_blocks_out, N, scratch64,
-                                     nullptr, st);
-  scan_exclusive<uint32_t, uint64_t>(J.b_isize, J.b_icum, &J.ctr->n_blocks_out, N, scratch64,
-                                     nullptr, st);
-  // Output capacity, bounded without waiting for the layout: every survivor
-  // costs at most its key, its value and 15 header bytes; every block at most
-  // 4 bytes of restart word per entry, 9 bytes of count and trailer, one index
-  // entry (key + 31) and a filter share; every file 256 bytes of metaindex,
-  // footer and trailers.  The layout kernel checks the real size against it.
-  const uint64_t bpk = j->opt.bits_per_key > 0 ? (uint64_t)j->opt.bits_per_key : 0;
-  J.cap_out = J.in_size + 2 * J.cap_key_bytes + N * (80 + max_klen + (bpk + 7) / 8) +
-              (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
-  J.out = A.own(J.cap_out);
-  launch_file_layout(J, st);
-  check_launch();
-  T.mark(kPartition);
-  launch_encode_blocks(J, N, st);
-  T.mark(kEncodeBlocks);
-  launch_encode_rest(J, N, J.cap_files, st);
-  T.mark(kEncodeMeta);
-  // smallest / largest key of every file, gathered on the device
-  const uint64_t key_cap = 2ull * J.cap_files * max_klen;
-  uint8_t* d_keys = A.get<uint8_t>(key_cap + 1);
-  uint64_t* d_koff = A.get<uint64_t>(2ull * J.cap_files + 1);
-  launch_file_keys(J, J.cap_files, d_keys, d_koff, st);
-  check_launch();
-  std::vector<FileOut> files(J.cap_files);
-  std::vector<uint64_t> koff(2ull * J.cap_files + 1);
-  j->key_bytes.resize(key_cap + 1);
-  CK(cudaMemcpyAsync(hc, J.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(files.data(), J.files, J.cap_files * sizeof(FileOut), cudaMemcpyDeviceToHost,
-                     st));
-  CK(cudaMemcpyAsync(koff.data(), d_koff, koff.size() * 8, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(j->key_bytes.data(), d_keys, key_cap + 1, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  check_counters(*hc);
-  const uint32_t nf = hc->n_files;
-  const uint64_t nbytes = hc->bytes_out;
-  if (!j->outputs_on_device && nbytes) {
-    j->h_out = j->eng->pinned.take(nbytes, &j->h_out_cap);
-    if (!j->h_out) throw StatusError{LC_ERR_NO_MEMORY, "pinned host buffer"};
-    CK(cudaMemcpyAsync(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st));
-  }
-  j->file_offset.resize(nf);
-  j->file_size.resize(nf);
-  j->file_entries.resize(nf);
-  j->small_off.resize(nf);
-  j->large_off.resize(nf);
-  j->small_len.resize(nf);
-  j->large_len.resize(nf);
-  for (uint32_t f = 0; f < nf; f++) {
-    j->file_offset[f] = files[f].out_off;
-    j->file_size[f] = files[f].size;
-    j->file_entries[f] = files[f].end_kept - files[f].first_kept;
-    j->small_off[f] = koff[2 * f];
-    j->small_len[f] = (uint32_t)(koff[2 * f + 1] - koff[2 * f]);
-    j->large_off[f] = koff[2 * f + 1];
-    j->large_len[f] = (uint32_t)(koff[2 * f + 2] - koff[2 * f + 1]);
-  }
-  T.mark(kDownload);
-  j->bytes_out = nbytes;
-  j->entries_out = hc->n_kept;
-  j->kept_key_bytes = hc->kept_key_bytes;
-  j->kept_value_bytes = hc->kept_value_bytes;
-  if (j->outputs_on_device) j->d_out = J.out;
-}
-
 void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   memset(&J, 0, sizeof(J));
   J.block_size = j->opt.block_size;
@@ -422,268 +337,664 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.max_gp_overlap = (int64_t)(10 * j->opt.max_file_size);  // db/version_set.cc:31-33
   J.crc_xpow = e->crc_xpow;
   J.crc_xpow_n = kCrcXpowN;
+  J.chunk = kChunk;
+  J.chain_smem_words = 12 * 1024;  // 48 KiB
 }
 
-void run_compaction(lc_job* j, cudaStream_t st) {
-  lc_engine* e = j->eng;
-  DevAlloc A(st);
-  PhaseTimer T((e->flags & LC_FLAG_PHASE_TIMING) != 0, st);
-  const uint32_t launches0 = launches_on_this_thread();
-  cudaEvent_t ev0, ev1;
-  CK(cudaEventCreate(&ev0));
-  CK(cudaEventCreate(&ev1));
-  try {
-    CK(cudaEventRecord(ev0, st));
-    T.start();
-    JobDev J;
-    fill_common(J, j, e);
-    const uint32_t nt = (uint32_t)j->tables.size();
-    std::vector<TableDesc> td(nt);
-    uint32_t run = 0, in_run = 0;
-    for (uint32_t t = 0; t < nt; t++) {
-      while (run < j->run_counts.size() && in_run >= (uint32_t)j->run_counts[run]) {
-        run++;
-        in_run = 0;
-      }
-      td[t].run = run;
-      td[t].size = j->tables[t].size;
-      in_run++;
-    }
-    J.n_tables = nt;
-    J.n_runs = (uint32_t)j->run_counts.size();
-    // input placement
-    uint8_t* d_in = nullptr;
-    uint64_t in_size = 0;
-    bool zero_copy = false;
-    if (j->inputs_on_device) {
-      uintptr_t lo = ~uintptr_t(0), hi = 0;
-      for (auto& t : j->tables) {
-        lo = std::min(lo, (uintptr_t)t.data);
-        hi = std::max(hi, (uintptr_t)t.data + (uintptr_t)t.size);
-      }
-      if (nt && hi - lo < (1ull << 32)) {
-        zero_copy = true;
-        d_in = (uint8_t*)lo;
-        in_size = hi - lo;
-        for (uint32_t t = 0; t < nt; t++) td[t].off = (uintptr_t)j->tables[t].data - lo;
-      }
-    }
-    if (!zero_copy) {
-      for (uint32_t t = 0; t < nt; t++) {
-        td[t].off = in_size;
-        in_size += round16(td[t].size);
-      }
-      if (in_size >= (1ull << 32))
-        throw StatusError{LC_ERR_UNSUPPORTED, "input of one job must be below 4 GiB"};
-      d_in = A.get<uint8_t>(in_size + 16);
-      for (uint32_t t = 0; t < nt; t++) {
-        if (!j->tables[t].size) continue;
-        CK(cudaMemcpyAsync(d_in + td[t].off, j->tables[t].data, j->tables[t].size,
-                           j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                           st));
-      }
-    }
-    J.in = d_in;
-    J.in_size = in_size;
-    J.in_end = d_in + in_size + (zero_copy ? 0 : 16);
-    TableDesc* d_td = A.get<TableDesc>(nt);
-    CK(cudaMemcpyAsync(d_td, td.data(), nt * sizeof(TableDesc), cudaMemcpyHostToDevice, st));
-    J.tables = d_td;
-    // grandparents
-    J.n_gp = (uint32_t)j->gp_largest.size();
-    {
-      std::vector<uint64_t> off(J.n_gp + 1, 0), pre(J.n_gp + 1, 0);
-      std::string kb;
-      for (uint32_t g = 0; g < J.n_gp; g++) {
-        kb += j->gp_largest[g];
-        off[g + 1] = kb.size();
-        pre[g + 1] = pre[g] + j->gp_size[g];
-      }
-      uint8_t* dk = A.get<uint8_t>(kb.size() + 1);
-      uint64_t* doff = A.get<uint64_t>(off.size());
-      uint64_t* dpre = A.get<uint64_t>(pre.size());
-      if (!kb.empty()) CK(cudaMemcpyAsync(dk, kb.data(), kb.size(), cudaMemcpyHostToDevice, st));
-      CK(cudaMemcpyAsync(doff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
-      CK(cudaMemcpyAsync(dpre, pre.data(), pre.size() * 8, cudaMemcpyHostToDevice, st));
-      J.gp_keys = dk;
-      J.gp_key_off = doff;
-      J.gp_prefix = dpre;
-    }
-    // base-level files, grouped by level (given in level then key order)
-    {
-      const uint32_t nb = (uint32_t)j->base_level.size();
-      std::vector<uint32_t> lvl_begin;
-      std::vector<uint64_t> so(nb), lo_(nb);
-      std::vector<uint32_t> sl(nb), ll(nb);
-      std::string kb;
-      for (uint32_t i = 0; i < nb; i++) {
-        if (i == 0 || j->base_level[i] != j->base_level[i - 1]) lvl_begin.push_back(i);
-        so[i] = kb.size();
-        sl[i] = (uint32_t)j->base_small[i].size();
-        kb += j->base_small[i];
-        lo_[i] = kb.size();
-        ll[i] = (uint32_t)j->base_large[i].size();
-        kb += j->base_large[i];
-      }
-      lvl_begin.push_back(nb);
-      J.n_base_levels = nb ? (uint32_t)lvl_begin.size() - 1 : 0;
-      uint32_t* d_lb = A.get<uint32_t>(lvl_begin.size());
-      uint8_t* d_kb = A.get<uint8_t>(kb.size() + 1);
-      uint64_t* d_so = A.get<uint64_t>(nb + 1);
-      uint64_t* d_lo = A.get<uint64_t>(nb + 1);
-      uint32_t* d_sl = A.get<uint32_t>(nb + 1);
-      uint32_t* d_ll = A.get<uint32_t>(nb + 1);
-      CK(cudaMemcpyAsync(d_lb, lvl_begin.data(), lvl_begin.size() * 4, cudaMemcpyHostToDevice, st));
-      if (nb) {
-        CK(cudaMemcpyAsync(d_kb, kb.data(), kb.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_so, so.data(), nb * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_lo, lo_.data(), nb * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_sl, sl.data(), nb * 4, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_ll, ll.data(), nb * 4, cudaMemcpyHostToDevice, st));
-      }
-      J.base_level_begin = d_lb;
-      J.base_keys = d_kb;
-      J.base_small_off = d_so;
-      J.base_large_off = d_lo;
-      J.base_small_len = d_sl;
-      J.base_large_len = d_ll;
-    }
-    J.ctr = A.get<Counters>(1);
-    CK(cudaMemsetAsync(J.ctr, 0, sizeof(Counters), st));
+uint32_t ceil_log2(uint64_t x) {
+  uint32_t r = 0;
+  while ((1ull << r) < x) r++;
+  return r;
+}
+uint64_t pow2_at_least(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
 
-    // blocks of the input tables (capacity: a data block with its trailer and
-    // index entry takes at least 13 bytes)
-    uint64_t cap_blk = 1;
-    for (auto& t : td) cap_blk += t.size / 13 + 1;
-    J.cap_blocks_in = cap_blk;
-    J.tbl_nblocks = A.get<uint32_t>(nt);
-    J.tbl_block_base = A.get<uint64_t>(nt + 1);
-    J.blk_off = A.get<uint64_t>(cap_blk);
-    J.blk_size = A.get<uint32_t>(cap_blk);
-    J.blk_run = A.get<uint32_t>(cap_blk);
-    J.blk_nent = A.get<uint32_t>(cap_blk);
-    J.blk_ent_base = A.get<uint64_t>(cap_blk + 1);
-    J.blk_kbytes = A.get<uint64_t>(cap_blk);
-    J.blk_key_base = A.get<uint64_t>(cap_blk + 1);
-    uint64_t* scratch = A.get<uint64_t>(scan_scratch_elems(cap_blk + nt + 1));
-    J.run_entry_begin_w = A.get<uint64_t>(J.n_runs + 1);
-    J.run_entry_begin = J.run_entry_begin_w;
+// Host-side state of one job inside a batch.
+struct JobRun {
+  lc_job* j = nullptr;
+  JobDev J;
+  uint64_t cap_blk = 0, N = 0, K = 0;
+  uint32_t max_klen = 8;
+  bool failed = false;
+  Counters hc{};
+  std::vector<FileOut> files;
+  std::vector<uint64_t> koff;
+};
 
-    T.mark(kUpload);
-    Counters hc;
-    if (nt) {
-      launch_table_index_count(J, st);
-      scan_exclusive<uint32_t, uint64_t>(J.tbl_nblocks, J.tbl_block_base, nullptr, nt, scratch,
-                                         &J.ctr->n_blocks_in, st);
-      launch_table_index_entries(J, st);
-      launch_block_count(J, cap_blk, st);
-      scan_exclusive<uint32_t, uint64_t>(J.blk_nent, J.blk_ent_base, &J.ctr->n_blocks_in, cap_blk,
-                                         scratch, &J.ctr->n_entries_in, st);
-      scan_exclusive<uint64_t, uint64_t>(J.blk_kbytes, J.blk_key_base, &J.ctr->n_blocks_in,
-                                         cap_blk, scratch, &J.ctr->key_bytes_in, st);
-    }
-    launch_run_bounds(J, st);
-    check_launch();
-    T.mark(kParse);
-    read_counters(&hc, J.ctr, st);
-    if (hc.n_blocks_in > cap_blk) throw StatusError{LC_ERR_CORRUPT, "more blocks than bytes allow"};
-    const uint64_t N = hc.n_entries_in, K = hc.key_bytes_in;
-    if (N >= (1ull << 32) - 2 || K >= (1ull << 32))
-      throw StatusError{LC_ERR_UNSUPPORTED, "more than 2^32 entries or key bytes in one job"};
-    j->entries_in = N;
-    j->key_bytes_in = K;
+void job_fail(JobRun& r, lc_status s, const std::string& m) {
+  if (r.failed) return;
+  r.failed = true;
+  r.j->status = s;
+  r.j->err = m;
+}
 
-    J.keys = A.get<uint8_t>(K + 16);
-    J.cap_key_bytes = K;
+lc_status counters_status(const Counters& c, std::string* msg) {
+  if (!c.error) return LC_OK;
+  *msg = std::string(err_name(c.error)) + " (detail " + std::to_string(c.error_detail) + ")";
+  return (c.error == kErrLimit || c.error == kErrArenaOverflow) ? LC_ERR_UNSUPPORTED : LC_ERR_CORRUPT;
+}
+
+// Small per-job host arrays packed into one staging buffer and uploaded with
+// one copy; device pointers are fixed up after the upload address is known.
+struct Stage {
+  std::vector<uint8_t> h;
+  template <typename T>
+  uint64_t put(const T* p, uint64_t n) {
+    const uint64_t off = (h.size() + 255) & ~uint64_t(255);
+    h.resize(off + std::max<uint64_t>(n * sizeof(T), 1) + 16);
+    if (n) memcpy(h.data() + off, p, n * sizeof(T));
+    return off;
+  }
+};
+
+// Kernel sequence after the first sync, shared by the compaction and the
+// flush-encoder paths.  Capturable: launches only, no host-side waits.
+void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer& T) {
+  if (decode_merge) {
+    launch_block_decode(bt, st);
+    T.mark(kDecode);
+    launch_merge(bt, st);
+    T.mark(kMerge);
+    launch_drop(bt, st);
+    launch_triggers(bt, st);
+    scan_batch(kScanKeep, bt, bt.max_entries, st);
+    launch_kept_compact(bt, st);
+    T.mark(kDrop);
+  }
+  launch_zero_bstart(bt, st);
+  launch_sizes(bt, st);
+  launch_next(bt, st);
+  launch_chain(bt, st);
+  scan_batch(kScanBstart, bt, bt.max_entries, st);
+  launch_block_list(bt, st);
+  launch_block_sizes(bt, st);
+  scan_batch(kScanBcum, bt, bt.max_entries, st);
+  launch_files(bt, st);
+  launch_block_layout(bt, st);
+  scan_batch(kScanGcum, bt, bt.max_entries, st);
+  scan_batch(kScanIcum, bt, bt.max_entries, st);
+  launch_file_layout(bt, st);
+  T.mark(kPartition);
+  launch_encode_blocks(bt, st);
+  T.mark(kEncodeBlocks);
+  launch_encode_rest(bt, st);
+  launch_file_keys(bt, st);
+  T.mark(kEncodeMeta);
+}
+
+// Allocates the post-parse arrays of one job from its entry count N (and key
+// bytes K for the arena) and fills its descriptor.
+void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
+  JobDev& J = r.J;
+  const uint64_t N = r.N;
+  if (with_merge) {
+    J.keys = A.get<uint8_t>(r.K + 16);
+    J.cap_key_bytes = r.K;
     J.cap_entries = N;
     J.e_koff = A.get<uint32_t>(N);
     J.e_klen = A.get<uint32_t>(N);
     J.e_voff = A.get<uint32_t>(N);
     J.e_vlen = A.get<uint32_t>(N);
     J.e_pfx = A.get<uint64_t>(N);
-    T.start();
-    launch_block_decode(J, hc.n_blocks_in, st);
-    T.mark(kDecode);
-
-    // merge rounds
     J.m_ids = A.get<uint32_t>(N);
     J.m_tmp = A.get<uint32_t>(N);
-    launch_iota(J.m_ids, N, st);
-    uint32_t* src = J.m_ids;
-    uint32_t* dst = J.m_tmp;
-    for (uint32_t w = 1; w < J.n_runs; w *= 2) {
-      launch_merge_round(J, src, dst, w, N, st);
-      std::swap(src, dst);
-    }
-    J.m_ids = src;
-    J.m_tmp = dst;
-    T.mark(kMerge);
-
-    // drop rule, grandparent cuts, survivors
     J.keep = A.get<uint8_t>(N);
     J.gp_idx = A.get<uint32_t>(J.n_gp ? N : 1);
     J.kept_pos = A.get<uint32_t>(N + 1);
-    J.cap_triggers = J.n_gp + 1;
-    J.triggers = A.get<uint32_t>(J.cap_triggers);
+    J.gp_first = A.get<uint32_t>(J.n_gp + 1);
     J.k_ids = A.get<uint32_t>(N);
     J.k_forced = A.get<uint8_t>(N + 1);
-    uint32_t* scratch32 = A.get<uint32_t>(scan_scratch_elems(N + 1));
-    launch_drop(J, N, st);
-    launch_triggers(J, N, A.get<uint32_t>(J.n_gp + 1), st);
-    scan_exclusive<uint8_t, uint32_t>(J.keep, J.kept_pos, &J.ctr->n_entries_in, N, scratch32,
-                                      &J.ctr->n_kept, st);
-    launch_kept_compact(J, N, st);
-    check_launch();
-    T.mark(kDrop);
-    encode_tail(j, J, A, N, &hc, st, T, std::max<uint32_t>(hc.max_klen, 8));
-    CK(cudaEventRecord(ev1, st));
-    CK(cudaStreamSynchronize(st));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    j->device_ms = ms;
-    T.collect(j->phase_ms);
-    j->launches = launches_on_this_thread() - launches0;
-    A.release(j->d_out);
-    CK(cudaStreamSynchronize(st));
-  } catch (...) {
-    cudaStreamSynchronize(st);
-    A.release();
-    j->d_out = nullptr;
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
-    throw;
   }
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
+  J.cap_triggers = J.n_gp + 1;
+  J.triggers = A.get<uint32_t>(J.cap_triggers);
+  J.k_a = A.get<uint32_t>(N);
+  J.k_b = A.get<uint32_t>(N);
+  J.k_shared = A.get<uint32_t>(N);
+  J.k_next = A.get<uint32_t>(N);
+  J.k_bstart = A.get<uint8_t>(N + 1);
+  J.k_block = A.get<uint32_t>(N + 1);
+  const uint64_t chunks = (N + J.chunk - 1) / J.chunk + 1;
+  J.chunk_table = A.get<uint32_t>(chunks * J.chunk);
+  J.chunk_entry = A.get<uint32_t>(chunks);
+  J.b_first = A.get<uint32_t>(N + 1);
+  J.b_size = A.get<uint32_t>(N);
+  J.tmp32 = A.get<uint32_t>(N);
+  J.b_cum = A.get<uint64_t>(N + 1);
+  J.cap_files = (uint32_t)std::min<uint64_t>(
+      N + 1, 64 + J.cap_triggers +
+                 (8 * (J.in_size + J.cap_key_bytes) + N * 64) / std::max<uint64_t>(1, J.max_file_size));
+  J.files = A.get<FileOut>(J.cap_files);
+  J.b_fnext = A.get<uint32_t>(N);
+  J.t_blocks = A.get<uint32_t>(J.cap_triggers);
+  J.b_file = A.get<uint32_t>(N);
+  J.b_off = A.get<uint64_t>(N);
+  J.b_isize = A.get<uint32_t>(N);
+  J.b_icum = A.get<uint64_t>(N + 1);
+  J.b_sep = A.get<uint32_t>(N);
+  J.b_ilen = A.get<uint32_t>(N);
+  J.b_gbytes = A.get<uint32_t>(N);
+  J.b_gcum = A.get<uint64_t>(N + 1);
+  J.b_gkeys = A.get<uint32_t>(N);
+  // Output capacity, bounded without waiting for the layout: every survivor
+  // costs at most its key, its value and 15 header bytes; every block at most
+  // 4 bytes of restart word per entry, 9 bytes of count and trailer, one index
+  // entry (key + 31) and a filter share; every file 256 bytes of metaindex,
+  // footer and trailers.  The layout kernel checks the real size against it.
+  const uint64_t bpk = J.bits_per_key > 0 ? (uint64_t)J.bits_per_key : 0;
+  J.cap_out = J.in_size + 2 * J.cap_key_bytes + N * (80 + r.max_klen + (bpk + 7) / 8) +
+              (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
+  J.out = A.own(J.cap_out);
+  J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
+  J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
+  J.cap_scan = N + 1;
+  J.scan_scratch = A.get<uint64_t>(scan_scratch_elems(N + 1));
 }
 
-void run_build(lc_job* j, cudaStream_t st) {
-  lc_engine* e = j->eng;
+}  // namespace
+
+// One set of device resources per thread that runs batches: a stream, a
+// persistent device array of job descriptors (so that captured graphs can be
+// replayed for other batches), and the graph cache.
+struct lc_slot {
+  cudaStream_t st = nullptr;
+  JobDev* d_jobs = nullptr;
+  uint32_t cap = 0;
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t uses = 0;
+    uint32_t launches = 0;  // kernels in the graph
+    std::vector<std::pair<int, cudaEvent_t>> events;  // phase marks inside the graph
+  };
+  std::map<std::string, GraphEntry> graphs;
+  uint64_t tick = 0;
+  void init(int device, uint32_t capacity) {
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cap = capacity;
+    CK(cudaMalloc(&d_jobs, sizeof(JobDev) * cap));
+  }
+  void destroy() {
+    for (auto& g : graphs) {
+      cudaGraphExecDestroy(g.second.exec);
+      for (auto& ev : g.second.events) cudaEventDestroy(ev.second);
+    }
+    graphs.clear();
+    if (d_jobs) cudaFree(d_jobs);
+    if (st) cudaStreamDestroy(st);
+    d_jobs = nullptr;
+    st = nullptr;
+  }
+  // Launches the post-parse sequence for `bt`, through a cached graph when
+  // one exists for the same grid shapes, else by capturing one.
+  void run_tail(const Batch& bt, bool decode_merge, bool use_graph, PhaseTimer& T) {
+    if (!use_graph) {
+      launch_tail(bt, decode_merge, st, T);
+      CK(cudaGetLastError());
+      return;
+    }
+    char key[256];
+    snprintf(key, sizeof(key), "%d|%d|%u|%u|%u|%u|%u|%llu|%llu|%u|%u|%u|%u|%u", (int)T.on,
+             (int)decode_merge, bt.B, bt.max_tables, bt.max_gp, bt.max_cap_triggers,
+             bt.max_cap_files, (unsigned long long)bt.max_blocks_in,
+             (unsigned long long)bt.max_entries, bt.merge_rounds, bt.chunk, bt.ctas_per_job,
+             bt.merge_items, bt.merge_threads);
+    auto it = graphs.find(key);
+    bool fresh = false;
+    if (it == graphs.end()) {
+      if (graphs.size() >= 24) {  // evict the least recently used
+        auto victim = graphs.begin();
+        for (auto g = graphs.begin(); g != graphs.end(); ++g)
+          if (g->second.uses < victim->second.uses) victim = g;
+        cudaGraphExecDestroy(victim->second.exec);
+        for (auto& ev : victim->second.events) cudaEventDestroy(ev.second);
+        graphs.erase(victim);
+      }
+      cudaGraph_t g;
+      PhaseTimer Tc(T.on, st);
+      Tc.external = true;
+      const uint32_t l0 = launches_on_this_thread();
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      launch_tail(bt, decode_merge, st, Tc);
+      cudaError_t le = cudaGetLastError();
+      cudaError_t ee = cudaStreamEndCapture(st, &g);
+      CK(le);
+      CK(ee);
+      GraphEntry ge;
+      ge.launches = launches_on_this_thread() - l0;  // counted once, at capture
+      ge.events = Tc.take();
+      cudaError_t ie = cudaGraphInstantiate(&ge.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        for (auto& ev : ge.events) cudaEventDestroy(ev.second);
+        CK(ie);
+      }
+      it = graphs.emplace(key, ge).first;
+      fresh = true;
+    }
+    it->second.uses = ++tick;
+    CK(cudaGraphLaunch(it->second.exec, st));
+    if (!fresh) note_launch(it->second.launches);
+    T.borrow(it->second.events);
+  }
+};
+
+lc_slot* lc_engine::take_slot() {
+  std::lock_guard<std::mutex> g(slot_mu);
+  if (!free_slots.empty()) {
+    lc_slot* r = free_slots.back();
+    free_slots.pop_back();
+    return r;
+  }
+  std::unique_ptr<lc_slot> n(new lc_slot());
+  n->init(device, max_batch);
+  slots.push_back(std::move(n));
+  return slots.back().get();
+}
+
+void lc_engine::put_slot(lc_slot* s) {
+  std::lock_guard<std::mutex> g(slot_mu);
+  free_slots.push_back(s);
+}
+
+lc_engine::~lc_engine() {
+  cudaSetDevice(device);
+  for (auto& sl : slots) sl->destroy();
+}
+
+namespace {
+
+// Runs a batch of compaction jobs (kind 0) on one slot.  Per-job failures are
+// recorded in the job; CUDA failures fail the whole batch.
+void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
+  if (jobs.empty()) return;
+  lc_engine* e = jobs[0]->eng;
+  cudaStream_t st = slot.st;
   DevAlloc A(st);
   PhaseTimer T((e->flags & LC_FLAG_PHASE_TIMING) != 0, st);
   const uint32_t launches0 = launches_on_this_thread();
+  const uint32_t B = (uint32_t)jobs.size();
+  if (B > slot.cap) {  // callers split batches at the slot's capacity
+    for (auto* j : jobs) {
+      j->status = LC_ERR_INVALID_ARG;
+      j->err = "batch larger than the engine's max_batch_jobs";
+    }
+    return;
+  }
+  std::vector<JobRun> runs(B);
   cudaEvent_t ev0, ev1;
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
   try {
     CK(cudaEventRecord(ev0, st));
     T.start();
-    JobDev J;
-    fill_common(J, j, e);
+    // ---- set-up: descriptors, input placement, small arrays
+    Stage S;
+    uint64_t in_total = 0;
+    std::vector<std::vector<TableDesc>> tds(B);
+    std::vector<uint64_t> in_base(B, 0);
+    std::vector<bool> zero_copy(B, false);
+    struct Offs {
+      uint64_t td, gpk, gpo, gpp, lb, bk, bso, blo, bsl, bll;
+    };
+    std::vector<Offs> offs(B);
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      lc_job* j = jobs[i];
+      r.j = j;
+      fill_common(r.J, j, e);
+      JobDev& J = r.J;
+      const uint32_t nt = (uint32_t)j->tables.size();
+      auto& td = tds[i];
+      td.resize(nt);
+      uint32_t run = 0, in_run = 0;
+      for (uint32_t t = 0; t < nt; t++) {
+        while (run < j->run_counts.size() && in_run >= (uint32_t)j->run_counts[run]) {
+          run++;
+          in_run = 0;
+        }
+        td[t].run = run;
+        td[t].size = j->tables[t].size;
+        in_run++;
+      }
+      J.n_tables = nt;
+      J.n_runs = (uint32_t)j->run_counts.size();
+      uint64_t in_size = 0;
+      if (j->inputs_on_device) {
+        uintptr_t lo = ~uintptr_t(0), hi = 0;
+        for (auto& t : j->tables) {
+          lo = std::min(lo, (uintptr_t)t.data);
+          hi = std::max(hi, (uintptr_t)t.data + (uintptr_t)t.size);
+        }
+        if (nt && hi - lo < (1ull << 32)) {
+          zero_copy[i] = true;
+          J.in = (const uint8_t*)lo;
+          in_size = hi - lo;
+          for (uint32_t t = 0; t < nt; t++) td[t].off = (uintptr_t)j->tables[t].data - lo;
+        }
+      }
+      if (!zero_copy[i]) {
+        for (uint32_t t = 0; t < nt; t++) {
+          td[t].off = in_size;
+          in_size += round16(td[t].size);
+        }
+        if (in_size >= (1ull << 32)) {
+          job_fail(r, LC_ERR_UNSUPPORTED, "input of one job must be below 4 GiB");
+          in_size = 0;
+        }
+        in_base[i] = in_total;
+        in_total += in_size + 16;
+      }
+      J.in_size = in_size;
+      uint64_t cap_blk = 1;
+      for (auto& t : td) cap_blk += t.size / 13 + 1;
+      r.cap_blk = cap_blk;
+      // grandparents: largest keys, offsets, size prefix
+      J.n_gp = (uint32_t)j->gp_largest.size();
+      std::vector<uint64_t> gpo(J.n_gp + 1, 0), gpp(J.n_gp + 1, 0);
+      std::string gpk;
+      for (uint32_t g = 0; g < J.n_gp; g++) {
+        gpk += j->gp_largest[g];
+        gpo[g + 1] = gpk.size();
+        gpp[g + 1] = gpp[g] + j->gp_size[g];
+      }
+      // base-level files, grouped by level
+      const uint32_t nb = (uint32_t)j->base_level.size();
+      std::vector<uint32_t> lb;
+      std::vector<uint64_t> so(nb), lo_(nb);
+      std::vector<uint32_t> sl(nb), ll(nb);
+      std::string bk;
+      for (uint32_t f = 0; f < nb; f++) {
+        if (f == 0 || j->base_level[f] != j->base_level[f - 1]) lb.push_back(f);
+        so[f] = bk.size();
+        sl[f] = (uint32_t)j->base_small[f].size();
+        bk += j->base_small[f];
+        lo_[f] = bk.size();
+        ll[f] = (uint32_t)j->base_large[f].size();
+        bk += j->base_large[f];
+      }
+      lb.push_back(nb);
+      J.n_base_levels = nb ? (uint32_t)lb.size() - 1 : 0;
+      Offs& o = offs[i];
+      o.td = S.put(td.data(), nt);
+      o.gpk = S.put(gpk.data(), gpk.size());
+      o.gpo = S.put(gpo.data(), gpo.size());
+      o.gpp = S.put(gpp.data(), gpp.size());
+      o.lb = S.put(lb.data(), lb.size());
+      o.bk = S.put(bk.data(), bk.size());
+      o.bso = S.put(so.data(), nb);
+      o.blo = S.put(lo_.data(), nb);
+      o.bsl = S.put(sl.data(), nb);
+      o.bll = S.put(ll.data(), nb);
+    }
+    uint8_t* d_stage = A.get<uint8_t>(S.h.size());
+    CK(cudaMemcpyAsync(d_stage, S.h.data(), S.h.size(), cudaMemcpyHostToDevice, st));
+    uint8_t* d_in_all = in_total ? A.get<uint8_t>(in_total) : nullptr;
+    Counters* d_ctr = A.get<Counters>(B);
+    CK(cudaMemsetAsync(d_ctr, 0, sizeof(Counters) * B, st));
+    uint64_t zero_word_off = S.h.size();  // (unused) keeps Stage layout stable
+    (void)zero_word_off;
+    Batch bt;
+    bt.d = slot.d_jobs;
+    bt.B = B;
+    bt.chunk = kChunk;
+    bt.ctas_per_job = tun.ctas_per_job;
+    bt.merge_items = tun.merge_items;
+    bt.merge_threads = tun.merge_threads;
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      JobDev& J = r.J;
+      lc_job* j = jobs[i];
+      const Offs& o = offs[i];
+      if (!zero_copy[i]) {
+        J.in = d_in_all + in_base[i];
+        for (uint32_t t = 0; t < J.n_tables && !r.failed; t++) {
+          if (!j->tables[t].size) continue;
+          CK(cudaMemcpyAsync((uint8_t*)J.in + tds[i][t].off, j->tables[t].data, j->tables[t].size,
+                             j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                             st));
+        }
+      }
+      J.in_end = J.in + J.in_size + (zero_copy[i] ? 0 : 16);
+      J.tables = (const TableDesc*)(d_stage + o.td);
+      J.gp_keys = d_stage + o.gpk;
+      J.gp_key_off = (const uint64_t*)(d_stage + o.gpo);
+      J.gp_prefix = (const uint64_t*)(d_stage + o.gpp);
+      J.base_level_begin = (const uint32_t*)(d_stage + o.lb);
+      J.base_keys = d_stage + o.bk;
+      J.base_small_off = (const uint64_t*)(d_stage + o.bso);
+      J.base_large_off = (const uint64_t*)(d_stage + o.blo);
+      J.base_small_len = (const uint32_t*)(d_stage + o.bsl);
+      J.base_large_len = (const uint32_t*)(d_stage + o.bll);
+      J.ctr = d_ctr + i;
+      if (r.failed) {
+        J.n_tables = 0;
+        J.n_runs = 0;
+      }
+      const uint64_t cap_blk = r.cap_blk;
+      J.cap_blocks_in = cap_blk;
+      J.tbl_nblocks = A.get<uint32_t>(J.n_tables);
+      J.tbl_block_base = A.get<uint64_t>(J.n_tables + 1);
+      J.blk_off = A.get<uint64_t>(cap_blk);
+      J.blk_size = A.get<uint32_t>(cap_blk);
+      J.blk_run = A.get<uint32_t>(cap_blk);
+      J.blk_nent = A.get<uint32_t>(cap_blk);
+      J.blk_ent_base = A.get<uint64_t>(cap_blk + 1);
+      J.blk_kbytes = A.get<uint64_t>(cap_blk);
+      J.blk_key_base = A.get<uint64_t>(cap_blk + 1);
+      J.scan_scratch = A.get<uint64_t>(scan_scratch_elems(cap_blk + J.n_tables + 1));
+      J.run_entry_begin_w = A.get<uint64_t>(J.n_runs + 1);
+      J.run_entry_begin = J.run_entry_begin_w;
+      bt.max_tables = std::max(bt.max_tables, J.n_tables);
+      bt.max_blocks_in = std::max(bt.max_blocks_in, cap_blk);
+    }
+    std::vector<JobDev> hj(B);
+    for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
+    CK(cudaMemcpyAsync(slot.d_jobs, hj.data(), sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
+    T.mark(kUpload);
+    // ---- parse: index blocks, block restart runs, entry and key totals
+    if (bt.max_tables) {
+      launch_table_index_count(bt, st);
+      scan_batch(kScanTblBlocks, bt, bt.max_tables, st);
+      launch_table_index_entries(bt, st);
+      launch_block_count(bt, st);
+      scan_batch(kScanBlkEnt, bt, bt.max_blocks_in, st);
+      scan_batch(kScanBlkKey, bt, bt.max_blocks_in, st);
+    }
+    launch_run_bounds(bt, st);
+    CK(cudaGetLastError());
+    T.mark(kParse);
+    std::vector<Counters> hc(B);
+    CK(cudaMemcpyAsync(hc.data(), d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // ---- allocate the rest from the totals
+    bool any_zeroed = false;
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      std::string m;
+      lc_status s = counters_status(hc[i], &m);
+      if (s != LC_OK) job_fail(r, s, m);
+      if (!r.failed && hc[i].n_blocks_in > r.cap_blk)
+        job_fail(r, LC_ERR_CORRUPT, "more blocks than bytes allow");
+      if (!r.failed && (hc[i].n_entries_in >= (1ull << 32) - 2 || hc[i].key_bytes_in >= (1ull << 32)))
+        job_fail(r, LC_ERR_UNSUPPORTED, "more than 2^32 entries or key bytes in one job");
+      if (r.failed) {
+        // a failed job does no more work: zero counts, no merge children
+        hc[i] = Counters{};
+        hc[i].error = kErrLimit;
+        r.J.n_runs = 0;
+        r.J.n_gp = 0;
+        any_zeroed = true;
+      }
+      r.N = r.failed ? 0 : hc[i].n_entries_in;
+      r.K = r.failed ? 0 : hc[i].key_bytes_in;
+      r.max_klen = std::max<uint32_t>(hc[i].max_klen, 8);
+      r.j->entries_in = r.N;
+      r.j->key_bytes_in = r.K;
+    }
+    if (any_zeroed) {
+      CK(cudaMemcpyAsync(d_ctr, hc.data(), sizeof(Counters) * B, cudaMemcpyHostToDevice, st));
+    }
+    uint32_t max_runs = 1;
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      alloc_tail(r, A, true);
+      if (r.failed) {
+        // run_entry_begin[0] must read 0 for the merge kernels
+        CK(cudaMemsetAsync(r.J.run_entry_begin_w, 0, 8, st));
+      }
+      max_runs = std::max<uint32_t>(max_runs, r.J.n_runs);
+      bt.max_entries = std::max<uint64_t>(bt.max_entries, r.N);
+      bt.max_gp = std::max<uint32_t>(bt.max_gp, r.J.n_gp);
+      bt.max_cap_triggers = std::max<uint32_t>(bt.max_cap_triggers, r.J.cap_triggers);
+      bt.max_cap_files = std::max<uint32_t>(bt.max_cap_files, r.J.cap_files);
+    }
+    // grid shapes in powers of two, so that batches of similar size share a
+    // captured graph (the kernels loop over whatever the grid leaves)
+    bt.max_entries = pow2_at_least(std::max<uint64_t>(bt.max_entries, 1));
+    bt.max_blocks_in = pow2_at_least(bt.max_blocks_in);  // decode grid size only
+    bt.max_cap_files = (uint32_t)pow2_at_least(bt.max_cap_files);
+    bt.max_cap_triggers = (uint32_t)pow2_at_least(bt.max_cap_triggers);
+    bt.max_gp = bt.max_gp ? (uint32_t)pow2_at_least(bt.max_gp + 1) - 1 : 0;
+    bt.merge_rounds = ceil_log2(max_runs);
+    for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
+    CK(cudaMemcpyAsync(slot.d_jobs, hj.data(), sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
+    T.start();
+    // ---- decode, merge, drop, partition, encode: one graph launch
+    slot.run_tail(bt, true, e->use_graphs, T);
+    // ---- per-job results
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      r.files.resize(r.J.cap_files);
+      r.koff.resize(2ull * r.J.cap_files + 1);
+      r.j->key_bytes.resize(2ull * r.J.cap_files * r.max_klen + 1);
+      CK(cudaMemcpyAsync(r.files.data(), r.J.files, r.J.cap_files * sizeof(FileOut),
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(r.koff.data(), r.J.fkoff, r.koff.size() * 8, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(r.j->key_bytes.data(), r.J.fkeys, r.j->key_bytes.size(),
+                         cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaMemcpyAsync(hc.data(), d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < B; i++) {
+      JobRun& r = runs[i];
+      if (r.failed) continue;
+      std::string m;
+      lc_status s = counters_status(hc[i], &m);
+      if (s != LC_OK) {
+        job_fail(r, s, m);
+        continue;
+      }
+      lc_job* j = r.j;
+      const uint64_t nbytes = hc[i].bytes_out;
+      if (!j->outputs_on_device && nbytes) {
+        j->h_out = e->pinned.take(nbytes, &j->h_out_cap);
+        if (!j->h_out) {
+          job_fail(r, LC_ERR_NO_MEMORY, "pinned host buffer");
+          continue;
+        }
+        CK(cudaMemcpyAsync(j->h_out, r.J.out, nbytes, cudaMemcpyDeviceToHost, st));
+      }
+      const uint32_t nf = hc[i].n_files;
+      j->file_offset.resize(nf);
+      j->file_size.resize(nf);
+      j->file_entries.resize(nf);
+      j->small_off.resize(nf);
+      j->large_off.resize(nf);
+      j->small_len.resize(nf);
+      j->large_len.resize(nf);
+      for (uint32_t f = 0; f < nf; f++) {
+        const FileOut& F = r.files[f];
+        j->file_offset[f] = F.out_off;
+        j->file_size[f] = F.size;
+        j->file_entries[f] = F.end_kept - F.first_kept;
+        j->small_off[f] = r.koff[2 * f];
+        j->small_len[f] = (uint32_t)(r.koff[2 * f + 1] - r.koff[2 * f]);
+        j->large_off[f] = r.koff[2 * f + 1];
+        j->large_len[f] = (uint32_t)(r.koff[2 * f + 2] - r.koff[2 * f + 1]);
+      }
+      j->bytes_out = nbytes;
+      j->entries_out = hc[i].n_kept;
+      j->kept_key_bytes = hc[i].kept_key_bytes;
+      j->kept_value_bytes = hc[i].kept_value_bytes;
+      if (j->outputs_on_device) j->d_out = r.J.out;
+    }
+    T.mark(kDownload);
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    std::vector<float> ph;
+    T.collect(ph);
+    const uint32_t launches = launches_on_this_thread() - launches0;
+    std::vector<void*> keep;
+    for (uint32_t i = 0; i < B; i++) {
+      lc_job* j = jobs[i];
+      j->device_ms = ms;
+      j->phase_ms = ph;
+      j->launches = launches;
+      if (!runs[i].failed) j->status = LC_OK;
+      if (j->d_out) keep.push_back(j->d_out);
+    }
+    A.release(keep);
+    CK(cudaStreamSynchronize(st));
+  } catch (const CudaError& ce) {
+    cudaStreamSynchronize(st);
+    A.release({});
+    for (auto* j : jobs) {
+      j->d_out = nullptr;
+      j->status = LC_ERR_CUDA;
+      j->err = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
+    }
+  } catch (const StatusError& se) {
+    cudaStreamSynchronize(st);
+    A.release({});
+    for (auto* j : jobs) {
+      j->d_out = nullptr;
+      j->status = se.s;
+      j->err = se.msg;
+    }
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+}
+
+// Flush encoder: one table from sorted entries (kind 1), a batch of one that
+// skips decode, merge and the drop rule.
+void run_build(lc_job* j, lc_slot& slot) {
+  lc_engine* e = j->eng;
+  cudaStream_t st = slot.st;
+  DevAlloc A(st);
+  PhaseTimer T((e->flags & LC_FLAG_PHASE_TIMING) != 0, st);
+  const uint32_t launches0 = launches_on_this_thread();
+  try {
+    T.start();
+    JobRun r;
+    r.j = j;
+    fill_common(r.J, j, e);
+    JobDev& J = r.J;
     J.max_file_size = ~0ull;  // BuildTable writes one file
     J.max_gp_overlap = 0;
     const uint64_t N = (uint64_t)j->bn;
-    uint64_t kb, vb;
+    std::vector<uint64_t> hk;
+    const uint64_t* ko = j->bkoffs;
+    uint64_t vb;
     if (j->inputs_on_device) {
-      CK(cudaMemcpyAsync(&kb, j->bkoffs + N, 8, cudaMemcpyDeviceToHost, st));
+      hk.resize(N + 1);
+      CK(cudaMemcpyAsync(hk.data(), j->bkoffs, (N + 1) * 8, cudaMemcpyDeviceToHost, st));
       CK(cudaMemcpyAsync(&vb, j->bvoffs + N, 8, cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
+      ko = hk.data();
     } else {
-      kb = j->bkoffs[N];
       vb = j->bvoffs[N];
     }
+    const uint64_t kb = ko[N];
     if (kb >= (1ull << 32) || vb >= (1ull << 32) || N >= (1ull << 32) - 2)
       throw StatusError{LC_ERR_UNSUPPORTED, "table input beyond 4 GiB"};
+    for (uint64_t i = 0; i < N; i++)
+      r.max_klen = std::max<uint32_t>(r.max_klen, (uint32_t)(ko[i + 1] - ko[i]));
     const cudaMemcpyKind kind = j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     J.keys = A.get<uint8_t>(kb + 16);
     uint8_t* d_vals = A.get<uint8_t>(vb + 16);
@@ -696,10 +1007,11 @@ void run_build(lc_job* j, cudaStream_t st) {
     J.in = d_vals;
     J.in_size = vb;
     J.in_end = d_vals + vb + 16;
+    J.src_koffs = d_ko;
+    J.src_voffs = d_vo;
     J.cap_key_bytes = kb;
     J.cap_entries = N;
     J.ctr = A.get<Counters>(1);
-    CK(cudaMemsetAsync(J.ctr, 0, sizeof(Counters), st));
     Counters init{};
     init.n_kept = N;
     init.n_entries_in = N;
@@ -712,66 +1024,81 @@ void run_build(lc_job* j, cudaStream_t st) {
     J.k_ids = A.get<uint32_t>(N);
     J.k_forced = A.get<uint8_t>(N + 1);
     CK(cudaMemsetAsync(J.k_forced, 0, N + 1, st));
-    J.cap_triggers = 1;
-    J.triggers = A.get<uint32_t>(1);
     J.kept_pos = A.get<uint32_t>(N + 1);
+    r.N = N;
+    r.K = kb;
+    alloc_tail(r, A, false);
+    CK(cudaMemcpyAsync(slot.d_jobs, &J, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    Batch bt;
+    bt.d = slot.d_jobs;
+    bt.B = 1;
+    bt.max_entries = std::max<uint64_t>(N, 1);
+    bt.max_cap_files = J.cap_files;
+    bt.max_cap_triggers = J.cap_triggers;
     T.mark(kUpload);
-    launch_entries_from_offsets(J, d_ko, d_vo, N, st);
-    check_launch();
-    T.mark(kDrop);
+    launch_entries_from_offsets(bt, st);
+    CK(cudaGetLastError());
+    launch_tail(bt, false, st, T);
+    CK(cudaGetLastError());
     Counters hc;
+    r.files.resize(J.cap_files);
+    r.koff.resize(2ull * J.cap_files + 1);
+    j->key_bytes.resize(2ull * J.cap_files * r.max_klen + 1);
+    CK(cudaMemcpyAsync(&hc, J.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(r.files.data(), J.files, J.cap_files * sizeof(FileOut), cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaMemcpyAsync(r.koff.data(), J.fkoff, r.koff.size() * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(j->key_bytes.data(), J.fkeys, j->key_bytes.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::string m;
+    lc_status s = counters_status(hc, &m);
+    if (s != LC_OK) throw StatusError{s, m};
+    const uint64_t nbytes = hc.bytes_out;
+    if (nbytes) {
+      j->h_out = e->pinned.take(nbytes, &j->h_out_cap);
+      if (!j->h_out) throw StatusError{LC_ERR_NO_MEMORY, "pinned host buffer"};
+      CK(cudaMemcpyAsync(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st));
+    }
+    const uint32_t nf = hc.n_files;
+    j->file_offset.resize(nf);
+    j->file_size.resize(nf);
+    j->file_entries.resize(nf);
+    j->small_off.resize(nf);
+    j->large_off.resize(nf);
+    j->small_len.resize(nf);
+    j->large_len.resize(nf);
+    for (uint32_t f = 0; f < nf; f++) {
+      j->file_offset[f] = r.files[f].out_off;
+      j->file_size[f] = r.files[f].size;
+      j->file_entries[f] = r.files[f].end_kept - r.files[f].first_kept;
+      j->small_off[f] = r.koff[2 * f];
+      j->small_len[f] = (uint32_t)(r.koff[2 * f + 1] - r.koff[2 * f]);
+      j->large_off[f] = r.koff[2 * f + 1];
+      j->large_len[f] = (uint32_t)(r.koff[2 * f + 2] - r.koff[2 * f + 1]);
+    }
+    T.mark(kDownload);
+    CK(cudaStreamSynchronize(st));
     j->entries_in = N;
     j->key_bytes_in = kb;
-    uint32_t max_klen = 8;
-    {
-      std::vector<uint64_t> hk;
-      const uint64_t* ko = j->bkoffs;
-      if (j->inputs_on_device) {
-        hk.resize(N + 1);
-        CK(cudaMemcpyAsync(hk.data(), j->bkoffs, (N + 1) * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        ko = hk.data();
-      }
-      for (uint64_t i = 0; i < N; i++)
-        max_klen = std::max<uint32_t>(max_klen, (uint32_t)(ko[i + 1] - ko[i]));
-    }
-    encode_tail(j, J, A, N, &hc, st, T, max_klen);
-    CK(cudaEventRecord(ev1, st));
-    CK(cudaStreamSynchronize(st));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    j->device_ms = ms;
+    j->bytes_out = nbytes;
+    j->entries_out = hc.n_kept;
+    j->kept_key_bytes = hc.kept_key_bytes;
+    j->kept_value_bytes = hc.kept_value_bytes;
     T.collect(j->phase_ms);
     j->launches = launches_on_this_thread() - launches0;
-    A.release(j->d_out);
-    CK(cudaStreamSynchronize(st));
-  } catch (...) {
-    cudaStreamSynchronize(st);
-    A.release();
-    j->d_out = nullptr;
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
-    throw;
-  }
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
-}
-
-void execute(lc_job* j, cudaStream_t st) {
-  try {
-    CK(cudaSetDevice(j->eng->device));
-    if (j->kind == 0) run_compaction(j, st);
-    else run_build(j, st);
     j->status = LC_OK;
+    A.release({});
+    CK(cudaStreamSynchronize(st));
   } catch (const CudaError& ce) {
+    cudaStreamSynchronize(st);
+    A.release({});
     j->status = LC_ERR_CUDA;
     j->err = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
   } catch (const StatusError& se) {
+    cudaStreamSynchronize(st);
+    A.release({});
     j->status = se.s;
     j->err = se.msg;
-  } catch (const std::bad_alloc&) {
-    j->status = LC_ERR_NO_MEMORY;
-    j->err = "host allocation failed";
   }
 }
 
@@ -788,40 +1115,55 @@ void finish(lc_job* j) {
   j->cv.notify_all();
 }
 
-void worker_main(lc_engine* e) {
-  cudaSetDevice(e->device);
-  cudaStream_t st;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+// Worker: takes the head of the queue plus every further queued job that
+// still fits the device budget (up to max_batch) and runs them as one batch.
+// Jobs that arrive while a batch is on the device join the next one.
+void worker_main(lc_engine* e, lc_slot* wslot) {
+  lc_slot& slot = *wslot;
   while (true) {
-    lc_job* j = nullptr;
+    std::vector<lc_job*> batch;
+    uint64_t bytes = 0;
     {
       std::unique_lock<std::mutex> lk(e->mu);
       e->cv.wait(lk, [&] { return e->stop || !e->queue.empty(); });
       if (e->stop && e->queue.empty()) break;
-      // admission against the device budget (head of line first)
       lc_job* head = e->queue.front();
       e->admit_cv.wait(lk, [&] {
         return e->stop || e->inflight_bytes == 0 || e->inflight_bytes + head->est_bytes <= e->budget;
       });
       if (e->queue.empty() || e->queue.front() != head) continue;
-      e->queue.pop_front();
-      j = head;
-      e->inflight_bytes += j->est_bytes;
+      while (!e->queue.empty() && batch.size() < e->max_batch) {
+        lc_job* j = e->queue.front();
+        if (j->kind != 0) {
+          if (batch.empty()) {
+            batch.push_back(j);
+            bytes += j->est_bytes;
+            e->queue.pop_front();
+          }
+          break;
+        }
+        if (!batch.empty() && e->inflight_bytes + bytes + j->est_bytes > e->budget) break;
+        batch.push_back(j);
+        bytes += j->est_bytes;
+        e->queue.pop_front();
+      }
+      e->inflight_bytes += bytes;
     }
     if (e->stop) {
-      j->status = LC_ERR_SHUTDOWN;
+      for (auto* j : batch) j->status = LC_ERR_SHUTDOWN;
     } else {
-      execute(j, st);
+      cudaSetDevice(e->device);
+      if (batch.size() == 1 && batch[0]->kind == 1) run_build(batch[0], slot);
+      else run_batch(batch, slot, e->tuning());
     }
     {
       std::lock_guard<std::mutex> g(e->mu);
-      e->inflight_bytes -= j->est_bytes;
+      e->inflight_bytes -= bytes;
     }
     e->admit_cv.notify_all();
     e->cv.notify_all();
-    finish(j);
+    for (auto* j : batch) finish(j);
   }
-  cudaStreamDestroy(st);
 }
 
 lc_status fail(lc_status s, const std::string& msg) {
@@ -936,24 +1278,37 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     e->device = cfg->device;
     if (cfg->device_budget_bytes) e->budget = cfg->device_budget_bytes;
     if (cfg->max_inflight_jobs > 0) e->max_inflight = cfg->max_inflight_jobs;
+    if (cfg->max_batch_jobs > 0) e->max_batch = (uint32_t)cfg->max_batch_jobs;
     e->flags = cfg->flags;
+    e->use_graphs = (cfg->flags & LC_FLAG_NO_GRAPHS) == 0;
   }
+  std::vector<lc_slot*> wslots;
   try {
     CK(cudaSetDevice(e->device));
     cudaMemPool_t pool;
     CK(cudaDeviceGetDefaultMemPool(&pool, e->device));
     uint64_t thr = ~0ull;
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    decode_kernel_attributes();
+    encode_kernel_attributes();
+    CK(cudaGetLastError());
     std::vector<uint32_t> t;
     host_crc_xpow(t);
     CK(cudaMalloc(&e->crc_xpow, t.size() * 4));
     CK(cudaMemcpy(e->crc_xpow, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    for (int i = 0; i < e->max_inflight; i++) {
+      std::unique_ptr<lc_slot> sl(new lc_slot());
+      sl->init(e->device, e->max_batch);
+      wslots.push_back(sl.get());
+      e->slots.push_back(std::move(sl));
+    }
   } catch (const CudaError& ce) {
     std::string m = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
+    if (e->crc_xpow) cudaFree(e->crc_xpow);
     delete e;
     return fail(LC_ERR_CUDA, m);
   }
-  for (int i = 0; i < e->max_inflight; i++) e->workers.emplace_back(worker_main, e);
+  for (lc_slot* sl : wslots) e->workers.emplace_back(worker_main, e, sl);
   *out = e;
   return LC_OK;
 }
@@ -968,10 +1323,9 @@ void lc_engine_destroy(lc_engine* e) {
   e->admit_cv.notify_all();
   for (auto& w : e->workers) w.join();
   cudaSetDevice(e->device);
-  for (auto s : e->free_streams) cudaStreamDestroy(s);
   e->pinned.clear();
   cudaFree(e->crc_xpow);
-  delete e;
+  delete e;  // destroys the slots
 }
 
 lc_status lc_job_submit(lc_engine* e, const lc_job_desc* desc, lc_job** out) {
@@ -1038,27 +1392,152 @@ void lc_job_release(lc_job* j) {
 
 lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_job** job_out) {
   if (!e || !desc || !out || !job_out) return fail(LC_ERR_INVALID_ARG, "null argument");
-  lc_job* j = new (std::nothrow) lc_job();
-  if (!j) return fail(LC_ERR_NO_MEMORY, "job");
-  j->eng = e;
-  lc_status s = copy_desc(j, desc);
+  *job_out = nullptr;
+  lc_job* j = nullptr;
+  lc_status s = lc_compact_batch(e, 1, desc, &j);
+  if (!j) return s;
   if (s != LC_OK) {
-    delete j;
-    return s;
-  }
-  cudaSetDevice(e->device);
-  cudaStream_t st = e->get_stream();
-  execute(j, st);
-  e->put_stream(st);
-  j->done = true;
-  if (j->status != LC_OK) {
-    lc_status r = fail(j->status, j->err);
     lc_job_release(j);
-    *job_out = nullptr;
-    return r;
+    return s;
   }
   fill_out(j, out);
   *job_out = j;
+  return LC_OK;
+}
+
+lc_status lc_compact_batch(lc_engine* e, int32_t n, const lc_job_desc* descs, lc_job** jobs) {
+  if (!e || n < 0 || (n && (!descs || !jobs))) return fail(LC_ERR_INVALID_ARG, "null argument");
+  std::vector<lc_job*> all(n, nullptr);
+  for (int32_t i = 0; i < n; i++) {
+    lc_job* j = new (std::nothrow) lc_job();
+    lc_status s = j ? copy_desc(j, &descs[i]) : fail(LC_ERR_NO_MEMORY, "job");
+    if (j) j->eng = e;
+    if (s != LC_OK) {
+      const std::string m = g_last_error;
+      delete j;
+      for (int32_t k = 0; k < i; k++) delete all[k];
+      return fail(s, "job " + std::to_string(i) + ": " + m);
+    }
+    all[i] = j;
+  }
+  lc_slot* slot = nullptr;
+  try {
+    CK(cudaSetDevice(e->device));
+    slot = e->take_slot();
+  } catch (const CudaError& ce) {
+    for (auto* j : all) delete j;
+    return fail(LC_ERR_CUDA, std::string(ce.what) + ": " + cudaGetErrorString(ce.e));
+  }
+  const Tunables tun = e->tuning();
+  for (int32_t i0 = 0; i0 < n; i0 += (int32_t)e->max_batch) {
+    std::vector<lc_job*> batch(all.begin() + i0,
+                               all.begin() + std::min<int64_t>(n, (int64_t)i0 + e->max_batch));
+    run_batch(batch, *slot, tun);
+  }
+  e->put_slot(slot);
+  lc_status first = LC_OK;
+  for (int32_t i = 0; i < n; i++) {
+    all[i]->done = true;
+    if (first == LC_OK && all[i]->status != LC_OK) {
+      first = all[i]->status;
+      g_last_error = "job " + std::to_string(i) + ": " + all[i]->err;
+    }
+    jobs[i] = all[i];
+  }
+  return first;
+}
+
+lc_status lc_get_tuning(lc_engine* e, lc_tuning* out) {
+  if (!e || !out) return fail(LC_ERR_INVALID_ARG, "null argument");
+  const Tunables t = e->tuning();
+  out->ctas_per_job = t.ctas_per_job;
+  out->merge_items = t.merge_items;
+  out->merge_threads = t.merge_threads;
+  return LC_OK;
+}
+
+lc_status lc_set_tuning(lc_engine* e, const lc_tuning* t) {
+  if (!e || !t) return fail(LC_ERR_INVALID_ARG, "null argument");
+  if (t->merge_items < 1 || t->merge_items > 32 || t->merge_threads < 64 ||
+      t->merge_threads > 1024 || t->merge_threads % 32 || t->ctas_per_job > 65535)
+    return fail(LC_ERR_INVALID_ARG, "tuning out of range");
+  std::lock_guard<std::mutex> g(e->tun_mu);
+  e->tun.ctas_per_job = t->ctas_per_job;
+  e->tun.merge_items = t->merge_items;
+  e->tun.merge_threads = t->merge_threads;
+  return LC_OK;
+}
+
+lc_status lc_autotune(lc_engine* e, int32_t n, const lc_job_desc* descs, int32_t repeats,
+                      lc_tuning* chosen) {
+  if (!e || n <= 0 || !descs || !chosen) return fail(LC_ERR_INVALID_ARG, "null argument");
+  if (repeats < 1) repeats = 1;
+  // outputs stay on the device: the tuner only needs the device time
+  std::vector<lc_job_desc> d(descs, descs + n);
+  for (auto& x : d) x.outputs_on_device = 1;
+  std::vector<lc_job*> jobs(n, nullptr);
+  // median device time of the whole set under one setting
+  auto time_of = [&](const Tunables& t, double* ms) -> lc_status {
+    {
+      std::lock_guard<std::mutex> g(e->tun_mu);
+      e->tun = t;
+    }
+    std::vector<double> v;
+    for (int32_t r = 0; r < repeats + 1; r++) {  // the first run captures the graphs
+      std::fill(jobs.begin(), jobs.end(), nullptr);
+      lc_status s = lc_compact_batch(e, n, d.data(), jobs.data());
+      double tot = 0;
+      for (int32_t i = 0; i < n; i++) {
+        if (jobs[i] && i % (int32_t)e->max_batch == 0) tot += jobs[i]->device_ms;  // per batch
+        lc_job_release(jobs[i]);
+      }
+      if (s != LC_OK) return s;
+      if (r > 0) v.push_back(tot);
+    }
+    std::sort(v.begin(), v.end());
+    *ms = v[v.size() / 2];
+    return LC_OK;
+  };
+  const Tunables saved = e->tuning();
+  Tunables best = saved;
+  double best_ms = 0;
+  lc_status s = time_of(best, &best_ms);
+  // coordinate search: merge tile (threads x items per thread), then CTAs per job
+  const uint32_t threads[] = {128, 256, 512};
+  const uint32_t items[] = {4, 8, 16};
+  for (uint32_t th : threads)
+    for (uint32_t it : items) {
+      if (s != LC_OK) break;
+      Tunables t = best;
+      t.merge_threads = th;
+      t.merge_items = it;
+      if (t.merge_threads == best.merge_threads && t.merge_items == best.merge_items) continue;
+      double ms;
+      s = time_of(t, &ms);
+      if (s == LC_OK && ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+  const uint32_t ctas[] = {0, 4, 16, 64, 256};
+  for (uint32_t c : ctas) {
+    if (s != LC_OK) break;
+    if (c == best.ctas_per_job) continue;
+    Tunables t = best;
+    t.ctas_per_job = c;
+    double ms;
+    s = time_of(t, &ms);
+    if (s == LC_OK && ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  std::lock_guard<std::mutex> g(e->tun_mu);
+  e->tun = s == LC_OK ? best : saved;
+  if (s != LC_OK) return s;
+  chosen->ctas_per_job = best.ctas_per_job;
+  chosen->merge_items = best.merge_items;
+  chosen->merge_threads = best.merge_threads;
   return LC_OK;
 }
 
@@ -1082,10 +1561,16 @@ lc_status lc_build_table(lc_engine* e, const lc_table_options* opt, int64_t n,
   j->bvoffs = value_offsets;
   j->inputs_on_device = on_device;
   j->outputs_on_device = 0;
-  cudaSetDevice(e->device);
-  cudaStream_t st = e->get_stream();
-  execute(j, st);
-  e->put_stream(st);
+  lc_slot* slot = nullptr;
+  try {
+    CK(cudaSetDevice(e->device));
+    slot = e->take_slot();
+  } catch (const CudaError& ce) {
+    delete j;
+    return fail(LC_ERR_CUDA, std::string(ce.what) + ": " + cudaGetErrorString(ce.e));
+  }
+  run_build(j, *slot);
+  e->put_slot(slot);
   j->done = true;
   if (j->status != LC_OK) {
     lc_status r = fail(j->status, j->err);
@@ -1102,10 +1587,12 @@ lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_de
                     uint32_t* masked_crc) {
   if (!e || !masked_crc || (n && !data)) return fail(LC_ERR_INVALID_ARG, "null argument");
   cudaStream_t st = nullptr;
+  lc_slot* slot = nullptr;
   std::vector<void*> ptrs;
   try {
     CK(cudaSetDevice(e->device));
-    st = e->get_stream();
+    slot = e->take_slot();
+    st = slot->st;
     const uint8_t* d_data = data;
     const uint32_t chunks = crc32c_chunk_count(n);
     void* p = nullptr;
@@ -1129,14 +1616,14 @@ lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_de
     for (void* q : ptrs) CK(cudaFreeAsync(q, st));
     ptrs.clear();
     CK(cudaStreamSynchronize(st));
-    e->put_stream(st);
+    e->put_slot(slot);
     *masked_crc = h;
     return LC_OK;
   } catch (const CudaError& ce) {
-    if (st) {
+    if (slot) {
       for (void* q : ptrs) cudaFreeAsync(q, st);
       cudaStreamSynchronize(st);
-      e->put_stream(st);
+      e->put_slot(slot);
     }
     return fail(LC_ERR_CUDA, std::string(ce.what) + ": " + cudaGetErrorString(ce.e));
   }

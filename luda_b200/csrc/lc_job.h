@@ -130,8 +130,8 @@ struct JobDev {
   uint64_t cap_entries;
 
   // merge
-  uint32_t* m_ids;           // merged order (ping)
-  uint32_t* m_tmp;           // (pong)
+  uint32_t* m_ids;           // merged order (holds the result after the last round)
+  uint32_t* m_tmp;           // the other buffer of the ping-pong
   uint8_t* keep;             // per merged position
   uint32_t* gp_idx;          // per merged position: grandparents passed
   uint32_t* kept_pos;        // exclusive scan of keep (n+1)
@@ -179,6 +179,16 @@ struct JobDev {
   uint32_t cap_files;
   uint8_t* out;
   uint64_t cap_out;
+
+  // scratch of the batched kernels
+  uint32_t* gp_first;        // per grandparent count g: first merged position reaching g
+  uint32_t* tmp32;           // block bytes with trailers (scan input)
+  uint8_t* fkeys;            // smallest / largest key of every file, packed
+  uint64_t* fkoff;           // 2 * cap_files + 1 offsets into fkeys
+  const uint64_t* src_koffs; // flush encoder: key offsets (n + 1)
+  const uint64_t* src_voffs; // flush encoder: value offsets (n + 1)
+  uint64_t* scan_scratch;    // tile sums of the prefix sums
+  uint64_t cap_scan;         // capacity of the arrays scanned (for the tile sums)
 
   // CRC32C shift table: x^(8m) mod P for m in [0, crc_tab_n)
   const uint32_t* crc_xpow;

@@ -1,7 +1,11 @@
-// Host-callable launchers for the engine's kernels.  Each launcher enqueues
-// work on `st` and never synchronises; counts that are only known on the
-// device are read by the kernels from JobDev::ctr, and grids are sized from
-// host-side capacities.
+// Host-callable launchers for the engine's kernels.
+//
+// Every kernel serves a batch of jobs in one launch: the grid's y dimension is
+// the job index, and each kernel reads its job's descriptor from a device
+// array (`jobs[blockIdx.y]`).  A plain compaction is a batch of one.  Launchers
+// enqueue work on `st` and never synchronise; counts that are only known on
+// the device are read by the kernels from each job's Counters, and grids are
+// sized from host-side capacities (maxima over the batch).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -10,14 +14,43 @@
 
 namespace lc {
 
-// Kernel launches made by the calling thread (each job runs on one thread).
+// Kernel launches made by the calling thread (each batch runs on one thread).
 void note_launch(uint32_t n = 1);
 uint32_t launches_on_this_thread();
 
-// lc_scan.cu
-template <typename TI, typename TO>
-void scan_exclusive(const TI* in, TO* out, const uint64_t* n_dev, uint64_t n_cap, TO* scratch,
-                    uint64_t* total_out, cudaStream_t st);
+// Raise the dynamic shared-memory limits of the kernels that need more than
+// 48 KiB; once per device, with that device current, before any launch or
+// stream capture.
+void decode_kernel_attributes();
+void encode_kernel_attributes();
+
+struct Batch {
+  const JobDev* d = nullptr;  // device array of B job descriptors
+  uint32_t B = 0;
+  // maxima over the batch, for grid sizes
+  uint32_t max_tables = 0, max_gp = 0, max_cap_triggers = 0, max_cap_files = 0;
+  uint64_t max_blocks_in = 0, max_entries = 0;
+  uint32_t merge_rounds = 0;
+  uint32_t chunk = 4096;
+  uint32_t chain_smem_words = 12 * 1024;
+  // tunables (chosen by the autotuner in lc_engine.cu)
+  uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
+  uint32_t merge_items = 8;   // outputs per thread in a merge round
+  uint32_t merge_threads = 256;  // threads per merge CTA (tile = threads * items)
+};
+
+// lc_scan.cu -- exclusive prefix sums over per-job arrays chosen by selector
+enum ScanSel : int {
+  kScanTblBlocks = 0,  // tbl_nblocks -> tbl_block_base      (total: n_blocks_in)
+  kScanBlkEnt,         // blk_nent -> blk_ent_base           (total: n_entries_in)
+  kScanBlkKey,         // blk_kbytes -> blk_key_base         (total: key_bytes_in)
+  kScanKeep,           // keep -> kept_pos                   (total: n_kept)
+  kScanBstart,         // k_bstart -> k_block                (total: n_blocks_out)
+  kScanBcum,           // tmp32 -> b_cum
+  kScanGcum,           // b_gbytes -> b_gcum
+  kScanIcum,           // b_isize -> b_icum
+};
+void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st);
 uint64_t scan_scratch_elems(uint64_t n_cap);
 
 // lc_crc.cu -- masked CRC32C of one buffer; `counter` must be zero at launch
@@ -25,34 +58,40 @@ void launch_crc32c_chunks(const uint8_t* data, uint64_t n, uint32_t* partials, u
                           uint32_t* out, cudaStream_t st);
 
 // lc_decode.cu -- input tables -> decoded entries
-void launch_table_index_count(const JobDev& J, cudaStream_t st);
-void launch_table_index_entries(const JobDev& J, cudaStream_t st);
-void launch_block_count(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st);
-void launch_run_bounds(const JobDev& J, cudaStream_t st);
-void launch_block_decode(const JobDev& J, uint64_t n_blocks_cap, cudaStream_t st);
-void launch_entries_from_offsets(const JobDev& J, const uint64_t* koffs, const uint64_t* voffs,
-                                 uint64_t n, cudaStream_t st);
+void launch_table_index_count(const Batch& bt, cudaStream_t st);
+void launch_table_index_entries(const Batch& bt, cudaStream_t st);
+void launch_block_count(const Batch& bt, cudaStream_t st);
+void launch_run_bounds(const Batch& bt, cudaStream_t st);
+void launch_block_decode(const Batch& bt, cudaStream_t st);
+void launch_entries_from_offsets(const Batch& bt, cudaStream_t st);
 
 // lc_merge.cu -- merge, drop rule, grandparent cuts, survivors
-void launch_iota(uint32_t* ids, uint64_t n, cudaStream_t st);
-void launch_merge_round(const JobDev& J, const uint32_t* src, uint32_t* dst, uint32_t width,
-                        uint64_t n, cudaStream_t st);
-void launch_drop(const JobDev& J, uint64_t n, cudaStream_t st);
-void launch_triggers(const JobDev& J, uint64_t n, uint32_t* gp_first, cudaStream_t st);
-void launch_kept_compact(const JobDev& J, uint64_t n, cudaStream_t st);
+void launch_merge(const Batch& bt, cudaStream_t st);
+void launch_drop(const Batch& bt, cudaStream_t st);
+void launch_triggers(const Batch& bt, cudaStream_t st);
+void launch_kept_compact(const Batch& bt, cudaStream_t st);
 
 // lc_encode.cu -- survivors -> output tables
-void launch_sizes(const JobDev& J, uint64_t n_cap, cudaStream_t st);
-void launch_next(const JobDev& J, uint64_t n_cap, cudaStream_t st);
-void launch_chain(const JobDev& J, uint64_t n_cap, cudaStream_t st);
-void launch_block_list(const JobDev& J, uint64_t n_cap, cudaStream_t st);
-void launch_block_sizes(const JobDev& J, uint32_t* tmp32, uint64_t nb_cap, cudaStream_t st);
-void launch_files(const JobDev& J, uint64_t nb_cap, cudaStream_t st);
-void launch_block_layout(const JobDev& J, uint64_t nb_cap, cudaStream_t st);
-void launch_file_layout(const JobDev& J, cudaStream_t st);
-void launch_encode_blocks(const JobDev& J, uint64_t nb, cudaStream_t st);
-void launch_encode_rest(const JobDev& J, uint64_t nb, uint32_t n_files, cudaStream_t st);
-void launch_file_keys(const JobDev& J, uint32_t cap_files, uint8_t* key_out, uint64_t* key_off,
-                      cudaStream_t st);
+void launch_zero_bstart(const Batch& bt, cudaStream_t st);
+void launch_sizes(const Batch& bt, cudaStream_t st);
+void launch_next(const Batch& bt, cudaStream_t st);
+void launch_chain(const Batch& bt, cudaStream_t st);
+void launch_block_list(const Batch& bt, cudaStream_t st);
+void launch_block_sizes(const Batch& bt, cudaStream_t st);
+void launch_files(const Batch& bt, cudaStream_t st);
+void launch_block_layout(const Batch& bt, cudaStream_t st);
+void launch_file_layout(const Batch& bt, cudaStream_t st);
+void launch_encode_blocks(const Batch& bt, cudaStream_t st);
+void launch_encode_rest(const Batch& bt, cudaStream_t st);
+void launch_file_keys(const Batch& bt, cudaStream_t st);
+
+// grid x for a kernel over up to `items` items per job, `per` items per CTA,
+// capped at `cap` CTAs (the kernel loops over the rest)
+inline unsigned grid_x(uint64_t items, unsigned per, uint64_t cap) {
+  uint64_t g = (items + per - 1) / per;
+  if (g == 0) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
 
 }  // namespace lc

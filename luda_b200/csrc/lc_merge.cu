@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "lc_device.cuh"
 #include "lc_kernels.h"
 
@@ -26,53 +28,62 @@ namespace lc {
 
 namespace {
 
-constexpr int kMergeItems = 8;
-
-__global__ void k_iota(uint32_t* ids, uint64_t n) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) ids[i] = (uint32_t)i;
+__global__ void k_iota(const JobDev* __restrict__ jobs, uint32_t rounds) {
+  const JobDev& J = jobs[blockIdx.y];
+  uint32_t* ids = (rounds & 1) ? J.m_tmp : J.m_ids;  // the buffer round 0 reads
+  const uint64_t n = J.ctr->n_entries_in;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    ids[i] = (uint32_t)i;
 }
 
-// Round with groups of `width` merge children; pairs (2p, 2p+1) merge.
-__global__ void k_merge_round(JobDev J, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
-                              uint32_t width) {
+// Round `r` of `rounds`: groups of width = 2^r merge children; pairs (2p,
+// 2p+1) merge.  Jobs with fewer children copy through, so every job of a
+// batch ends with its merged order in m_ids.
+__global__ void k_merge_round(const JobDev* __restrict__ jobs, uint32_t r, uint32_t rounds,
+                              uint32_t items) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint32_t* __restrict__ src = ((rounds - r) & 1) ? J.m_tmp : J.m_ids;
+  uint32_t* __restrict__ dst = ((rounds - r) & 1) ? J.m_ids : J.m_tmp;
+  const uint32_t width = 1u << r;
   const uint64_t n = J.run_entry_begin[J.n_runs];
-  const uint64_t o0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kMergeItems;
-  if (o0 >= n) return;
-  const uint64_t o1 = min(n, o0 + kMergeItems);
-  uint64_t o = o0;
-  while (o < o1) {
-    // find the pair that owns output position o
-    uint32_t pair_runs = 2 * width;
-    uint32_t r0 = 0;
-    while (true) {
-      uint32_t r2 = min(r0 + pair_runs, J.n_runs);
-      if (o < J.run_entry_begin[r2]) break;
-      r0 = r2;
-    }
-    const uint32_t r1 = min(r0 + width, J.n_runs);
-    const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
-    const uint64_t a0 = J.run_entry_begin[r0], b0 = J.run_entry_begin[r1],
-                   b1 = J.run_entry_begin[r2];
-    const uint64_t na = b0 - a0, nb = b1 - b0;
-    const uint64_t stop = min(o1, b1);
-    if (nb == 0) {
-      for (; o < stop; o++) dst[o] = src[o];
-      continue;
-    }
-    const uint32_t* A = src + a0;
-    const uint32_t* B = src + b0;
-    const uint64_t d = o - a0;
-    uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (entry_cmp(J, A[mid], B[d - 1 - mid]) <= 0) lo = mid + 1;
-      else hi = mid;
-    }
-    uint64_t i = lo, j = d - lo;
-    for (; o < stop; o++) {
-      bool take_a = i < na && (j >= nb || entry_cmp(J, A[i], B[j]) <= 0);
-      dst[o] = take_a ? A[i++] : B[j++];
+  for (uint64_t o0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * items; o0 < n;
+       o0 += (uint64_t)gridDim.x * blockDim.x * items) {
+    const uint64_t o1 = min(n, o0 + items);
+    uint64_t o = o0;
+    while (o < o1) {
+      // find the pair that owns output position o
+      const uint32_t pair_runs = 2 * width;
+      uint32_t r0 = 0;
+      while (true) {
+        const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
+        if (o < J.run_entry_begin[r2]) break;
+        r0 = r2;
+      }
+      const uint32_t r1 = min(r0 + width, J.n_runs);
+      const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
+      const uint64_t a0 = J.run_entry_begin[r0], b0 = J.run_entry_begin[r1],
+                     b1 = J.run_entry_begin[r2];
+      const uint64_t na = b0 - a0, nb = b1 - b0;
+      const uint64_t stop = min(o1, b1);
+      if (nb == 0) {
+        for (; o < stop; o++) dst[o] = src[o];
+        continue;
+      }
+      const uint32_t* A = src + a0;
+      const uint32_t* B = src + b0;
+      const uint64_t d = o - a0;
+      uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+      while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (entry_cmp(J, A[mid], B[d - 1 - mid]) <= 0) lo = mid + 1;
+        else hi = mid;
+      }
+      uint64_t i = lo, j = d - lo;
+      for (; o < stop; o++) {
+        const bool take_a = i < na && (j >= nb || entry_cmp(J, A[i], B[j]) <= 0);
+        dst[o] = take_a ? A[i++] : B[j++];
+      }
     }
   }
 }
@@ -96,10 +107,8 @@ __device__ __forceinline__ bool is_base_level(const JobDev& J, const uint8_t* uk
   return true;
 }
 
-__global__ void k_drop(JobDev J, const uint32_t* __restrict__ ids) {
-  const uint64_t n = J.ctr->n_entries_in;
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+__device__ __forceinline__ void drop_one(const JobDev& J, const uint32_t* __restrict__ ids,
+                                         uint64_t p) {
   const uint32_t id = ids[p];
   const uint8_t* key = J.keys + J.e_koff[id];
   const uint32_t klen = J.e_klen[id];
@@ -140,9 +149,19 @@ __global__ void k_drop(JobDev J, const uint32_t* __restrict__ ids) {
   }
 }
 
+__global__ void k_drop(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = J.ctr->n_entries_in;
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (uint64_t)gridDim.x * blockDim.x)
+    drop_one(J, J.m_ids, p);
+}
+
 // gp_first[g] = first merged position whose grandparent count reaches g
 // (gp_idx is non-decreasing along the merge order).
-__global__ void k_gp_first(JobDev J, uint32_t* gp_first) {
+__global__ void k_gp_first(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  uint32_t* gp_first = J.gp_first;
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g > J.n_gp) return;
   const uint64_t n = J.ctr->n_entries_in;
@@ -160,7 +179,9 @@ __global__ void k_gp_first(JobDev J, uint32_t* gp_first) {
 // position whose grandparent count reaches the smallest g with
 // prefix[g] - prefix[gp_idx[t]] > limit.  Few cuts; one thread walks them
 // over shared-memory copies of the prefix and first-position arrays.
-__global__ void k_triggers(JobDev J, const uint32_t* gp_first, bool in_smem) {
+__global__ void k_triggers(const JobDev* __restrict__ jobs, bool in_smem) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint32_t* gp_first = J.gp_first;
   extern __shared__ uint64_t s_tr[];
   const uint64_t n = J.ctr->n_entries_in;
   const uint32_t G = J.n_gp;
@@ -203,18 +224,22 @@ __global__ void k_triggers(JobDev J, const uint32_t* gp_first, bool in_smem) {
   J.ctr->n_triggers = cnt;
 }
 
-__global__ void k_kept_compact(JobDev J, const uint32_t* __restrict__ ids) {
+__global__ void k_kept_compact(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  const uint32_t* __restrict__ ids = J.m_ids;
   const uint64_t n = J.ctr->n_entries_in;
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p == 0) J.ctr->n_kept = J.kept_pos[n];
-  if (p < n && J.keep[p]) {
-    const uint32_t k = J.kept_pos[p];
-    J.k_ids[k] = ids[p];
-    J.k_forced[k] = 0;
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (uint64_t)gridDim.x * blockDim.x) {
+    if (J.keep[p]) {
+      const uint32_t k = J.kept_pos[p];
+      J.k_ids[k] = ids[p];
+      J.k_forced[k] = 0;
+    }
   }
 }
 
-__global__ void k_forced(JobDev J) {
+__global__ void k_forced(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t nk = J.kept_pos[J.ctr->n_entries_in];
   if (i == 0 && nk > 0) J.k_forced[0] = 1;
@@ -226,30 +251,36 @@ __global__ void k_forced(JobDev J) {
 
 }  // namespace
 
-void launch_iota(uint32_t* ids, uint64_t n, cudaStream_t st) {
-  if (n) note_launch(), k_iota<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ids, n);
+static unsigned flat_ctas(const Batch& bt, uint64_t items, unsigned per) {
+  const uint64_t cap = std::max<uint64_t>(1, bt.ctas_per_job ? bt.ctas_per_job : 148 * 8 / bt.B);
+  return grid_x(items, per, cap);
 }
 
-void launch_merge_round(const JobDev& J, const uint32_t* src, uint32_t* dst, uint32_t width,
-                        uint64_t n, cudaStream_t st) {
-  const uint64_t threads = (n + kMergeItems - 1) / kMergeItems;
-  if (threads) note_launch(), k_merge_round<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(J, src, dst, width);
+void launch_merge(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_iota<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(
+      bt.d, bt.merge_rounds);
+  const uint32_t items = bt.merge_items;
+  const uint32_t threads = bt.merge_threads;
+  for (uint32_t r = 0; r < bt.merge_rounds; r++)
+    note_launch(), k_merge_round<<<dim3(flat_ctas(bt, (bt.max_entries + items - 1) / items, threads),
+                                        bt.B), threads, 0, st>>>(bt.d, r, bt.merge_rounds, items);
 }
 
-void launch_drop(const JobDev& J, uint64_t n, cudaStream_t st) {
-  if (n) note_launch(), k_drop<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(J, J.m_ids);
+void launch_drop(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_drop<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(bt.d);
 }
 
-void launch_triggers(const JobDev& J, uint64_t n, uint32_t* gp_first, cudaStream_t st) {
-  if (J.n_gp) note_launch(), k_gp_first<<<(J.n_gp + 1 + 255) / 256, 256, 0, st>>>(J, gp_first);
-  const size_t smem = (size_t)(J.n_gp + 1) * 12;
+void launch_triggers(const Batch& bt, cudaStream_t st) {
+  if (bt.max_gp)
+    note_launch(), k_gp_first<<<dim3((bt.max_gp + 1 + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
+  const size_t smem = (size_t)(bt.max_gp + 1) * 12;
   const bool in_smem = smem <= 48 * 1024;
-  note_launch(), k_triggers<<<1, 256, in_smem ? smem : 0, st>>>(J, gp_first, in_smem);
+  note_launch(), k_triggers<<<dim3(1, bt.B), 256, in_smem ? smem : 0, st>>>(bt.d, in_smem);
 }
 
-void launch_kept_compact(const JobDev& J, uint64_t n, cudaStream_t st) {
-  note_launch(), k_kept_compact<<<(unsigned)((n + 256) / 256), 256, 0, st>>>(J, J.m_ids);
-  note_launch(), k_forced<<<(J.cap_triggers + 255) / 256 + 1, 256, 0, st>>>(J);
+void launch_kept_compact(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_kept_compact<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_forced<<<dim3((bt.max_cap_triggers + 255) / 256 + 1, bt.B), 256, 0, st>>>(bt.d);
 }
 
 }  // namespace lc

@@ -1,9 +1,11 @@
-// Device-wide exclusive prefix sums (reduce, scan of tile sums, scan).
+// Exclusive prefix sums of per-job arrays (reduce, scan of tile sums, scan),
+// one launch per step for a whole batch (grid y = job).
 //
-// The element count may live in device memory (n_dev) so that a scan can be
-// enqueued before the producing kernel's count is known on the host; the grid
-// is sized from a host-side capacity and tiles past the count exit early.
-// out has n+1 entries: out[n] is the total.
+// The array and its length are chosen by a selector from the job descriptor;
+// the length lives in device memory, so a scan can be enqueued before the
+// producing kernel's count is known on the host.  The grid is sized from a
+// host-side capacity and tiles past the count exit early.  out has n+1
+// entries: out[n] is the total, optionally also stored to a counter.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -23,6 +25,81 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kTile = kScanThreads * kScanItems;
+
+template <int S>
+struct ScanOf;
+template <>
+struct ScanOf<kScanTblBlocks> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.tbl_nblocks; }
+  static __device__ TO* out(const JobDev& J) { return J.tbl_block_base; }
+  static __device__ uint64_t n(const JobDev& J) { return J.n_tables; }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->n_blocks_in; }
+};
+template <>
+struct ScanOf<kScanBlkEnt> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.blk_nent; }
+  static __device__ TO* out(const JobDev& J) { return J.blk_ent_base; }
+  static __device__ uint64_t n(const JobDev& J) { return min(J.ctr->n_blocks_in, J.cap_blocks_in); }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->n_entries_in; }
+};
+template <>
+struct ScanOf<kScanBlkKey> {
+  using TI = uint64_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.blk_kbytes; }
+  static __device__ TO* out(const JobDev& J) { return J.blk_key_base; }
+  static __device__ uint64_t n(const JobDev& J) { return min(J.ctr->n_blocks_in, J.cap_blocks_in); }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->key_bytes_in; }
+};
+template <>
+struct ScanOf<kScanKeep> {
+  using TI = uint8_t;
+  using TO = uint32_t;
+  static __device__ const TI* in(const JobDev& J) { return J.keep; }
+  static __device__ TO* out(const JobDev& J) { return J.kept_pos; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_entries_in; }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->n_kept; }
+};
+template <>
+struct ScanOf<kScanBstart> {
+  using TI = uint8_t;
+  using TO = uint32_t;
+  static __device__ const TI* in(const JobDev& J) { return J.k_bstart; }
+  static __device__ TO* out(const JobDev& J) { return J.k_block; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_kept; }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->n_blocks_out; }
+};
+template <>
+struct ScanOf<kScanBcum> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.tmp32; }
+  static __device__ TO* out(const JobDev& J) { return J.b_cum; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_blocks_out; }
+  static __device__ uint64_t* total(const JobDev&) { return nullptr; }
+};
+template <>
+struct ScanOf<kScanGcum> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.b_gbytes; }
+  static __device__ TO* out(const JobDev& J) { return J.b_gcum; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_blocks_out; }
+  static __device__ uint64_t* total(const JobDev&) { return nullptr; }
+};
+template <>
+struct ScanOf<kScanIcum> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.b_isize; }
+  static __device__ TO* out(const JobDev& J) { return J.b_icum; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_blocks_out; }
+  static __device__ uint64_t* total(const JobDev&) { return nullptr; }
+};
 
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
@@ -57,92 +134,108 @@ __device__ __forceinline__ T block_excl_scan(T v, T* total) {
   return res;
 }
 
-__device__ __forceinline__ uint64_t resolve_n(const uint64_t* n_dev, uint64_t n_host) {
-  return n_dev ? *n_dev : n_host;
-}
-
-template <typename TI, typename TO>
-__global__ void k_tile_reduce(const TI* in, const uint64_t* n_dev, uint64_t n_host,
-                              TO* tile_sums) {
-  const uint64_t n = resolve_n(n_dev, n_host);
-  const uint64_t base = (uint64_t)blockIdx.x * kTile;
-  TO s = 0;
-  if (base < n) {
+template <int S>
+__global__ void k_tile_reduce(const JobDev* __restrict__ jobs) {
+  using SP = ScanOf<S>;
+  using TO = typename SP::TO;
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = SP::n(J);
+  TO* tile_sums = reinterpret_cast<TO*>(J.scan_scratch);
+  const typename SP::TI* in = SP::in(J);
+  for (uint64_t t = blockIdx.x; t * kTile <= n; t += gridDim.x) {
+    const uint64_t base = t * kTile;
+    TO s = 0;
     for (int k = 0; k < kScanItems; k++) {
-      uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
+      const uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
       if (i < n) s += (TO)in[i];
     }
+    TO total;
+    block_excl_scan<TO>(s, &total);
+    if (threadIdx.x == 0) tile_sums[t] = total;
   }
-  TO total;
-  block_excl_scan<TO>(s, &total);
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-template <typename TO>
-__global__ void k_scan_tiles(TO* tile_sums, uint32_t n_tiles) {
+template <int S>
+__global__ void k_scan_tiles(const JobDev* __restrict__ jobs) {
+  using SP = ScanOf<S>;
+  using TO = typename SP::TO;
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = SP::n(J);
+  const uint64_t n_tiles = n / kTile + 1;
+  TO* tile_sums = reinterpret_cast<TO*>(J.scan_scratch);
   TO carry = 0;
-  for (uint32_t base = 0; base < n_tiles; base += blockDim.x) {
-    uint32_t i = base + threadIdx.x;
+  for (uint64_t base = 0; base < n_tiles; base += blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
     TO v = i < n_tiles ? tile_sums[i] : TO(0);
     TO total;
     TO ex = block_excl_scan<TO>(v, &total);
     if (i < n_tiles) tile_sums[i] = carry + ex;
     carry += total;
   }
-  if (threadIdx.x == 0) tile_sums[n_tiles] = carry;
 }
 
-template <typename TI, typename TO>
-__global__ void k_tile_scan(const TI* in, const uint64_t* n_dev, uint64_t n_host,
-                            const TO* tile_offsets, TO* out, uint64_t* total_out) {
-  const uint64_t n = resolve_n(n_dev, n_host);
-  const uint64_t base = (uint64_t)blockIdx.x * kTile;
-  if (base > n) return;
-  TO vals[kScanItems];
-  TO s = 0;
-  const uint64_t tb = base + (uint64_t)threadIdx.x * kScanItems;
+template <int S>
+__global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
+  using SP = ScanOf<S>;
+  using TO = typename SP::TO;
+  const JobDev& J = jobs[blockIdx.y];
+  const uint64_t n = SP::n(J);
+  const TO* tile_offsets = reinterpret_cast<const TO*>(J.scan_scratch);
+  const typename SP::TI* in = SP::in(J);
+  TO* out = SP::out(J);
+  uint64_t* total_out = SP::total(J);
+  for (uint64_t t = blockIdx.x; t * kTile <= n; t += gridDim.x) {
+    const uint64_t base = t * kTile;
+    TO vals[kScanItems];
+    TO s = 0;
+    const uint64_t tb = base + (uint64_t)threadIdx.x * kScanItems;
 #pragma unroll
-  for (int k = 0; k < kScanItems; k++) {
-    uint64_t i = tb + k;
-    vals[k] = i < n ? (TO)in[i] : TO(0);
-    s += vals[k];
-  }
-  TO total;
-  TO ex = block_excl_scan<TO>(s, &total) + tile_offsets[blockIdx.x];
-#pragma unroll
-  for (int k = 0; k < kScanItems; k++) {
-    uint64_t i = tb + k;
-    if (i < n) out[i] = ex;
-    else if (i == n) {
-      out[n] = ex;
-      if (total_out) *total_out = (uint64_t)ex;
+    for (int k = 0; k < kScanItems; k++) {
+      const uint64_t i = tb + k;
+      vals[k] = i < n ? (TO)in[i] : TO(0);
+      s += vals[k];
     }
-    ex += vals[k];
+    TO total;
+    TO ex = block_excl_scan<TO>(s, &total) + tile_offsets[t];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+      const uint64_t i = tb + k;
+      if (i < n) {
+        out[i] = ex;
+      } else if (i == n) {
+        out[n] = ex;
+        if (total_out) *total_out = (uint64_t)ex;
+      }
+      ex += vals[k];
+    }
   }
+}
+
+template <int S>
+void scan_sel(const Batch& bt, uint64_t n_cap, cudaStream_t st) {
+  const unsigned tiles = grid_x(n_cap + 1, kTile, 148 * 8);
+  note_launch(3);
+  k_tile_reduce<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
+  k_scan_tiles<S><<<dim3(1, bt.B), 1024, 0, st>>>(bt.d);
+  k_tile_scan<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
 }
 
 }  // namespace
 
-template <typename TI, typename TO>
-void scan_exclusive(const TI* in, TO* out, const uint64_t* n_dev, uint64_t n_cap,
-                    TO* scratch, uint64_t* total_out, cudaStream_t st) {
-  uint32_t tiles = (uint32_t)((n_cap + 1 + kTile - 1) / kTile);
-  if (tiles == 0) tiles = 1;
-  note_launch(3);
-  k_tile_reduce<TI, TO><<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_cap, scratch);
-  k_scan_tiles<TO><<<1, 1024, 0, st>>>(scratch, tiles);
-  k_tile_scan<TI, TO><<<tiles, kScanThreads, 0, st>>>(in, n_dev, n_cap, scratch, out, total_out);
+void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st) {
+  switch (sel) {
+    case kScanTblBlocks: scan_sel<kScanTblBlocks>(bt, n_cap, st); break;
+    case kScanBlkEnt: scan_sel<kScanBlkEnt>(bt, n_cap, st); break;
+    case kScanBlkKey: scan_sel<kScanBlkKey>(bt, n_cap, st); break;
+    case kScanKeep: scan_sel<kScanKeep>(bt, n_cap, st); break;
+    case kScanBstart: scan_sel<kScanBstart>(bt, n_cap, st); break;
+    case kScanBcum: scan_sel<kScanBcum>(bt, n_cap, st); break;
+    case kScanGcum: scan_sel<kScanGcum>(bt, n_cap, st); break;
+    case kScanIcum: scan_sel<kScanIcum>(bt, n_cap, st); break;
+  }
 }
 
-uint64_t scan_scratch_elems(uint64_t n_cap) { return (n_cap + 1 + kTile - 1) / kTile + 2; }
-
-template void scan_exclusive<uint32_t, uint64_t>(const uint32_t*, uint64_t*, const uint64_t*,
-                                                 uint64_t, uint64_t*, uint64_t*, cudaStream_t);
-template void scan_exclusive<uint64_t, uint64_t>(const uint64_t*, uint64_t*, const uint64_t*,
-                                                 uint64_t, uint64_t*, uint64_t*, cudaStream_t);
-template void scan_exclusive<uint8_t, uint32_t>(const uint8_t*, uint32_t*, const uint64_t*,
-                                                uint64_t, uint32_t*, uint64_t*, cudaStream_t);
-template void scan_exclusive<uint32_t, uint32_t>(const uint32_t*, uint32_t*, const uint64_t*,
-                                                 uint64_t, uint32_t*, uint64_t*, cudaStream_t);
+// tile sums for arrays of up to n_cap elements (TO up to 8 bytes)
+uint64_t scan_scratch_elems(uint64_t n_cap) { return (n_cap + 1) / kTile + 2; }
 
 }  // namespace lc

@@ -35,7 +35,13 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "corruption", 3: "cuda error", 4: "
 
 class LcConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("device_budget_bytes", C.c_uint64),
-                ("max_inflight_jobs", C.c_int32), ("flags", C.c_uint32)]
+                ("max_inflight_jobs", C.c_int32), ("flags", C.c_uint32),
+                ("max_batch_jobs", C.c_int32)]
+
+
+class LcTuning(C.Structure):
+    _fields_ = [("ctas_per_job", C.c_uint32), ("merge_items", C.c_uint32),
+                ("merge_threads", C.c_uint32)]
 
 
 class LcTable(C.Structure):
@@ -73,11 +79,13 @@ class LcJobOut(C.Structure):
                 ("key_bytes_out", C.c_uint64)]
 
 LC_FLAG_PHASE_TIMING = 1
+LC_FLAG_NO_GRAPHS = 2
 
 
 EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wait",
            "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
-           "lc_status_string", "lc_version", "lc_crc32c", "lc_crc32c_noalloc"]
+           "lc_status_string", "lc_version", "lc_crc32c", "lc_crc32c_noalloc",
+           "lc_compact_batch", "lc_get_tuning", "lc_set_tuning", "lc_autotune"]
 
 
 class LcError(RuntimeError):
@@ -112,6 +120,16 @@ def load_library(path: str = LIB_PATH):
     l.lc_compact.argtypes = [C.c_void_p, C.POINTER(LcJobDesc), C.POINTER(LcJobOut),
                              C.POINTER(C.c_void_p)]
     l.lc_compact.restype = C.c_int
+    l.lc_compact_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(LcJobDesc),
+                                   C.POINTER(C.c_void_p)]
+    l.lc_compact_batch.restype = C.c_int
+    l.lc_get_tuning.argtypes = [C.c_void_p, C.POINTER(LcTuning)]
+    l.lc_get_tuning.restype = C.c_int
+    l.lc_set_tuning.argtypes = [C.c_void_p, C.POINTER(LcTuning)]
+    l.lc_set_tuning.restype = C.c_int
+    l.lc_autotune.argtypes = [C.c_void_p, C.c_int32, C.POINTER(LcJobDesc), C.c_int32,
+                              C.POINTER(LcTuning)]
+    l.lc_autotune.restype = C.c_int
     l.lc_build_table.argtypes = [C.c_void_p, C.POINTER(LcTableOptions), C.c_int64, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                  C.POINTER(LcJobOut), C.POINTER(C.c_void_p)]
@@ -264,10 +282,10 @@ class Engine:
     """One CUDA device's compaction engine (``lc_engine``)."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 0, max_inflight: int = 4,
-                 phase_timing: bool = False):
+                 phase_timing: bool = False, graphs: bool = True, max_batch: int = 0):
         self.lib = load_library()
-        cfg = LcConfig(device, budget_bytes, max_inflight,
-                       LC_FLAG_PHASE_TIMING if phase_timing else 0)
+        flags = (LC_FLAG_PHASE_TIMING if phase_timing else 0) | (0 if graphs else LC_FLAG_NO_GRAPHS)
+        cfg = LcConfig(device, budget_bytes, max_inflight, flags, max_batch)
         h = C.c_void_p()
         st = self.lib.lc_engine_create(C.byref(cfg), C.byref(h))
         if st != LC_OK:
@@ -317,10 +335,69 @@ class Engine:
                 outputs_on_device: bool = False) -> CompactionResult:
         return self.run(self.prepare(job, device_tables, outputs_on_device))
 
+    @staticmethod
+    def _desc_array(prepared: Sequence["PreparedJob"]):
+        arr = (LcJobDesc * max(1, len(prepared)))()
+        for i, p in enumerate(prepared):
+            arr[i] = p.desc
+        return arr
+
+    def run_batch(self, prepared: Sequence["PreparedJob"], errors: str = "raise") -> list:
+        """Runs the prepared jobs as batches (``lc_compact_batch``); every
+        result is byte-identical to running the job alone.  With
+        ``errors="raise"`` the first failed job raises (after every handle is
+        released); with ``errors="return"`` a failed job's slot holds its
+        :class:`LcError` and the other results are returned."""
+        n = len(prepared)
+        arr = self._desc_array(prepared)
+        hs = (C.c_void_p * max(1, n))()
+        st = self.lib.lc_compact_batch(self.h, n, arr, hs)
+        if st != LC_OK and (errors == "raise" or not any(hs[i] for i in range(n))):
+            msg = self.lib.lc_last_error().decode()
+            for i in range(n):
+                if hs[i]:
+                    self.lib.lc_job_release(hs[i])
+            raise LcError(st, msg)
+        res = []
+        for i in range(n):
+            out = LcJobOut()
+            jst = self.lib.lc_job_result(hs[i], C.byref(out))
+            if jst != LC_OK:
+                res.append(LcError(jst, self.lib.lc_last_error().decode()))
+                self.lib.lc_job_release(hs[i])
+                continue
+            r = _result(out, prepared[i].outputs_on_device)
+            r._handle = _JobHandle(self.lib, C.c_void_p(hs[i]), self)
+            res.append(r)
+        return res
+
+    def compact_batch(self, jobs: Sequence[CompactionJob],
+                      outputs_on_device: bool = False) -> List[CompactionResult]:
+        return self.run_batch([self.prepare(j, None, outputs_on_device) for j in jobs])
+
+    def tuning(self) -> dict:
+        t = LcTuning()
+        self._check(self.lib.lc_get_tuning(self.h, C.byref(t)))
+        return {"ctas_per_job": t.ctas_per_job, "merge_items": t.merge_items,
+                "merge_threads": t.merge_threads}
+
+    def set_tuning(self, ctas_per_job: int = 0, merge_items: int = 8, merge_threads: int = 256):
+        t = LcTuning(ctas_per_job, merge_items, merge_threads)
+        self._check(self.lib.lc_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, prepared: Sequence["PreparedJob"], repeats: int = 2) -> dict:
+        """Times candidate launch settings on these jobs (``lc_autotune``) and
+        keeps the fastest for the engine."""
+        arr = self._desc_array(prepared)
+        t = LcTuning()
+        self._check(self.lib.lc_autotune(self.h, len(prepared), arr, repeats, C.byref(t)))
+        return {"ctas_per_job": t.ctas_per_job, "merge_items": t.merge_items,
+                "merge_threads": t.merge_threads}
+
     def submit_prepared(self, p: "PreparedJob") -> "AsyncJob":
         jh = C.c_void_p()
         self._check(self.lib.lc_job_submit(self.h, C.byref(p.desc), C.byref(jh)))
-        return AsyncJob(self, jh, p.keep)
+        return AsyncJob(self, jh, p.keep, p.outputs_on_device)
 
     def submit(self, job: CompactionJob) -> "AsyncJob":
         keep = _Keep()
@@ -366,8 +443,9 @@ class PreparedJob:
 
 
 class AsyncJob:
-    def __init__(self, eng: Engine, h, keep):
+    def __init__(self, eng: Engine, h, keep, outputs_on_device: bool = False):
         self.eng, self.h, self.keep = eng, h, keep
+        self.outputs_on_device = outputs_on_device
 
     def wait(self, timeout_s: float = -1.0) -> CompactionResult:
         lib = self.eng.lib
@@ -382,7 +460,7 @@ class AsyncJob:
             lib.lc_job_release(self.h)
             self.h = None
             raise
-        res = _result(out, False)
+        res = _result(out, self.outputs_on_device)
         res._handle = _JobHandle(lib, self.h, self.eng)
         self.h = None
         return res
