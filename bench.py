@@ -53,6 +53,9 @@ def parse_args():
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="bound on the CPU baseline sample")
+    p.add_argument("--batch-jobs", type=int, default=64)
+    p.add_argument("--batch-steps", type=int, default=5,
+                   help="timed repetitions of the 64-job set (0: skip the batched leg)")
     return p.parse_args()
 
 
@@ -206,6 +209,120 @@ def cpu_baseline(job, bound_s):
                       f"DoCompactionWork time {med * 1e3:.1f} ms"}
 
 
+def _upload(tables, torch):
+    """Input tables back to back in one device buffer (16-byte aligned starts)."""
+    offs, total = [], 0
+    for f in tables:
+        offs.append(total)
+        total += (len(f.data) + 15) // 16 * 16
+    buf = torch.zeros(total + 16, dtype=torch.uint8, device="cuda")
+    for f, o in zip(tables, offs):
+        buf[o:o + len(f.data)] = torch.frombuffer(bytearray(f.data), dtype=torch.uint8).to("cuda")
+    return buf, [buf.data_ptr() + o for o in offs]
+
+
+def _pin(tables, torch):
+    keep = []
+    for f in tables:
+        t = torch.empty(max(1, len(f.data)), dtype=torch.uint8).pin_memory()
+        t[:len(f.data)].copy_(torch.frombuffer(bytearray(f.data), dtype=torch.uint8))
+        keep.append(t)
+        f.data = t[:len(f.data)].numpy()
+    return keep
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
+
+
+def batched_leg(eng, args, rank, flush, torch):
+    """64 independent jobs (log-uniform 1-64 MiB input, 2-12 tables, 16-byte
+    keys and 100-byte values), all submitted at once: run one after another
+    through lc_compact (plain) and as batches through lc_compact_batch after
+    the autotuner has picked the launch settings.  A job's latency is the
+    time from the common start to its own completion."""
+    from luda_b200 import workloads
+    jobs = [workloads.batched_job(s + 1000 * rank) for s in range(args.batch_jobs)]
+    for j in jobs:
+        j.materialize(lambda e, o: eng.build_table(e, o))
+    in_bytes = [j.input_bytes() for j in jobs]
+    total_in = float(sum(in_bytes))
+    bufs, prep_dev = [], []
+    for j in jobs:
+        buf, ptrs = _upload(j.input_tables(), torch)
+        bufs.append(buf)
+        prep_dev.append(eng.prepare(j, device_tables=ptrs, outputs_on_device=True))
+    pins = []
+    for j in jobs:
+        pins += _pin(j.input_tables(), torch)
+    prep_host = [eng.prepare(j) for j in jobs]
+    torch.cuda.synchronize()
+    # same bytes alone and batched (untimed)
+    alone = [eng.run(p) for p in prep_host[:8]]
+    batched = eng.run_batch(prep_host[:8])
+    assert [a.file_bytes() for a in alone] == [b.file_bytes() for b in batched]
+    for r in alone + batched:
+        r.release()
+    tuning = eng.autotune(prep_dev, repeats=1)
+    steps = max(1, args.batch_steps)
+
+    def plain_step(preps):
+        lat = []
+        t0 = time.perf_counter()
+        launches = 0
+        for p in preps:
+            r = eng.run(p)
+            lat.append((time.perf_counter() - t0) * 1e3)
+            launches += r.kernel_launches
+            r.release()
+        return lat, launches
+
+    def batch_step(preps):
+        t0 = time.perf_counter()
+        rs = eng.run_batch(preps)
+        ms = (time.perf_counter() - t0) * 1e3
+        launches = rs[0].kernel_launches if rs else 0
+        for r in rs:
+            r.release()
+        return [ms] * len(preps), launches
+
+    out = {}
+    for name, fn, preps in (("plain", plain_step, prep_dev), ("batched", batch_step, prep_dev),
+                            ("plain_e2e", plain_step, prep_host),
+                            ("batched_e2e", batch_step, prep_host)):
+        for _ in range(2):
+            fn(preps)
+        dev_ms, lats, launches = [], [], 0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            lat, nl = fn(preps)
+            e1.record()
+            torch.cuda.synchronize()
+            dev_ms.append(e0.elapsed_time(e1))
+            lats += lat
+            launches += nl
+        ms = float(np.sum(dev_ms))
+        out[name] = {"value": steps * total_in / MiB / (ms / 1e3), "unit": UNIT,
+                     "ms_per_step": ms / steps, "p50_ms": _pct(lats, 50), "p99_ms": _pct(lats, 99),
+                     "kernel_launches_per_step": launches / steps}
+    for b in bufs:
+        del b
+    return {
+        "workload": "batched_64 (log-uniform 1-64 MiB per job, 2-12 tables, 16 B keys, 100 B values)",
+        "jobs": len(jobs), "input_mib": total_in / MiB,
+        "job_mib_min": min(in_bytes) / MiB, "job_mib_max": max(in_bytes) / MiB,
+        "steps": steps, "tuning": tuning, **out,
+        "speedup_batched_vs_plain": out["batched"]["value"] / out["plain"]["value"],
+        "speedup_batched_vs_plain_e2e": out["batched_e2e"]["value"] / out["plain_e2e"]["value"],
+        "note": "device-resident inputs and outputs for plain/batched; host pinned buffers for *_e2e; "
+                "all jobs start together, latency = completion time from the common start",
+    }
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -322,6 +439,10 @@ def main():
         seq_ms.append((time.perf_counter() - t0) * 1e3)
         r.release()
 
+    batched = None
+    if args.batch_steps > 0:
+        batched = batched_leg(eng, args, rank, flush, torch)
+
     # max over ranks
     if dist is not None:
         t = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
@@ -380,6 +501,7 @@ def main():
                     "sequential_ms_per_step": float(np.mean(seq_ms)),
                     "sequential_value": in_bytes / MiB / (float(np.mean(seq_ms)) / 1e3)},
             "roofline": roofline,
+            "batched": batched,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
