@@ -53,10 +53,18 @@ def parse_args():
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="bound on the CPU baseline sample")
+    p.add_argument("--no-graphs", action="store_true",
+                   help="launch every kernel directly instead of replaying CUDA graphs")
     p.add_argument("--batch-jobs", type=int, default=64)
     p.add_argument("--batch-steps", type=int, default=5,
                    help="timed repetitions of the 64-job set (0: skip the batched leg)")
     return p.parse_args()
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of each kernel on
+# this workload at scale 1 (profiles/k_encode_blocks_l1_l2_at_size.md,
+# profiles/k_block_decode_l1_l2_at_size.md).
+NCU_TRAFFIC = {"encode_blocks": 89.274624e6 + 30.812160e6, "decode": 68.140032e6 + 3.020800e6}
 
 
 def measured_peak():
@@ -343,7 +351,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     job = make_job(args.scale, 1 + 1000 * rank)
-    eng = Engine(local, phase_timing=True, max_inflight=4)
+    eng = Engine(local, phase_timing=True, max_inflight=4, graphs=not args.no_graphs)
     # input tables built by the engine's own flush encoder
     job.materialize(lambda e, o: eng.build_table(e, o))
     tables = job.input_tables()
@@ -471,7 +479,9 @@ def main():
     achieved = alg[dominant] / (mean_ph[dominant] / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "algorithmic_bytes": alg[dominant],
+                "traffic": (NCU_TRAFFIC.get(dominant) if args.scale == 1.0 else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
+                "algorithmic_bytes": alg[dominant],
                 "phase_ms": mean_ph,
                 "per_kernel_gbs": {k: alg[k] / (mean_ph[k] / 1e3) / 1e9 for k in alg
                                    if mean_ph[k] > 0}}
