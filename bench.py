@@ -56,6 +56,10 @@ def parse_args():
     p.add_argument("--no-graphs", action="store_true",
                    help="launch every kernel directly instead of replaying CUDA graphs")
     p.add_argument("--batch-jobs", type=int, default=64)
+    p.add_argument("--served-dbs", type=int, default=16)
+    p.add_argument("--served-flushes", type=int, default=16,
+                   help="flushes per database (0: skip the served leg)")
+    p.add_argument("--served-loads", type=float, nargs="*", default=[0.5, 0.9])
     p.add_argument("--batch-steps", type=int, default=5,
                    help="timed repetitions of the 64-job set (0: skip the batched leg)")
     return p.parse_args()
@@ -331,6 +335,76 @@ def batched_leg(eng, args, rank, flush, torch):
     }
 
 
+def served_leg(args, local, rank, torch):
+    """Served compaction: simulated databases fed by a random-fill stream
+    (4 MiB flushes of 16-byte keys uniform over 2^26 and 100-byte values)
+    whose level-0 -> level-1 and deeper compactions run through one engine.
+    Capacity is measured closed-loop (every flush available at once); then
+    flushes arrive as a Poisson process at fractions of the served capacity.
+    The plain drop-in (one compaction at a time, host buffers) runs the same
+    traces.  Both engines are long-lived, as a server keeps them."""
+    from luda_b200 import served
+    from luda_b200.device_buffers import TorchUploader
+    from luda_b200.engine import Engine
+    builder = Engine(local, max_inflight=1)
+    flushes = served.make_flushes(args.served_dbs, args.served_flushes,
+                                  lambda e, o: builder.build_table(e, o), seed=3 + 100 * rank)
+    builder.close()
+    for fl in flushes:  # pinned host copies: an arriving table is in host memory
+        for f in fl:
+            t = torch.empty(len(f.data), dtype=torch.uint8).pin_memory()
+            t.copy_(torch.frombuffer(bytearray(f.data), dtype=torch.uint8))
+            f.data = t.numpy()
+    up = TorchUploader(local)
+    engines = {"served": Engine(local, max_inflight=4, pinned_reserve=4 << 30),
+               "plain": Engine(local, max_inflight=1, max_batch=1, pinned_reserve=4 << 30)}
+
+    def run(mode, rate):
+        eng = engines[mode]
+        if mode == "served":
+            srv = served.Server(eng, len(flushes), mode="served", upload=up.upload, free=up.free)
+        else:
+            srv = served.Server(eng, len(flushes), mode="plain")
+        s0 = eng.stats()
+        try:
+            st = srv.run(served.schedule(flushes, rate))
+        finally:
+            srv.close()
+        s1 = eng.stats()
+        out = st.summary()
+        out["offered_flushes_per_s"] = rate
+        out["engine"] = {k: s1[k] - s0[k] for k in ("batches", "graph_captures", "graph_replays",
+                                                    "direct_tails")}
+        out["engine"]["pinned_mib"] = s1["pinned_bytes"] / float(1 << 20)
+        return out
+
+    # warm-up: graphs, memory pools, pinned slabs, at every arrival pattern
+    run("served", None)
+    run("plain", None)
+    cap = run("served", None)
+    plain_cap = run("plain", None)
+    flush_rate = cap["flushes"] / cap["makespan_s"]
+    for rho in args.served_loads:
+        run("served", rho * flush_rate)
+    loads = {}
+    for rho in args.served_loads:
+        rate = rho * flush_rate
+        loads[f"{rho:g}"] = {"served": run("served", rate), "plain": run("plain", rate)}
+    for e in engines.values():
+        e.close()
+    n_flushes = sum(len(f) for f in flushes)
+    return {
+        "workload": f"served ({args.served_dbs} databases x {args.served_flushes} flushes of 4 MiB, "
+                    "random fill, 16 B keys uniform over 2^26, 100 B values)",
+        "flushes": n_flushes, "flush_mib": n_flushes * 4.0,
+        "capacity": {"served": cap, "plain": plain_cap,
+                     "speedup_served_vs_plain": cap["value"] / plain_cap["value"]},
+        "loads": loads,
+        "note": "job latency = engine submit -> completion; value = compaction input MiB / makespan; "
+                "loads are fractions of the closed-loop served capacity in flushes/s",
+    }
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -450,6 +524,9 @@ def main():
     batched = None
     if args.batch_steps > 0:
         batched = batched_leg(eng, args, rank, flush, torch)
+    served_res = None
+    if args.served_flushes > 0:
+        served_res = served_leg(args, local, rank, torch)
 
     # max over ranks
     if dist is not None:
@@ -512,6 +589,7 @@ def main():
                     "sequential_value": in_bytes / MiB / (float(np.mean(seq_ms)) / 1e3)},
             "roofline": roofline,
             "batched": batched,
+            "served": served_res,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,

@@ -46,6 +46,10 @@ typedef struct {
   int32_t max_inflight_jobs;    /* worker threads, i.e. batches on the device at once; 0 = 4 */
   uint32_t flags;               /* LC_FLAG_* */
   int32_t max_batch_jobs;       /* jobs one batch (one set of launches) may hold; 0 = 64 */
+  uint64_t max_batch_bytes;     /* input bytes a worker gathers into one batch (a larger
+                                   job still runs, alone); 0 = 512 MiB */
+  uint64_t pinned_reserve_bytes;/* pinned host memory for job outputs taken up front (more
+                                   is added on demand in slabs of >= 256 MiB); 0 = none */
 } lc_config;
 
 /* lc_config.flags: record CUDA events around each phase of every job on the
@@ -99,8 +103,11 @@ typedef struct {
   uint64_t smallest_snapshot; /* CompactionState::smallest_snapshot (db/db_impl.cc:1073) */
   lc_table_options options;
   int32_t inputs_on_device; /* 1: lc_table.data are device pointers on the engine's device */
-  int32_t outputs_on_device;/* 1: leave output bytes on the device (lc_job_out.data is a
-                               device pointer); 0: copy them to host memory */
+  int32_t outputs_on_device;/* 0: copy the output bytes to host memory;
+                               1: leave them on the device only (lc_job_out.data is a
+                               device pointer); 2: both -- host copy in data, device
+                               copy in device_data, e.g. to feed a later job's
+                               inputs_on_device without crossing PCIe again */
 } lc_job_desc;
 
 /* Output of one compaction: what DoCompactionWork records in
@@ -130,6 +137,12 @@ typedef struct {
   uint64_t key_bytes_in;    /* decoded internal-key bytes (input) */
   uint64_t value_bytes_out; /* value bytes written */
   uint64_t key_bytes_out;   /* internal-key bytes of the survivors */
+  const uint8_t* device_data; /* outputs_on_device 1 or 2: the output bytes in device
+                                 memory (same layout as data), else NULL */
+  uint32_t batch_jobs;        /* jobs in the batch that ran this job (device_ms and
+                                 kernel_launches are the batch's) */
+  double queue_ms;            /* lc_job_submit -> start of its batch (0 for synchronous
+                                 calls) */
 } lc_job_out;
 
 /* Engine lifetime.  An engine owns one CUDA device, its streams, a stream-
@@ -145,6 +158,14 @@ void lc_engine_destroy(lc_engine* e);
 lc_status lc_job_submit(lc_engine* e, const lc_job_desc* desc, lc_job** out);
 lc_status lc_job_wait(lc_job* j, int64_t timeout_ns);
 lc_status lc_job_result(lc_job* j, lc_job_out* out);
+/* Blocks until any of the n jobs (all of engine e) is done, or timeout_ns
+ * passes (< 0: forever; LC_ERR_TIMEOUT), and stores its position in *index.
+ * No counterpart in the reference (its compactions run one at a time on the
+ * Env background thread): it is the completion queue of a request loop that
+ * keeps many jobs in flight.  The finished job's own status comes from
+ * lc_job_wait / lc_job_result. */
+lc_status lc_job_wait_any(lc_engine* e, lc_job* const* jobs, int32_t n, int64_t timeout_ns,
+                          int32_t* index);
 void lc_job_release(lc_job* j);
 
 /* Synchronous compaction on the calling thread: the drop-in for one
@@ -162,6 +183,22 @@ lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_
  * lc_job_result its output.  Returns LC_OK when every job succeeded, else the
  * status of the first job that failed; argument errors create no handles. */
 lc_status lc_compact_batch(lc_engine* e, int32_t n, const lc_job_desc* descs, lc_job** jobs);
+
+/* Engine counters (no counterpart in the reference; the nearest is the
+ * per-level CompactionStats behind GetProperty("leveldb.stats"),
+ * db/db_impl.cc:1930). */
+typedef struct {
+  uint64_t batches;          /* batches run (a synchronous compaction is one) */
+  uint64_t jobs;             /* compaction jobs run */
+  uint64_t graph_captures;   /* kernel sequences captured into a new CUDA graph */
+  uint64_t graph_replays;    /* batches that replayed a cached graph */
+  uint64_t direct_tails;     /* batches whose shape was new: kernels launched directly */
+  uint64_t pinned_bytes;     /* pinned host memory held for outputs */
+  uint64_t pinned_free_bytes;/* ... of which not in use */
+  uint64_t inflight_bytes;   /* device-memory estimate of the admitted jobs */
+  uint64_t queued_jobs;      /* submitted jobs not yet admitted */
+} lc_engine_stats;
+lc_status lc_engine_get_stats(lc_engine* e, lc_engine_stats* out);
 
 /* Launch parameters the autotuner chooses (no counterpart in the reference). */
 typedef struct {

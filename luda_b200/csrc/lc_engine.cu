@@ -64,40 +64,82 @@ struct StatusError {
 
 uint64_t round16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
 
+// Pinned host memory for job outputs.  cudaMallocHost costs milliseconds
+// (page locking), far more than a small job's device time, so pinned memory
+// is taken from the driver in slabs of at least 256 MiB and handed out by
+// first fit from a free list with neighbour coalescing; it returns to the
+// driver only when the engine is destroyed.
 struct PinnedCache {
+  static constexpr uint64_t kSlab = 256ull << 20;
+  static constexpr uint64_t kAlign = 4096;
   std::mutex mu;
-  std::vector<std::pair<uint8_t*, uint64_t>> free_list;
+  std::vector<std::pair<uint8_t*, uint64_t>> slabs;
+  std::map<uint8_t*, uint64_t> free_blocks;  // start -> size, address order
+  uint64_t total = 0;                         // bytes in slabs
   uint8_t* take(uint64_t n, uint64_t* cap) {
-    {
-      std::lock_guard<std::mutex> g(mu);
-      size_t best = free_list.size();
-      for (size_t i = 0; i < free_list.size(); i++)
-        if (free_list[i].second >= n &&
-            (best == free_list.size() || free_list[i].second < free_list[best].second))
-          best = i;
-      if (best != free_list.size()) {
-        auto r = free_list[best];
-        free_list.erase(free_list.begin() + best);
-        *cap = r.second;
-        return r.first;
+    const uint64_t want = (std::max<uint64_t>(n, 1) + kAlign - 1) & ~(kAlign - 1);
+    while (true) {
+      uint64_t grow;
+      {
+        std::lock_guard<std::mutex> g(mu);
+        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+          if (it->second < want) continue;
+          uint8_t* p = it->first;
+          const uint64_t rest = it->second - want;
+          free_blocks.erase(it);
+          if (rest) free_blocks.emplace(p + want, rest);
+          *cap = want;
+          return p;
+        }
+        // grow geometrically, so that a growing working set pins few slabs
+        grow = std::max(std::max(kSlab, want), total / 2);
       }
+      // pinning takes milliseconds: not under the lock, so that returns
+      // (give) and other takes proceed meanwhile
+      if (!add_slab(grow)) return nullptr;
     }
-    uint64_t c = std::max<uint64_t>(n, 1 << 20);
-    c = (c + (1 << 20) - 1) & ~uint64_t((1 << 20) - 1);
+  }
+  bool add_slab(uint64_t sz) {
     void* p = nullptr;
-    if (cudaMallocHost(&p, c) != cudaSuccess) return nullptr;
-    *cap = c;
-    return (uint8_t*)p;
+    if (cudaMallocHost(&p, sz) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> g(mu);
+    slabs.emplace_back((uint8_t*)p, sz);
+    free_blocks.emplace((uint8_t*)p, sz);
+    total += sz;
+    return true;
   }
   void give(uint8_t* p, uint64_t cap) {
     if (!p) return;
     std::lock_guard<std::mutex> g(mu);
-    free_list.emplace_back(p, cap);
+    auto it = free_blocks.emplace(p, cap).first;
+    // merge with the following block, then with the preceding one, when they
+    // touch within one slab (two slabs may be adjacent in the address space,
+    // but each goes back to the driver on its own)
+    auto nx = std::next(it);
+    if (nx != free_blocks.end() && it->first + it->second == nx->first &&
+        same_slab(it->first, nx->first)) {
+      it->second += nx->second;
+      free_blocks.erase(nx);
+    }
+    if (it != free_blocks.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first && same_slab(pv->first, it->first)) {
+        pv->second += it->second;
+        free_blocks.erase(it);
+      }
+    }
+  }
+  bool same_slab(const uint8_t* a, const uint8_t* b) const {
+    for (auto& sl : slabs)
+      if (a >= sl.first && a < sl.first + sl.second) return b >= sl.first && b < sl.first + sl.second;
+    return false;
   }
   void clear() {
     std::lock_guard<std::mutex> g(mu);
-    for (auto& f : free_list) cudaFreeHost(f.first);
-    free_list.clear();
+    for (auto& sl : slabs) cudaFreeHost(sl.first);
+    slabs.clear();
+    free_blocks.clear();
+    total = 0;
   }
 };
 
@@ -121,11 +163,15 @@ struct lc_engine {
   std::mutex mu;
   std::condition_variable cv;
   std::condition_variable admit_cv;
+  std::mutex done_mu;  // completion of any job (lc_job_wait_any)
+  std::condition_variable done_cv;
   std::deque<lc_job*> queue;
   std::vector<std::thread> workers;
   bool stop = false;
   uint64_t inflight_bytes = 0;
+  cudaStream_t free_st = nullptr;  // stream-ordered frees of released outputs
   uint32_t max_batch = 64;
+  uint64_t max_batch_bytes = 512ull << 20;
   bool use_graphs = true;
   std::mutex tun_mu;
   Tunables tun;
@@ -134,6 +180,8 @@ struct lc_engine {
   std::vector<std::unique_ptr<lc_slot>> slots;
   std::mutex slot_mu;
   std::vector<lc_slot*> free_slots;
+  // counters for lc_engine_get_stats
+  std::atomic<uint64_t> n_batches{0}, n_jobs{0}, n_captures{0}, n_replays{0}, n_direct{0};
   lc_slot* take_slot();
   void put_slot(lc_slot* s);
   Tunables tuning() {
@@ -166,13 +214,16 @@ struct lc_job {
   std::string err;
   uint8_t* h_out = nullptr;
   uint64_t h_out_cap = 0;
-  uint8_t* d_out = nullptr;  // kept when outputs_on_device
+  uint8_t* d_out = nullptr;  // kept when outputs_on_device is 1 or 2
   std::vector<uint64_t> file_offset, file_size, file_entries, small_off, large_off;
   std::vector<uint32_t> small_len, large_len;
   std::vector<uint8_t> key_bytes;
   uint64_t bytes_in = 0, bytes_out = 0, entries_in = 0, entries_out = 0;
   double device_ms = 0;
   uint32_t launches = 0;
+  uint32_t batch_jobs = 1;
+  std::chrono::steady_clock::time_point t_submit;
+  double queue_ms = 0;  // submit -> start of the batch that ran it
   std::vector<float> phase_ms;
   uint64_t key_bytes_in = 0, kept_key_bytes = 0, kept_value_bytes = 0;
   uint64_t est_bytes = 0;
@@ -527,13 +578,17 @@ struct lc_slot {
     d_jobs = nullptr;
     st = nullptr;
   }
-  // Launches the post-parse sequence for `bt`, through a cached graph when
-  // one exists for the same grid shapes, else by capturing one.
-  void run_tail(const Batch& bt, bool decode_merge, bool use_graph, PhaseTimer& T) {
+  std::map<std::string, uint32_t> seen;  // shape keys met without a graph
+  // Launches the post-parse sequence for `bt`: replays the cached graph of
+  // the same grid shapes, or captures one when the shape comes back a second
+  // time (capturing and instantiating cost more than launching directly, so
+  // a shape met once runs without a graph).  Returns 0 direct, 1 captured,
+  // 2 replayed.
+  int run_tail(const Batch& bt, bool decode_merge, bool use_graph, PhaseTimer& T) {
     if (!use_graph) {
       launch_tail(bt, decode_merge, st, T);
       CK(cudaGetLastError());
-      return;
+      return 0;
     }
     char key[256];
     snprintf(key, sizeof(key), "%d|%d|%u|%u|%u|%u|%u|%llu|%llu|%u|%u|%u|%u|%u", (int)T.on,
@@ -544,6 +599,13 @@ struct lc_slot {
     auto it = graphs.find(key);
     bool fresh = false;
     if (it == graphs.end()) {
+      if (seen.size() > 1024) seen.clear();
+      if (++seen[key] < 2) {
+        launch_tail(bt, decode_merge, st, T);
+        CK(cudaGetLastError());
+        return 0;
+      }
+      seen.erase(key);
       if (graphs.size() >= 24) {  // evict the least recently used
         auto victim = graphs.begin();
         for (auto g = graphs.begin(); g != graphs.end(); ++g)
@@ -578,6 +640,7 @@ struct lc_slot {
     CK(cudaGraphLaunch(it->second.exec, st));
     if (!fresh) note_launch(it->second.launches);
     T.borrow(it->second.events);
+    return fresh ? 1 : 2;
   }
 };
 
@@ -863,7 +926,10 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
     CK(cudaMemcpyAsync(slot.d_jobs, hj.data(), sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
     T.start();
     // ---- decode, merge, drop, partition, encode: one graph launch
-    slot.run_tail(bt, true, e->use_graphs, T);
+    const int how = slot.run_tail(bt, true, e->use_graphs, T);
+    (how == 0 ? e->n_direct : how == 1 ? e->n_captures : e->n_replays)++;
+    e->n_batches++;
+    e->n_jobs += B;
     // ---- per-job results
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
@@ -889,7 +955,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       }
       lc_job* j = r.j;
       const uint64_t nbytes = hc[i].bytes_out;
-      if (!j->outputs_on_device && nbytes) {
+      if (j->outputs_on_device != 1 && nbytes) {
         j->h_out = e->pinned.take(nbytes, &j->h_out_cap);
         if (!j->h_out) {
           job_fail(r, LC_ERR_NO_MEMORY, "pinned host buffer");
@@ -919,7 +985,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       j->entries_out = hc[i].n_kept;
       j->kept_key_bytes = hc[i].kept_key_bytes;
       j->kept_value_bytes = hc[i].kept_value_bytes;
-      if (j->outputs_on_device) j->d_out = r.J.out;
+      if (j->outputs_on_device == 1 || j->outputs_on_device == 2) j->d_out = r.J.out;
     }
     T.mark(kDownload);
     CK(cudaEventRecord(ev1, st));
@@ -935,6 +1001,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       j->device_ms = ms;
       j->phase_ms = ph;
       j->launches = launches;
+      j->batch_jobs = B;
       if (!runs[i].failed) j->status = LC_OK;
       if (j->d_out) keep.push_back(j->d_out);
     }
@@ -1110,9 +1177,19 @@ uint64_t estimate_bytes(const lc_job* j) {
 }
 
 void finish(lc_job* j) {
+  lc_engine* e = j->eng;
+  {
+    std::lock_guard<std::mutex> g(j->mu);
+    j->done = true;
+    j->cv.notify_all();
+  }
+  std::lock_guard<std::mutex> g(e->done_mu);
+  e->done_cv.notify_all();
+}
+
+bool job_done(lc_job* j) {
   std::lock_guard<std::mutex> g(j->mu);
-  j->done = true;
-  j->cv.notify_all();
+  return j->done;
 }
 
 // Worker: takes the head of the queue plus every further queued job that
@@ -1122,7 +1199,7 @@ void worker_main(lc_engine* e, lc_slot* wslot) {
   lc_slot& slot = *wslot;
   while (true) {
     std::vector<lc_job*> batch;
-    uint64_t bytes = 0;
+    uint64_t bytes = 0, in_bytes = 0;
     {
       std::unique_lock<std::mutex> lk(e->mu);
       e->cv.wait(lk, [&] { return e->stop || !e->queue.empty(); });
@@ -1142,13 +1219,19 @@ void worker_main(lc_engine* e, lc_slot* wslot) {
           }
           break;
         }
-        if (!batch.empty() && e->inflight_bytes + bytes + j->est_bytes > e->budget) break;
+        if (!batch.empty() && (e->inflight_bytes + bytes + j->est_bytes > e->budget ||
+                               in_bytes + j->bytes_in > e->max_batch_bytes))
+          break;
         batch.push_back(j);
         bytes += j->est_bytes;
+        in_bytes += j->bytes_in;
         e->queue.pop_front();
       }
       e->inflight_bytes += bytes;
     }
+    const auto t_start = std::chrono::steady_clock::now();
+    for (auto* j : batch)
+      j->queue_ms = std::chrono::duration<double, std::milli>(t_start - j->t_submit).count();
     if (e->stop) {
       for (auto* j : batch) j->status = LC_ERR_SHUTDOWN;
     } else {
@@ -1208,6 +1291,8 @@ lc_status copy_desc(lc_job* j, const lc_job_desc* d) {
   j->smallest_snapshot = d->smallest_snapshot;
   j->opt = d->options;
   j->inputs_on_device = d->inputs_on_device;
+  if (d->outputs_on_device < 0 || d->outputs_on_device > 2)
+    return fail(LC_ERR_INVALID_ARG, "outputs_on_device must be 0, 1 or 2");
   j->outputs_on_device = d->outputs_on_device;
   for (auto& t : j->tables) j->bytes_in += t.size;
   return LC_OK;
@@ -1216,7 +1301,7 @@ lc_status copy_desc(lc_job* j, const lc_job_desc* d) {
 void fill_out(lc_job* j, lc_job_out* o) {
   memset(o, 0, sizeof(*o));
   o->n_files = (int32_t)j->file_size.size();
-  o->data = j->outputs_on_device ? j->d_out : j->h_out;
+  o->data = j->outputs_on_device == 1 ? j->d_out : j->h_out;
   o->file_offset = j->file_offset.data();
   o->file_size = j->file_size.data();
   o->file_entries = j->file_entries.data();
@@ -1237,6 +1322,9 @@ void fill_out(lc_job* j, lc_job_out* o) {
   o->key_bytes_in = j->key_bytes_in;
   o->value_bytes_out = j->kept_value_bytes;
   o->key_bytes_out = j->kept_key_bytes;
+  o->device_data = j->d_out;
+  o->batch_jobs = j->batch_jobs;
+  o->queue_ms = j->queue_ms;
 }
 
 void host_crc_xpow(std::vector<uint32_t>& t) {
@@ -1274,21 +1362,27 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
   if (!out) return fail(LC_ERR_INVALID_ARG, "null engine pointer");
   lc_engine* e = new (std::nothrow) lc_engine();
   if (!e) return fail(LC_ERR_NO_MEMORY, "engine");
+  uint64_t pinned_reserve = 0;
   if (cfg) {
     e->device = cfg->device;
     if (cfg->device_budget_bytes) e->budget = cfg->device_budget_bytes;
     if (cfg->max_inflight_jobs > 0) e->max_inflight = cfg->max_inflight_jobs;
     if (cfg->max_batch_jobs > 0) e->max_batch = (uint32_t)cfg->max_batch_jobs;
+    if (cfg->max_batch_bytes) e->max_batch_bytes = cfg->max_batch_bytes;
+    pinned_reserve = cfg->pinned_reserve_bytes;
     e->flags = cfg->flags;
     e->use_graphs = (cfg->flags & LC_FLAG_NO_GRAPHS) == 0;
   }
   std::vector<lc_slot*> wslots;
   try {
     CK(cudaSetDevice(e->device));
+    if (pinned_reserve && !e->pinned.add_slab(pinned_reserve))
+      throw CudaError{cudaErrorMemoryAllocation, "cudaMallocHost (pinned_reserve_bytes)"};
     cudaMemPool_t pool;
     CK(cudaDeviceGetDefaultMemPool(&pool, e->device));
     uint64_t thr = ~0ull;
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    CK(cudaStreamCreateWithFlags(&e->free_st, cudaStreamNonBlocking));
     decode_kernel_attributes();
     encode_kernel_attributes();
     CK(cudaGetLastError());
@@ -1305,6 +1399,8 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
   } catch (const CudaError& ce) {
     std::string m = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
     if (e->crc_xpow) cudaFree(e->crc_xpow);
+    if (e->free_st) cudaStreamDestroy(e->free_st);
+    e->pinned.clear();
     delete e;
     return fail(LC_ERR_CUDA, m);
   }
@@ -1323,6 +1419,10 @@ void lc_engine_destroy(lc_engine* e) {
   e->admit_cv.notify_all();
   for (auto& w : e->workers) w.join();
   cudaSetDevice(e->device);
+  if (e->free_st) {
+    cudaStreamSynchronize(e->free_st);
+    cudaStreamDestroy(e->free_st);
+  }
   e->pinned.clear();
   cudaFree(e->crc_xpow);
   delete e;  // destroys the slots
@@ -1349,6 +1449,7 @@ lc_status lc_job_submit(lc_engine* e, const lc_job_desc* desc, lc_job** out) {
       delete j;
       return fail(LC_ERR_SHUTDOWN, "engine stopping");
     }
+    j->t_submit = std::chrono::steady_clock::now();
     e->queue.push_back(j);
   }
   e->cv.notify_one();
@@ -1368,6 +1469,35 @@ lc_status lc_job_wait(lc_job* j, int64_t timeout_ns) {
   return j->status;
 }
 
+lc_status lc_job_wait_any(lc_engine* e, lc_job* const* jobs, int32_t n, int64_t timeout_ns,
+                          int32_t* index) {
+  if (!e || !index || n <= 0 || !jobs) return fail(LC_ERR_INVALID_ARG, "null argument");
+  for (int32_t i = 0; i < n; i++)
+    if (!jobs[i] || jobs[i]->eng != e) return fail(LC_ERR_INVALID_ARG, "job of another engine");
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::nanoseconds(
+                                                                 timeout_ns < 0 ? 0 : timeout_ns);
+  std::unique_lock<std::mutex> lk(e->done_mu);
+  while (true) {
+    // finish() notifies under done_mu, so no completion is missed between
+    // this check and the wait
+    for (int32_t i = 0; i < n; i++)
+      if (job_done(jobs[i])) {
+        *index = i;
+        return LC_OK;
+      }
+    if (timeout_ns < 0) {
+      e->done_cv.wait(lk);
+    } else if (e->done_cv.wait_until(lk, deadline) == std::cv_status::timeout) {
+      for (int32_t i = 0; i < n; i++)
+        if (job_done(jobs[i])) {
+          *index = i;
+          return LC_OK;
+        }
+      return LC_ERR_TIMEOUT;
+    }
+  }
+}
+
 lc_status lc_job_result(lc_job* j, lc_job_out* out) {
   if (!j || !out) return fail(LC_ERR_INVALID_ARG, "null argument");
   {
@@ -1384,8 +1514,10 @@ void lc_job_release(lc_job* j) {
   if (j->h_out) j->eng->pinned.give(j->h_out, j->h_out_cap);
   if (j->d_out) {
     // the job has completed; return the output to the stream-ordered pool
+    // (on the engine's own non-blocking stream: the legacy default stream
+    // would order the free after every blocking stream of the process)
     cudaSetDevice(j->eng->device);
-    cudaFreeAsync(j->d_out, 0);
+    cudaFreeAsync(j->d_out, j->eng->free_st);
   }
   delete j;
 }
@@ -1445,6 +1577,27 @@ lc_status lc_compact_batch(lc_engine* e, int32_t n, const lc_job_desc* descs, lc
     jobs[i] = all[i];
   }
   return first;
+}
+
+lc_status lc_engine_get_stats(lc_engine* e, lc_engine_stats* out) {
+  if (!e || !out) return fail(LC_ERR_INVALID_ARG, "null argument");
+  memset(out, 0, sizeof(*out));
+  out->batches = e->n_batches;
+  out->jobs = e->n_jobs;
+  out->graph_captures = e->n_captures;
+  out->graph_replays = e->n_replays;
+  out->direct_tails = e->n_direct;
+  {
+    std::lock_guard<std::mutex> g(e->pinned.mu);
+    out->pinned_bytes = e->pinned.total;
+    for (auto& b : e->pinned.free_blocks) out->pinned_free_bytes += b.second;
+  }
+  {
+    std::lock_guard<std::mutex> g(e->mu);
+    out->inflight_bytes = e->inflight_bytes;
+    out->queued_jobs = e->queue.size();
+  }
+  return LC_OK;
 }
 
 lc_status lc_get_tuning(lc_engine* e, lc_tuning* out) {

@@ -36,7 +36,14 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "corruption", 3: "cuda error", 4: "
 class LcConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("device_budget_bytes", C.c_uint64),
                 ("max_inflight_jobs", C.c_int32), ("flags", C.c_uint32),
-                ("max_batch_jobs", C.c_int32)]
+                ("max_batch_jobs", C.c_int32), ("max_batch_bytes", C.c_uint64),
+                ("pinned_reserve_bytes", C.c_uint64)]
+
+
+class LcEngineStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "batches", "jobs", "graph_captures", "graph_replays", "direct_tails", "pinned_bytes",
+        "pinned_free_bytes", "inflight_bytes", "queued_jobs")]
 
 
 class LcTuning(C.Structure):
@@ -76,7 +83,8 @@ class LcJobOut(C.Structure):
                 ("kernel_launches", C.c_uint32), ("n_phases", C.c_uint32),
                 ("phase_name", C.POINTER(C.c_char_p)), ("phase_ms", C.POINTER(C.c_float)),
                 ("key_bytes_in", C.c_uint64), ("value_bytes_out", C.c_uint64),
-                ("key_bytes_out", C.c_uint64)]
+                ("key_bytes_out", C.c_uint64), ("device_data", C.c_void_p),
+                ("batch_jobs", C.c_uint32), ("queue_ms", C.c_double)]
 
 LC_FLAG_PHASE_TIMING = 1
 LC_FLAG_NO_GRAPHS = 2
@@ -85,7 +93,8 @@ LC_FLAG_NO_GRAPHS = 2
 EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wait",
            "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
            "lc_status_string", "lc_version", "lc_crc32c", "lc_crc32c_noalloc",
-           "lc_compact_batch", "lc_get_tuning", "lc_set_tuning", "lc_autotune"]
+           "lc_compact_batch", "lc_get_tuning", "lc_set_tuning", "lc_autotune",
+           "lc_job_wait_any", "lc_engine_get_stats"]
 
 
 class LcError(RuntimeError):
@@ -120,6 +129,11 @@ def load_library(path: str = LIB_PATH):
     l.lc_compact.argtypes = [C.c_void_p, C.POINTER(LcJobDesc), C.POINTER(LcJobOut),
                              C.POINTER(C.c_void_p)]
     l.lc_compact.restype = C.c_int
+    l.lc_engine_get_stats.argtypes = [C.c_void_p, C.POINTER(LcEngineStats)]
+    l.lc_engine_get_stats.restype = C.c_int
+    l.lc_job_wait_any.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.c_int64,
+                                  C.POINTER(C.c_int32)]
+    l.lc_job_wait_any.restype = C.c_int
     l.lc_compact_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(LcJobDesc),
                                    C.POINTER(C.c_void_p)]
     l.lc_compact_batch.restype = C.c_int
@@ -162,13 +176,15 @@ class CompactionResult:
     entries_in: int
     entries_out: int
     device_ms: float
-    device_ptr: Optional[int] = None  # output base when left on the device
+    device_ptr: Optional[int] = None  # output base in device memory (outputs_on_device 1 or 2)
     file_offsets: Optional[List[int]] = None
     kernel_launches: int = 0
     phase_ms: Optional[dict] = None
     key_bytes_in: int = 0
     value_bytes_out: int = 0
     key_bytes_out: int = 0
+    batch_jobs: int = 1
+    queue_ms: float = 0.0
     _handle: object = None
 
     def release(self):
@@ -200,9 +216,15 @@ class _JobHandle:
 
 
 def _u8(b) -> np.ndarray:
+    """A uint8 array over b without copying when b is a contiguous buffer."""
     if isinstance(b, np.ndarray):
         return np.ascontiguousarray(b, dtype=np.uint8)
-    return np.frombuffer(bytes(b), np.uint8) if len(b) else np.zeros(1, np.uint8)
+    if not len(b):
+        return np.zeros(1, np.uint8)
+    try:
+        return np.frombuffer(b, np.uint8)
+    except (TypeError, ValueError):
+        return np.frombuffer(bytes(b), np.uint8)
 
 
 class _Keep:
@@ -220,7 +242,7 @@ def table_options(o: TableOptions) -> LcTableOptions:
 
 
 def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[int]] = None,
-              outputs_on_device: bool = False) -> LcJobDesc:
+              outputs_on_device: int = 0) -> LcJobDesc:
     """The descriptor a patched DoCompactionWork would build from its
     Compaction: runs in MakeInputIterator order, grandparents_, and every file
     at levels >= L+2 for the base-level test."""
@@ -234,7 +256,7 @@ def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[
             a = _u8(f.data)
             keep.objs.append(a)
             t_arr[i].data = a.ctypes.data
-        t_arr[i].size = len(f.data)
+        t_arr[i].size = len(f.data) if f.data is not None else f.file_size
     rc = (C.c_int32 * max(1, len(runs)))(*[len(r) for r in runs])
 
     def ranges(fs):
@@ -253,10 +275,12 @@ def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[
     keep.objs += [t_arr, rc, gpa, ba]
     return LcJobDesc(job.level, len(tables), t_arr, len(runs), rc, len(gp), gpa, len(base), ba,
                      job.smallest_snapshot(), table_options(job.options),
-                     1 if device_tables is not None else 0, 1 if outputs_on_device else 0)
+                     1 if device_tables is not None else 0, int(outputs_on_device))
 
 
-def _result(out: LcJobOut, on_device: bool) -> CompactionResult:
+def _result(out: LcJobOut, outputs_on_device) -> CompactionResult:
+    """outputs_on_device: 0/False host bytes, 1/True device only, 2 both."""
+    on_device = int(outputs_on_device) == 1
     files = []
     offs = []
     whole = None
@@ -273,19 +297,22 @@ def _result(out: LcJobOut, on_device: bool) -> CompactionResult:
         files.append(OutputFile(data, sm, lg, int(out.file_entries[i])))
     phases = {out.phase_name[i].decode(): out.phase_ms[i] for i in range(out.n_phases)}
     return CompactionResult(files, out.bytes_in, out.bytes_out, out.entries_in, out.entries_out,
-                            out.device_ms, out.data if on_device else None, offs,
+                            out.device_ms, out.device_data, offs,
                             out.kernel_launches, phases or None, out.key_bytes_in,
-                            out.value_bytes_out, out.key_bytes_out)
+                            out.value_bytes_out, out.key_bytes_out, out.batch_jobs,
+                            out.queue_ms)
 
 
 class Engine:
     """One CUDA device's compaction engine (``lc_engine``)."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 0, max_inflight: int = 4,
-                 phase_timing: bool = False, graphs: bool = True, max_batch: int = 0):
+                 phase_timing: bool = False, graphs: bool = True, max_batch: int = 0,
+                 max_batch_bytes: int = 0, pinned_reserve: int = 0):
         self.lib = load_library()
         flags = (LC_FLAG_PHASE_TIMING if phase_timing else 0) | (0 if graphs else LC_FLAG_NO_GRAPHS)
-        cfg = LcConfig(device, budget_bytes, max_inflight, flags, max_batch)
+        cfg = LcConfig(device, budget_bytes, max_inflight, flags, max_batch, max_batch_bytes,
+                       pinned_reserve)
         h = C.c_void_p()
         st = self.lib.lc_engine_create(C.byref(cfg), C.byref(h))
         if st != LC_OK:
@@ -317,7 +344,7 @@ class Engine:
             raise LcError(st, self.lib.lc_last_error().decode())
 
     def prepare(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: bool = False) -> "PreparedJob":
+                outputs_on_device: int = 0) -> "PreparedJob":
         """Builds the C descriptor once, for repeated runs of the same job."""
         keep = _Keep()
         return PreparedJob(make_desc(job, keep, device_tables, outputs_on_device), keep,
@@ -332,7 +359,7 @@ class Engine:
         return res
 
     def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: bool = False) -> CompactionResult:
+                outputs_on_device: int = 0) -> CompactionResult:
         return self.run(self.prepare(job, device_tables, outputs_on_device))
 
     @staticmethod
@@ -372,8 +399,27 @@ class Engine:
         return res
 
     def compact_batch(self, jobs: Sequence[CompactionJob],
-                      outputs_on_device: bool = False) -> List[CompactionResult]:
+                      outputs_on_device: int = 0) -> List[CompactionResult]:
         return self.run_batch([self.prepare(j, None, outputs_on_device) for j in jobs])
+
+    def stats(self) -> dict:
+        """Engine counters (``lc_engine_get_stats``)."""
+        st = LcEngineStats()
+        self._check(self.lib.lc_engine_get_stats(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in LcEngineStats._fields_}
+
+    def wait_any(self, jobs: Sequence["AsyncJob"], timeout_s: float = -1.0) -> Optional[int]:
+        """Index of a finished job among ``jobs`` (``lc_job_wait_any``), or
+        None when ``timeout_s`` passes first."""
+        arr = (C.c_void_p * max(1, len(jobs)))(*[j.h for j in jobs])
+        idx = C.c_int32(-1)
+        st = self.lib.lc_job_wait_any(self.h, arr, len(jobs),
+                                      int(timeout_s * 1e9) if timeout_s >= 0 else -1,
+                                      C.byref(idx))
+        if st == 6:
+            return None
+        self._check(st)
+        return idx.value
 
     def tuning(self) -> dict:
         t = LcTuning()
@@ -439,11 +485,11 @@ class Engine:
 class PreparedJob:
     desc: LcJobDesc
     keep: object
-    outputs_on_device: bool
+    outputs_on_device: int
 
 
 class AsyncJob:
-    def __init__(self, eng: Engine, h, keep, outputs_on_device: bool = False):
+    def __init__(self, eng: Engine, h, keep, outputs_on_device: int = 0):
         self.eng, self.h, self.keep = eng, h, keep
         self.outputs_on_device = outputs_on_device
 

@@ -76,11 +76,15 @@ def test_batch_uneven_jobs_match_oracle(engine, mix_jobs, mix_want):
 
 def test_graph_replay_for_other_batches(mix_jobs, mix_want):
     with Engine(0) as e:
-        first = e.compact_batch(mix_jobs[:6])
-        again = e.compact_batch(mix_jobs[:6])  # same shapes: replayed graph
+        first = e.compact_batch(mix_jobs[:6])  # new shape: direct launches
+        again = e.compact_batch(mix_jobs[:6])  # second sighting: captured
+        third = e.compact_batch(mix_jobs[:6])  # replayed
         other = e.compact_batch(mix_jobs[6:])
-        assert [r.file_bytes() for r in first] == mix_want[:6]
-        assert [r.file_bytes() for r in again] == mix_want[:6]
+        st = e.stats()
+        assert st["direct_tails"] >= 1 and st["graph_captures"] >= 1 and st["graph_replays"] >= 1
+        assert st["batches"] == 4 and st["jobs"] == 12
+        for rs in (first, again, third):
+            assert [r.file_bytes() for r in rs] == mix_want[:6]
         assert [r.file_bytes() for r in other] == mix_want[6:]
 
 
