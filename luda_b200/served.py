@@ -356,6 +356,10 @@ class ServeStats:
             "queue_ms_mean": float(q.mean()), "queue_ms_p99": float(np.percentile(q, 99)),
             "device_ms_mean": float(np.mean([j.device_ms for j in self.jobs])) if self.jobs else 0,
             "batch_jobs_mean": float(np.mean([j.batch_jobs for j in self.jobs])) if self.jobs else 0,
+            "slowest": [{"latency_ms": j.latency_ms, "queue_ms": j.queue_ms,
+                         "device_ms": j.device_ms, "batch_jobs": j.batch_jobs, "level": j.level,
+                         "input_mib": j.input_bytes / float(1 << 20), "submit_s": j.submit_s}
+                        for j in sorted(self.jobs, key=lambda j: -j.latency_ms)[:4]],
         }
 
 

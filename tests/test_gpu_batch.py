@@ -82,7 +82,7 @@ def test_graph_replay_for_other_batches(mix_jobs, mix_want):
         other = e.compact_batch(mix_jobs[6:])
         st = e.stats()
         assert st["direct_tails"] >= 1 and st["graph_captures"] >= 1 and st["graph_replays"] >= 1
-        assert st["batches"] == 4 and st["jobs"] == 12
+        assert st["batches"] == 4 and st["jobs"] == 24
         for rs in (first, again, third):
             assert [r.file_bytes() for r in rs] == mix_want[:6]
         assert [r.file_bytes() for r in other] == mix_want[6:]
