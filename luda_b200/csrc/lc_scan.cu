@@ -113,9 +113,11 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
 }
 
 // Exclusive scan across the CTA; returns the exclusive prefix, *total = sum.
+// The total has its own slot: with 32 warps every one of warp_sums[0..31]
+// holds a warp's exclusive prefix.
 template <typename T>
 __device__ __forceinline__ T block_excl_scan(T v, T* total) {
-  __shared__ T warp_sums[32];
+  __shared__ T warp_sums[33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
   T incl = warp_incl_scan(v);
@@ -125,11 +127,11 @@ __device__ __forceinline__ T block_excl_scan(T v, T* total) {
     T w = lane < nwarps ? warp_sums[lane] : T(0);
     T wi = warp_incl_scan(w);
     if (lane < nwarps) warp_sums[lane] = wi - w;
-    if (lane == nwarps - 1) warp_sums[31] = wi;
+    if (lane == 31) warp_sums[32] = wi;  // lanes past nwarps add nothing
   }
   __syncthreads();
   T res = warp_sums[warp] + incl - v;
-  *total = warp_sums[31];
+  *total = warp_sums[32];
   __syncthreads();
   return res;
 }

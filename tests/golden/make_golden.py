@@ -10,6 +10,7 @@ smallest/largest internal keys, so that the GPU tests can check byte identity
 on a machine where the reference sources are absent.
 
 Run from the repository root:  python tests/golden/make_golden.py
+(``--large`` re-records only the 1 GiB cases, keeping the others.)
 """
 from __future__ import annotations
 
@@ -38,6 +39,13 @@ WORKLOAD_CASES = [
     ("large_B_small", "large_l2_l3", {"run": "B", "seed": 4, "scale": 0.05}),
 ] + [(f"batched_{i}", "batched_job", {"seed": i, "scale": 0.1}) for i in range(4)]
 
+# The 1 GiB L2->L3 compactions at size (1 + 15 tables of 64 MiB): run A with
+# 8-byte keys and 1 KiB values, run B with 24-byte keys and 32-byte values.
+LARGE_CASES = [
+    ("large_A", "large_l2_l3", {"run": "A", "seed": 4, "scale": 1.0}),
+    ("large_B", "large_l2_l3", {"run": "B", "seed": 4, "scale": 1.0}),
+]
+
 
 def sha(b: bytes) -> str:
     return hashlib.sha256(b).hexdigest()
@@ -47,7 +55,7 @@ def make_job(gen: str, kwargs: dict):
     return getattr(workloads, gen)(**kwargs)
 
 
-def record(name, job, spec):
+def record(name, job, spec, large=False):
     job.materialize(lambda e, o: oracle.build_table(e, o, "ref"))
     # the restatement's builder must agree with the reference's
     for f in job.files:
@@ -64,19 +72,27 @@ def record(name, job, spec):
                     for (d, s, l) in full],
         "ref_seconds": secs,
     }
+    if large:
+        rec["large"] = True
     print(f"{name:28s} in={job.input_bytes():>10d} files={len(full):3d} ref={secs * 1e3:8.1f} ms",
           flush=True)
     return rec
 
 
-def main():
+def main(argv):
     if not oracle.has_ref():
         oracle.build(ref=True)
     cases = []
-    for name, gen, kw in WORKLOAD_CASES:
-        cases.append(record(name, make_job(gen, kw), {"workload": gen, "kwargs": kw}))
-    for job in edge_jobs.all_cases():
-        cases.append(record(job.name, job, {"edge": job.name}))
+    if "--large" in argv:
+        with open(OUT) as f:
+            cases = [c for c in json.load(f)["cases"] if not c.get("large")]
+    else:
+        for name, gen, kw in WORKLOAD_CASES:
+            cases.append(record(name, make_job(gen, kw), {"workload": gen, "kwargs": kw}))
+        for job in edge_jobs.all_cases():
+            cases.append(record(job.name, job, {"edge": job.name}))
+    for name, gen, kw in LARGE_CASES:
+        cases.append(record(name, make_job(gen, kw), {"workload": gen, "kwargs": kw}, large=True))
     with open(OUT, "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py",
                    "reference": "xpsair/luda CPU DoCompactionWork (GPU_ACCELERATE 0)",
@@ -85,4 +101,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -28,7 +28,7 @@ def sha(b):
     return hashlib.sha256(b).hexdigest()
 
 
-ALL = _golden()
+ALL = [c for c in _golden() if not c.get("large")]  # 1 GiB cases: test_gpu_large.py
 
 
 @pytest.fixture(scope="module")
