@@ -449,14 +449,29 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
   }
 }
 
-// One warp per output data block.  The block is assembled in this warp's
-// shared-memory stage at the same 16-byte phase as its destination, entries are
-// copied by four 8-lane groups with 16-byte loads, the CRC32C trailer is
-// computed from shared memory, and the block leaves with 16-byte stores.
-// Blocks larger than the stage are written straight to global memory.
-constexpr uint32_t kEncWarps = 4;
-constexpr uint32_t kEncStage = 8448;    // bytes per warp: 8 KiB blocks + phase + trailer
-constexpr uint32_t kEncScratch = 8192;  // bytes per warp: gathered 16-byte source chunks
+// One warp per output data block, which is produced as the 16-byte chunks of
+// the global 16-byte grid that cover it.  Lane l takes a contiguous run of
+// chunks: for each chunk it copies the bytes of the entries' headers, key
+// deltas and values (and of the restart array) that fall in the chunk into a
+// 16-byte slot in shared memory, feeds them to its CRC32C register and stores
+// the chunk with one 16-byte store (byte stores for the partial chunks at the
+// block's two ends).  The lanes' CRC registers are combined with shifts
+// x^(8n) mod P.  The per-warp entry table (output offset, key/value sources
+// and lengths) holds up to kEncMaxEnt entries; larger blocks take the direct
+// path.
+constexpr uint32_t kEncWarps = 8;
+constexpr uint32_t kEncMaxEnt = 128;
+constexpr uint32_t kEncSlot = 20;  // bytes per lane slot: 5 words, distinct banks
+struct EncWarp {
+  uint32_t off[kEncMaxEnt + 1];  // entry output offset in the block (+ end)
+  uint32_t ksrc[kEncMaxEnt];     // key delta: offset in the key arena
+  uint32_t vsrc[kEncMaxEnt];     // value: offset in the input bytes
+  uint32_t kd[kEncMaxEnt];       // key delta length
+  uint32_t vl[kEncMaxEnt];       // value length
+  uint32_t sh[kEncMaxEnt];       // shared prefix length
+  uint8_t slot[32 * kEncSlot];
+};
+constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * sizeof(EncWarp);
 
 __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab, uint64_t b,
                                            uint8_t* dst, uint32_t lane) {
@@ -503,181 +518,199 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab,
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
-// Copies len bytes from global src to shared dst with the 8 lanes of one
-// group: 16-byte loads of the aligned chunks that cover src, bytes scattered
-// into place.  Chunks that would read past `limit` fall back to byte loads.
-__device__ __forceinline__ void group_copy(const uint8_t* src, uint32_t len, uint8_t* dst,
-                                           uint32_t sub, const uint8_t* limit) {
-  if (len == 0) return;
+// Prefetch into L1 the 128-byte lines of [p, p + n).
+__device__ __forceinline__ void prefetch_l1(const uint8_t* p, uint32_t n) {
+  if (!n) return;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127);
+  const uintptr_t e = reinterpret_cast<uintptr_t>(p) + n;
+  for (uintptr_t q = a; q < e; q += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+}
+
+// Copies L <= 16 bytes from global src to slot[d, d + L) (d + L <= 16): up to
+// five independent 4-byte loads of the aligned words covering src (the
+// arenas are padded, so the words past the end are readable), funnel shifts
+// that line the bytes up, predicated byte stores.
+__device__ __forceinline__ void copy_piece(uint8_t* slot, uint32_t d, const uint8_t* src, uint32_t L) {
   const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-  const uintptr_t base = a & ~uintptr_t(15);
-  const uint32_t lead = (uint32_t)(a - base);
-  const uint32_t nch = (lead + len + 15) >> 4;
-  for (uint32_t c = sub; c < nch; c += 8) {
-    const uint8_t* q = reinterpret_cast<const uint8_t*>(base + 16ull * c);
-    uint4 v;
-    if (q + 16 <= limit) {
-      v = *reinterpret_cast<const uint4*>(q);
-    } else {
-      uint32_t w[4] = {0, 0, 0, 0};
-      for (int i = 0; i < 16; i++)
-        if (q + i < limit) w[i >> 2] |= (uint32_t)q[i] << (8 * (i & 3));
-      v = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-    const uint32_t o = 16 * c - lead;  // offset of chunk byte 0 in dst (may wrap)
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = 8 * (uint32_t)(a & 3);
+  const uint32_t nw = (uint32_t)(((a & 3) + L + 3) >> 2);
+  uint32_t x0 = __ldg(w), x1 = 0, x2 = 0, x3 = 0, x4 = 0;
+  if (nw > 1) x1 = __ldg(w + 1);
+  if (nw > 2) x2 = __ldg(w + 2);
+  if (nw > 3) x3 = __ldg(w + 3);
+  if (nw > 4) x4 = __ldg(w + 4);
+  const uint32_t o[4] = {__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh),
+                         __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh)};
+  uint8_t* out = slot + d;
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-      const uint32_t word = i < 4 ? v.x : (i < 8 ? v.y : (i < 12 ? v.z : v.w));
-      const uint32_t off = o + i;
-      if (off < len) dst[off] = (uint8_t)(word >> (8 * (i & 3)));
+  for (uint32_t i = 0; i < 16; i++)
+    if (i < L) out[i] = (uint8_t)(o[i >> 2] >> (8 * (i & 3)));
+}
+
+// Byte i of the entry header varint(sh) varint(kd) varint(vl).
+__device__ __forceinline__ uint32_t header_byte(uint32_t sh, uint32_t kd, uint32_t vl, uint32_t i) {
+  uint32_t v = sh;
+  uint32_t n = varint_len(sh);
+  if (i >= n) {
+    i -= n;
+    v = kd;
+    n = varint_len(kd);
+    if (i >= n) {
+      i -= n;
+      v = vl;
+      n = varint_len(vl);
     }
   }
+  const uint32_t bits = (v >> (7 * i)) & 0x7f;
+  return i + 1 < n ? (bits | 0x80) : bits;
 }
 
 __global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t enc_smem[];
   uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
-  uint8_t* stages = enc_smem + 4096;
   crc_tables4_init(tab4);
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t sub = lane & 7, grp = lane >> 3;
+  EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem + 4096)[warp];
+  uint8_t* slot = W.slot + kEncSlot * lane;
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t R = J.restart_interval;
-  const uint8_t* in_limit = J.in_end;
-  const uint8_t* key_limit = J.keys + J.cap_key_bytes + 16;
-  uint8_t* stage = stages + warp * (kEncStage + kEncScratch);
-  uint8_t* scratch = stage + kEncStage;
+  const uint8_t* keys = J.keys;
+  const uint8_t* in = J.in;
   for (uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp; b < nb;
        b += (uint64_t)gridDim.x * kEncWarps) {
     const FileOut& F = J.files[J.b_file[b]];
     uint8_t* dst = J.out + F.out_off + J.b_off[b];
     const uint32_t bsz = J.b_size[b];
-    const uint32_t phase = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
-    if (bsz + kTrailer + phase > kEncStage) {
+    const uint64_t s = J.b_first[b];
+    const uint32_t n = (uint32_t)(J.b_first[b + 1] - s);
+    if (n > kEncMaxEnt) {
       enc_direct(J, tab4, b, dst, lane);
       continue;
     }
-    uint8_t* st = stage + phase;
-    const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
-    const uint64_t nrest = (n + R - 1) / R;
-    const uint32_t rbase = bsz - 4 * (uint32_t)nrest - 4;
+    // entry table
     uint32_t carry = 0;
-    for (uint64_t j0 = 0; j0 < n; j0 += 32) {
-      const uint64_t j = j0 + lane;
-      const bool valid = j < n;
-      const bool restart = (j % R) == 0;
-      uint32_t size = 0, ksrc = 0, klen = 0, vsrc = 0, vlen = 0, hl = 0, sh = 0;
-      if (valid) {
+    for (uint32_t j0 = 0; j0 < n; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      uint32_t size = 0;
+      if (j < n) {
         const uint64_t k = s + j;
         const uint32_t id = J.k_ids[k];
         const uint32_t kl = J.e_klen[id];
-        vlen = J.e_vlen[id];
-        vsrc = J.e_voff[id];
-        sh = restart ? 0 : J.k_shared[k];
-        ksrc = J.e_koff[id] + sh;
-        klen = kl - sh;
-        size = restart ? J.k_a[k] : J.k_b[k];
-        hl = varint_len(sh) + varint_len(klen) + varint_len(vlen);
+        const uint32_t sh = (j % R == 0) ? 0 : J.k_shared[k];
+        const uint32_t kd = kl - sh, vl = J.e_vlen[id];
+        size = varint_len(sh) + varint_len(kd) + varint_len(vl) + kd + vl;
+        W.ksrc[j] = J.e_koff[id] + sh;
+        W.vsrc[j] = J.e_voff[id];
+        // start the source lines on their way to L1 before the chunk pass
+        prefetch_l1(keys + J.e_koff[id] + sh, kd);
+        prefetch_l1(in + J.e_voff[id], vl);
+        W.kd[j] = kd;
+        W.vl[j] = vl;
+        W.sh[j] = sh;
       }
       uint32_t tot;
       const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
+      if (j < n) W.off[j] = ex;
       carry += tot;
-      if (valid) {
-        uint8_t* p = st + ex;
-        p = put_varint(p, sh);
-        p = put_varint(p, klen);
-        put_varint(p, vlen);
-        if (restart) {
-          const uint64_t rem = n - j;
-          const uint32_t cnt = (uint32_t)(rem < R ? rem : R);
-          st_le32(st + rbase + 4 * (uint32_t)(j / R), (ex << 8) | cnt);
+    }
+    if (lane == 0) W.off[n] = carry;
+    __syncwarp();
+    const uint32_t rbase = carry;  // restart array, then the restart count
+    const uint32_t nrest = (n + R - 1) / R;
+    // this lane's chunks of the global 16-byte grid
+    const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+    uint8_t* gbase = dst - ph;
+    const uint32_t nch = (ph + bsz + 15) >> 4;
+    const uint32_t per = (nch + 31) >> 5;
+    const uint32_t c0 = lane * per, c1 = min(nch, c0 + per);
+    const int32_t pb = (int32_t)(16 * c0) - (int32_t)ph;
+    const uint32_t seg_b = pb < 0 ? 0u : (uint32_t)pb;
+    const uint32_t seg_e = c0 < c1 ? min(bsz, 16 * c1 - ph) : seg_b;
+    // cursor: the entry holding seg_b
+    uint32_t j = 0;
+    if (seg_b < rbase) {
+      uint32_t lo = 0, hi = n;  // last j with off[j] <= seg_b
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (W.off[mid] <= seg_b) lo = mid;
+        else hi = mid;
+      }
+      j = lo;
+    }
+    uint32_t crc = 0;
+    for (uint32_t c = c0; c < c1; c++) {
+      const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
+      const uint32_t q0 = p0 < 0 ? 0u : (uint32_t)p0;
+      const uint32_t q1 = min(bsz, (uint32_t)(p0 + 16));
+      uint32_t p = q0;
+      while (p < q1) {
+        if (p < rbase) {
+          while (W.off[j + 1] <= p) j++;
+          const uint32_t e = p - W.off[j];
+          const uint32_t sh = W.sh[j], kd = W.kd[j], vl = W.vl[j];
+          const uint32_t hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
+          const uint32_t lim = min(q1, W.off[j + 1]);
+          if (e < hl) {
+            const uint32_t m = min(lim, p + (hl - e));
+            for (uint32_t i = 0; p < m; i++, p++) slot[p - p0] = (uint8_t)header_byte(sh, kd, vl, e + i);
+          } else if (e < hl + kd) {
+            const uint32_t m = min(lim, p + (hl + kd - e));
+            copy_piece(slot, p - p0, keys + W.ksrc[j] + (e - hl), m - p);
+            p = m;
+          } else {
+            copy_piece(slot, p - p0, in + W.vsrc[j] + (e - hl - kd), lim - p);
+            p = lim;
+          }
+        } else {
+          // restart words (offset << 8) | entries in the run, then their count
+          const uint32_t w = (p - rbase) >> 2, sb = 8 * ((p - rbase) & 3);
+          uint32_t val;
+          if (w < nrest) {
+            const uint32_t rem = n - w * R;
+            val = (W.off[w * R] << 8) | (rem < R ? rem : R);
+          } else {
+            val = nrest;
+          }
+          slot[p - p0] = (uint8_t)(val >> sb);
+          p++;
         }
       }
-      const uint32_t cnt_here = (uint32_t)((n - j0) < 32 ? (n - j0) : 32);
-      // 16-byte chunks that cover this entry's key delta and value
-      const uintptr_t ka = reinterpret_cast<uintptr_t>(J.keys + ksrc) & ~uintptr_t(15);
-      const uint32_t klead = (uint32_t)(reinterpret_cast<uintptr_t>(J.keys + ksrc) - ka);
-      const uint32_t nk = klen ? (klead + klen + 15) >> 4 : 0;
-      const uintptr_t va = reinterpret_cast<uintptr_t>(J.in + vsrc) & ~uintptr_t(15);
-      const uint32_t vlead = (uint32_t)(reinterpret_cast<uintptr_t>(J.in + vsrc) - va);
-      const uint32_t nv = vlen ? (vlead + vlen + 15) >> 4 : 0;
-      uint32_t gchunks;
-      const uint32_t sc = warp_excl<uint32_t>(nk + nv, &gchunks);
-      if (gchunks * 16 <= kEncScratch) {
-        // gather every chunk of the group with asynchronous copies, wait once
-        for (uint32_t e = 0; e < cnt_here; e++) {
-          const uint32_t e_nk = __shfl_sync(0xffffffffu, nk, e);
-          const uint32_t e_n = e_nk + __shfl_sync(0xffffffffu, nv, e);
-          const uint32_t e_sc = __shfl_sync(0xffffffffu, sc, e);
-          const uintptr_t e_ka = __shfl_sync(0xffffffffu, (unsigned long long)ka, e);
-          const uintptr_t e_va = __shfl_sync(0xffffffffu, (unsigned long long)va, e);
-          for (uint32_t c = lane; c < e_n; c += 32) {
-            const uint8_t* src = reinterpret_cast<const uint8_t*>(
-                c < e_nk ? e_ka + 16ull * c : e_va + 16ull * (c - e_nk));
-            uint8_t* d = scratch + 16 * (e_sc + c);
-            const uint8_t* lim = c < e_nk ? key_limit : in_limit;
-            if (src + 16 <= lim) {
-              cp_async16(d, src);
-            } else {
-              for (int i = 0; i < 16; i++) d[i] = src + i < lim ? src[i] : 0;
-            }
-          }
+      if (q0 == (uint32_t)p0 && q1 == (uint32_t)(p0 + 16)) {
+        uint32_t x[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          x[i] = *reinterpret_cast<const uint32_t*>(slot + 4 * i);
+          crc ^= x[i];
+          crc = tab4[768 + (crc & 0xff)] ^ tab4[512 + ((crc >> 8) & 0xff)] ^
+                tab4[256 + ((crc >> 16) & 0xff)] ^ tab4[crc >> 24];
         }
-        cp_async_wait_all();
-        __syncwarp();
-        // shift the gathered bytes into place in the stage
-        for (uint32_t e = 0; e < cnt_here; e++) {
-          const uint32_t e_ex = __shfl_sync(0xffffffffu, ex + hl, e);
-          const uint32_t e_kl = __shfl_sync(0xffffffffu, klen, e);
-          const uint32_t e_vl = __shfl_sync(0xffffffffu, vlen, e);
-          const uint32_t e_ks = __shfl_sync(0xffffffffu, 16 * sc + klead, e);
-          const uint32_t e_vs = __shfl_sync(0xffffffffu, 16 * (sc + nk) + vlead, e);
-          for (uint32_t t = lane; t < e_kl; t += 32) st[e_ex + t] = scratch[e_ks + t];
-          for (uint32_t t = lane; t < e_vl; t += 32) st[e_ex + e_kl + t] = scratch[e_vs + t];
-        }
-        __syncwarp();
+        *reinterpret_cast<uint4*>(gbase + 16 * c) = make_uint4(x[0], x[1], x[2], x[3]);
       } else {
-        // large values: four entries at a time, one per 8-lane group
-        for (uint32_t e0 = 0; e0 < cnt_here; e0 += 4) {
-          const uint32_t q = e0 + grp;
-          const uint32_t q_ex = __shfl_sync(0xffffffffu, ex, q & 31);
-          const uint32_t q_hl = __shfl_sync(0xffffffffu, hl, q & 31);
-          const uint32_t q_ks = __shfl_sync(0xffffffffu, ksrc, q & 31);
-          const uint32_t q_kl = __shfl_sync(0xffffffffu, klen, q & 31);
-          const uint32_t q_vs = __shfl_sync(0xffffffffu, vsrc, q & 31);
-          const uint32_t q_vl = __shfl_sync(0xffffffffu, vlen, q & 31);
-          if (q < cnt_here) {
-            uint8_t* d = st + q_ex + q_hl;
-            group_copy(J.keys + q_ks, q_kl, d, sub, key_limit);
-            group_copy(J.in + q_vs, q_vl, d + q_kl, sub, in_limit);
-          }
+        for (uint32_t q = q0; q < q1; q++) {
+          const uint8_t v = slot[q - p0];
+          crc = tab4[(crc ^ v) & 0xff] ^ (crc >> 8);
+          dst[q] = v;
         }
       }
     }
-    if (lane == 0) {
-      st_le32(st + bsz - 4, (uint32_t)nrest);
-      st[bsz] = 0;  // kNoCompression
+    // the zero type byte closes the CRC; lanes combine their registers
+    const uint32_t total = bsz + 1;
+    uint32_t e_end = seg_e;
+    if (seg_b < seg_e && seg_e == bsz) {
+      crc = tab4[crc & 0xff] ^ (crc >> 8);
+      e_end = total;
     }
-    __syncwarp();
-    const uint32_t crc = warp_block_crc_smem(J, tab4, st, bsz);
-    if (lane == 0) st_le32(st + bsz + 1, crc);
-    __syncwarp();
-    // write out [0, bsz + 5): bytes up to the first 16-byte boundary, 16-byte
-    // stores, then the tail
-    {
-      const uint32_t total = bsz + kTrailer;
-      const uint32_t head = (16 - phase) & 15;
-      const uint32_t h = head < total ? head : total;
-      if (lane < h) dst[lane] = st[lane];
-      const uint32_t body = (total - h) & ~15u;
-      const uint4* srcv = reinterpret_cast<const uint4*>(st + h);
-      uint4* dstv = reinterpret_cast<uint4*>(dst + h);
-      for (uint32_t c = lane; c < body / 16; c += 32) dstv[c] = srcv[c];
-      const uint32_t t0 = h + body;
-      if (t0 + lane < total) dst[t0 + lane] = st[t0 + lane];
+    uint32_t v = seg_b < e_end ? crc_shift(J, crc, total - e_end) : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+      const uint32_t full = v ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+      dst[bsz] = 0;  // kNoCompression
+      st_le32(dst + bsz + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
     }
     __syncwarp();
   }
@@ -941,18 +974,15 @@ void launch_block_layout(const Batch& bt, cudaStream_t st) {
 void launch_file_layout(const Batch& bt, cudaStream_t st) {
   note_launch(), k_file_layout<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
 }
-constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * (kEncStage + kEncScratch);
-
 void encode_kernel_attributes() {
   cudaFuncSetAttribute(k_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEncSmem);
 }
 
 void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
-  const size_t smem = kEncSmem;
-  // grid-stride over the device-side block count: 3 CTAs per SM x 8 waves,
+  // grid-stride over the device-side block count: 5 CTAs per SM x 4 waves,
   // shared out among the jobs
-  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 3 * 8)),
-                                        bt.B), kEncWarps * 32, smem, st>>>(bt.d);
+  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 5 * 4)),
+                                        bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);
 }
 void launch_encode_rest(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries * 32, 256, per_job(bt, 148 * 16)), bt.B),
