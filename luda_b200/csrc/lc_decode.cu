@@ -253,6 +253,7 @@ constexpr uint32_t kDecWarps = 4;
 constexpr uint32_t kDecStage = 8448;    // data block bytes + 16-byte phase
 constexpr uint32_t kDecMaxEnt = 512;    // entries of one staged block
 constexpr uint32_t kDecKeyBuf = 4096 + 32;
+constexpr uint32_t kDecLastKey = 256;   // longest key the staged path rebuilds
 struct DecWarpSmem {
   uint8_t stage[kDecStage];
   uint8_t keybuf[kDecKeyBuf];
@@ -260,6 +261,7 @@ struct DecWarpSmem {
   uint16_t sh[kDecMaxEnt];    // shared prefix
   uint16_t kl[kDecMaxEnt];    // key length
   uint16_t vl[kDecMaxEnt];    // value length
+  uint8_t lastkey[kDecLastKey];  // last key of the previous group of 32 entries
 };
 
 // Copies data block b into this warp's stage at the block's own 16-byte phase
@@ -416,11 +418,10 @@ __device__ void decode_direct(const JobDev& J, uint64_t b, uint32_t lane) {
 
 // Decode of one staged block.  Lanes first walk the restart runs (one lane
 // per run, headers only) and record every entry's key-delta position, shared
-// prefix and lengths; then, 32 entries at a time, each lane rebuilds one key
-// in shared memory: the delta from its own entry, and the shared prefix from
-// the deltas of earlier entries of the same run (walking back until the
-// prefix is covered -- a restart entry has no shared prefix).  Keys leave in
-// 16-byte stores; descriptors are written one lane per entry.
+// prefix and lengths; then, 32 entries at a time, the warp rebuilds the keys
+// in entry order in shared memory (lanes over bytes: the shared prefix is the
+// front of the previous key, already rebuilt), writes them out with 16-byte
+// stores, and writes the descriptors one lane per entry.
 __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const uint8_t* st,
                               DecWarpSmem& W) {
   BlockView v = block_view(J, b, st);
@@ -470,46 +471,38 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
     const uint32_t kofs = warp_excl<uint32_t>(kl, &gk);
     uint8_t* gdst = J.keys + kbase;
     const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
-    if (gk + kph + 16 > kDecKeyBuf) {
-      // keys of this group do not fit the buffer: write them directly
-      if (valid) {
-        uint8_t* d = gdst + kofs;
-        uint32_t m = W.sh[i];
-        for (uint32_t t = m; t < kl; t++) d[t] = st[W.dpos[i] + (t - m)];
-        for (int32_t j = (int32_t)i - 1; m > 0 && j >= 0; j--) {
-          const uint32_t lo = W.sh[j];
-          if (lo < m) {
-            for (uint32_t t = lo; t < m; t++) d[t] = st[W.dpos[j] + (t - lo)];
-            m = lo;
-          }
-        }
-      }
-    } else {
-      uint8_t* kb = W.keybuf + kph;
-      if (valid) {
-        uint8_t* d = kb + kofs;
-        uint32_t m = W.sh[i];
-        for (uint32_t t = m; t < kl; t++) d[t] = st[W.dpos[i] + (t - m)];
-        for (int32_t j = (int32_t)i - 1; m > 0 && j >= 0; j--) {
-          const uint32_t lo = W.sh[j];
-          if (lo < m) {
-            for (uint32_t t = lo; t < m; t++) d[t] = st[W.dpos[j] + (t - lo)];
-            m = lo;
-          }
-        }
-      }
+    // the rest of the block goes through the direct path (which rewrites
+    // the whole block) when a group's keys overflow the buffers
+    if (__any_sync(0xffffffffu, kl > kDecLastKey) || gk + kph + 16 > kDecKeyBuf) return false;
+    uint8_t* kb = W.keybuf + kph;
+    const uint32_t cnt = min(32u, nent - g0);
+    for (uint32_t e = 0; e < cnt; e++) {
+      const uint32_t ie = g0 + e;
+      const uint32_t esh = W.sh[ie], ekl = W.kl[ie], edp = W.dpos[ie];
+      const uint32_t eofs = __shfl_sync(0xffffffffu, kofs, e);
+      const uint32_t pofs = __shfl_sync(0xffffffffu, kofs, (e + 31) & 31);
+      const uint8_t* prev = e == 0 ? W.lastkey : kb + pofs;
+      uint8_t* d = kb + eofs;
+      for (uint32_t t = lane; t < ekl; t += 32) d[t] = t < esh ? prev[t] : st[edp + t - esh];
       __syncwarp();
-      // keys out: head bytes, 16-byte body, tail
-      const uint32_t head = (16 - kph) & 15;
-      const uint32_t h = head < gk ? head : gk;
-      if (lane < h) gdst[lane] = kb[lane];
-      const uint32_t body = (gk - h) & ~15u;
-      const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
-      uint4* dv = reinterpret_cast<uint4*>(gdst + h);
-      for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
-      const uint32_t t0 = h + body;
-      if (t0 + lane < gk) gdst[t0 + lane] = kb[t0 + lane];
     }
+    {
+      // the group's last key is the next group's first prefix
+      const uint32_t lofs = __shfl_sync(0xffffffffu, kofs, cnt - 1);
+      const uint32_t lkl = W.kl[g0 + cnt - 1];
+      for (uint32_t t = lane; t < lkl; t += 32) W.lastkey[t] = kb[lofs + t];
+    }
+    __syncwarp();
+    // keys out: head bytes, 16-byte body, tail
+    const uint32_t head = (16 - kph) & 15;
+    const uint32_t h = head < gk ? head : gk;
+    if (lane < h) gdst[lane] = kb[lane];
+    const uint32_t body = (gk - h) & ~15u;
+    const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
+    uint4* dv = reinterpret_cast<uint4*>(gdst + h);
+    for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
+    const uint32_t t0 = h + body;
+    if (t0 + lane < gk) gdst[t0 + lane] = kb[t0 + lane];
     if (valid) {
       const uint64_t e = ebase + i;
       const uint32_t ko = (uint32_t)(kbase + kofs);
@@ -517,8 +510,7 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
       J.e_klen[e] = kl;
       J.e_voff[e] = voff0 + W.dpos[i] + (kl - W.sh[i]);
       J.e_vlen[e] = W.vl[i];
-      const uint8_t* kp = (gk + kph + 16 > kDecKeyBuf) ? J.keys + ko : W.keybuf + kph + kofs;
-      J.e_pfx[e] = user_prefix(kp, kl);
+      J.e_pfx[e] = user_prefix(kb + kofs, kl);
     }
     kbase += gk;
     __syncwarp();
