@@ -358,6 +358,18 @@ class Engine:
         res._handle = _JobHandle(self.lib, jh, self)
         return res
 
+    def run_raw(self, p: "PreparedJob"):
+        """``lc_compact`` on a prepared descriptor, returning the raw job
+        handle (release with :meth:`release_raw`) and the ``lc_job_out``: the
+        bare C-ABI call, without building Python result objects."""
+        out = LcJobOut()
+        jh = C.c_void_p()
+        self._check(self.lib.lc_compact(self.h, C.byref(p.desc), C.byref(out), C.byref(jh)))
+        return jh, out
+
+    def release_raw(self, jh) -> None:
+        self.lib.lc_job_release(jh)
+
     def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
                 outputs_on_device: int = 0) -> CompactionResult:
         return self.run(self.prepare(job, device_tables, outputs_on_device))
