@@ -1,5 +1,6 @@
-// Exclusive prefix sums of per-job arrays (reduce, scan of tile sums, scan),
-// one launch per step for a whole batch (grid y = job).
+// Exclusive prefix sums of per-job arrays in two launches for a whole batch
+// (grid y = job): per-tile sums, then the scan of each tile from its offset,
+// which every CTA sums from the tile sums before it.
 //
 // The array and its length are chosen by a selector from the job descriptor;
 // the length lives in device memory, so a scan can be enqueued before the
@@ -157,23 +158,14 @@ __global__ void k_tile_reduce(const JobDev* __restrict__ jobs) {
   }
 }
 
-template <int S>
-__global__ void k_scan_tiles(const JobDev* __restrict__ jobs) {
-  using SP = ScanOf<S>;
-  using TO = typename SP::TO;
-  const JobDev& J = jobs[blockIdx.y];
-  const uint64_t n = SP::n(J);
-  const uint64_t n_tiles = n / kTile + 1;
-  TO* tile_sums = reinterpret_cast<TO*>(J.scan_scratch);
-  TO carry = 0;
-  for (uint64_t base = 0; base < n_tiles; base += blockDim.x) {
-    const uint64_t i = base + threadIdx.x;
-    TO v = i < n_tiles ? tile_sums[i] : TO(0);
-    TO total;
-    TO ex = block_excl_scan<TO>(v, &total);
-    if (i < n_tiles) tile_sums[i] = carry + ex;
-    carry += total;
-  }
+// Sum of a[lo, hi) over the CTA (every thread gets it).
+template <typename T>
+__device__ __forceinline__ T block_sum(const T* a, uint64_t lo, uint64_t hi) {
+  T v = 0;
+  for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) v += a[i];
+  T total;
+  block_excl_scan<T>(v, &total);
+  return total;
 }
 
 template <int S>
@@ -182,10 +174,14 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = SP::n(J);
-  const TO* tile_offsets = reinterpret_cast<const TO*>(J.scan_scratch);
+  const TO* tile_sums = reinterpret_cast<const TO*>(J.scan_scratch);
+  const uint64_t n_tiles = n / kTile + 1;
   const typename SP::TI* in = SP::in(J);
   TO* out = SP::out(J);
   uint64_t* total_out = SP::total(J);
+  // offset of this CTA's first tile: the sums of the tiles before it; each
+  // step of the grid stride adds the sums of the tiles it skips
+  TO carry = block_sum<TO>(tile_sums, 0, (uint64_t)blockIdx.x < n_tiles ? blockIdx.x : n_tiles);
   for (uint64_t t = blockIdx.x; t * kTile <= n; t += gridDim.x) {
     const uint64_t base = t * kTile;
     TO vals[kScanItems];
@@ -198,7 +194,7 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
       s += vals[k];
     }
     TO total;
-    TO ex = block_excl_scan<TO>(s, &total) + tile_offsets[t];
+    TO ex = block_excl_scan<TO>(s, &total) + carry;
 #pragma unroll
     for (int k = 0; k < kScanItems; k++) {
       const uint64_t i = tb + k;
@@ -210,15 +206,15 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
       }
       ex += vals[k];
     }
+    carry += block_sum<TO>(tile_sums, t, t + gridDim.x < n_tiles ? t + gridDim.x : n_tiles);
   }
 }
 
 template <int S>
 void scan_sel(const Batch& bt, uint64_t n_cap, cudaStream_t st) {
   const unsigned tiles = grid_x(n_cap + 1, kTile, 148 * 8);
-  note_launch(3);
+  note_launch(2);
   k_tile_reduce<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
-  k_scan_tiles<S><<<dim3(1, bt.B), 1024, 0, st>>>(bt.d);
   k_tile_scan<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
 }
 
