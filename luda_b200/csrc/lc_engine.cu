@@ -561,6 +561,22 @@ struct lc_slot {
   };
   std::map<std::string, GraphEntry> graphs;
   uint64_t tick = 0;
+  // Pinned host staging for the slot's small copies (descriptors, counters,
+  // per-file results), so that they are asynchronous DMA; it grows only at
+  // points where none of its copies is in flight.
+  uint8_t* pin = nullptr;
+  size_t pin_cap = 0;
+  uint8_t* pinned(size_t n) {
+    if (n > pin_cap) {
+      if (pin) cudaFreeHost(pin);
+      pin = nullptr;
+      pin_cap = 0;
+      const size_t c = std::max<size_t>(n, std::max<size_t>(1 << 20, 2 * pin_cap));
+      CK(cudaMallocHost(&pin, c));
+      pin_cap = c;
+    }
+    return pin;
+  }
   void init(int device, uint32_t capacity) {
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -573,6 +589,9 @@ struct lc_slot {
       for (auto& ev : g.second.events) cudaEventDestroy(ev.second);
     }
     graphs.clear();
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_cap = 0;
     if (d_jobs) cudaFree(d_jobs);
     if (st) cudaStreamDestroy(st);
     d_jobs = nullptr;
@@ -792,8 +811,13 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       o.bsl = S.put(sl.data(), nb);
       o.bll = S.put(ll.data(), nb);
     }
+    // pinned staging before the first sync: [stage | descriptors | counters]
+    const size_t o_hj = (S.h.size() + 255) & ~size_t(255);
+    const size_t o_hc = o_hj + ((sizeof(JobDev) * B + 255) & ~size_t(255));
+    uint8_t* pin1 = slot.pinned(o_hc + sizeof(Counters) * B);
+    memcpy(pin1, S.h.data(), S.h.size());
     uint8_t* d_stage = A.get<uint8_t>(S.h.size());
-    CK(cudaMemcpyAsync(d_stage, S.h.data(), S.h.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_stage, pin1, S.h.size(), cudaMemcpyHostToDevice, st));
     uint8_t* d_in_all = in_total ? A.get<uint8_t>(in_total) : nullptr;
     Counters* d_ctr = A.get<Counters>(B);
     CK(cudaMemsetAsync(d_ctr, 0, sizeof(Counters) * B, st));
@@ -853,9 +877,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       bt.max_tables = std::max(bt.max_tables, J.n_tables);
       bt.max_blocks_in = std::max(bt.max_blocks_in, cap_blk);
     }
-    std::vector<JobDev> hj(B);
+    JobDev* hj = reinterpret_cast<JobDev*>(pin1 + o_hj);
     for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
-    CK(cudaMemcpyAsync(slot.d_jobs, hj.data(), sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(slot.d_jobs, hj, sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
     T.mark(kUpload);
     // ---- parse: index blocks, block restart runs, entry and key totals
     if (bt.max_tables) {
@@ -870,8 +894,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
     CK(cudaGetLastError());
     T.mark(kParse);
     std::vector<Counters> hc(B);
-    CK(cudaMemcpyAsync(hc.data(), d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(pin1 + o_hc, d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    memcpy(hc.data(), pin1 + o_hc, sizeof(Counters) * B);
     // ---- allocate the rest from the totals
     bool any_zeroed = false;
     for (uint32_t i = 0; i < B; i++) {
@@ -897,9 +922,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       r.j->entries_in = r.N;
       r.j->key_bytes_in = r.K;
     }
-    if (any_zeroed) {
-      CK(cudaMemcpyAsync(d_ctr, hc.data(), sizeof(Counters) * B, cudaMemcpyHostToDevice, st));
-    }
+    // (the zeroed counters are uploaded below, from pinned memory)
     uint32_t max_runs = 1;
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
@@ -922,28 +945,62 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
     bt.max_cap_triggers = (uint32_t)pow2_at_least(bt.max_cap_triggers);
     bt.max_gp = bt.max_gp ? (uint32_t)pow2_at_least(bt.max_gp + 1) - 1 : 0;
     bt.merge_rounds = ceil_log2(max_runs);
-    for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
-    CK(cudaMemcpyAsync(slot.d_jobs, hj.data(), sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
+    // every job's per-file results in one device region, read back with one
+    // copy: [files | key offsets | keys] per job
+    std::vector<size_t> res_off(B + 1, 0);
+    for (uint32_t i = 0; i < B; i++) {
+      const JobDev& J = runs[i].J;
+      const size_t sz = ((sizeof(FileOut) * J.cap_files + 15) & ~size_t(15)) +
+                        ((8 * (2ull * J.cap_files + 1) + 15) & ~size_t(15)) +
+                        ((2ull * J.cap_files * runs[i].max_klen + 1 + 15) & ~size_t(15));
+      res_off[i + 1] = res_off[i] + sz;
+    }
+    uint8_t* d_res = A.get<uint8_t>(res_off[B]);
+    for (uint32_t i = 0; i < B; i++) {
+      JobDev& J = runs[i].J;
+      uint8_t* q = d_res + res_off[i];
+      J.files = reinterpret_cast<FileOut*>(q);
+      q += (sizeof(FileOut) * J.cap_files + 15) & ~size_t(15);
+      J.fkoff = reinterpret_cast<uint64_t*>(q);
+      q += (8 * (2ull * J.cap_files + 1) + 15) & ~size_t(15);
+      J.fkeys = q;
+    }
+    // pinned staging after the first sync: [counters | descriptors | results]
+    const size_t p_hj = (sizeof(Counters) * B + 255) & ~size_t(255);
+    const size_t p_res = p_hj + ((sizeof(JobDev) * B + 255) & ~size_t(255));
+    uint8_t* pin2 = slot.pinned(p_res + res_off[B]);
+    if (any_zeroed) {
+      memcpy(pin2, hc.data(), sizeof(Counters) * B);
+      CK(cudaMemcpyAsync(d_ctr, pin2, sizeof(Counters) * B, cudaMemcpyHostToDevice, st));
+    }
+    JobDev* hj2 = reinterpret_cast<JobDev*>(pin2 + p_hj);
+    for (uint32_t i = 0; i < B; i++) hj2[i] = runs[i].J;
+    CK(cudaMemcpyAsync(slot.d_jobs, hj2, sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
     T.start();
     // ---- decode, merge, drop, partition, encode: one graph launch
     const int how = slot.run_tail(bt, true, e->use_graphs, T);
     (how == 0 ? e->n_direct : how == 1 ? e->n_captures : e->n_replays)++;
     e->n_batches++;
     e->n_jobs += B;
-    // ---- per-job results
+    // ---- per-job results: two copies into pinned memory, one sync
+    CK(cudaMemcpyAsync(pin2 + p_res, d_res, res_off[B], cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(pin2, d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    memcpy(hc.data(), pin2, sizeof(Counters) * B);
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
+      const uint8_t* q = pin2 + p_res + res_off[i];
       r.files.resize(r.J.cap_files);
       r.koff.resize(2ull * r.J.cap_files + 1);
       r.j->key_bytes.resize(2ull * r.J.cap_files * r.max_klen + 1);
-      CK(cudaMemcpyAsync(r.files.data(), r.J.files, r.J.cap_files * sizeof(FileOut),
-                         cudaMemcpyDeviceToHost, st));
-      CK(cudaMemcpyAsync(r.koff.data(), r.J.fkoff, r.koff.size() * 8, cudaMemcpyDeviceToHost, st));
-      CK(cudaMemcpyAsync(r.j->key_bytes.data(), r.J.fkeys, r.j->key_bytes.size(),
-                         cudaMemcpyDeviceToHost, st));
+      const uint32_t nf = std::min<uint32_t>(hc[i].n_files, r.J.cap_files);
+      memcpy(r.files.data(), q, sizeof(FileOut) * nf);
+      q += (sizeof(FileOut) * r.J.cap_files + 15) & ~size_t(15);
+      memcpy(r.koff.data(), q, 8 * (2ull * nf + 1));
+      q += (8 * (2ull * r.J.cap_files + 1) + 15) & ~size_t(15);
+      const uint64_t kb = nf ? r.koff[2ull * nf] : 0;
+      memcpy(r.j->key_bytes.data(), q, std::min<uint64_t>(kb, r.j->key_bytes.size()));
     }
-    CK(cudaMemcpyAsync(hc.data(), d_ctr, sizeof(Counters) * B, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       if (r.failed) continue;
@@ -1005,8 +1062,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       if (!runs[i].failed) j->status = LC_OK;
       if (j->d_out) keep.push_back(j->d_out);
     }
-    A.release(keep);
-    CK(cudaStreamSynchronize(st));
+    A.release(keep);  // stream-ordered: later batches of this slot reuse the memory in order
   } catch (const CudaError& ce) {
     cudaStreamSynchronize(st);
     A.release({});
