@@ -346,24 +346,19 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_count(const JobDev* __
   }
 }
 
+// Entries of merge child r start at the first block of its first table: one
+// thread per table, the first table of each run writes the run's start.
 __global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
-  // one thread: entries of merge child r start at the first block of its
-  // first table
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  uint32_t next_run = 0;
   const bool bad = J.ctr->error != 0;  // the job fails; keep every read in bounds
-  for (uint32_t t = 0; t < J.n_tables; t++) {
-    while (next_run <= J.tables[t].run) {
-      J.run_entry_begin_w[next_run] =
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < J.n_tables;
+       t += gridDim.x * blockDim.x) {
+    const uint32_t run = J.tables[t].run;
+    if (t == 0 || J.tables[t - 1].run != run)
+      J.run_entry_begin_w[run] =
           bad ? 0 : J.blk_ent_base[min(J.tbl_block_base[t], J.cap_blocks_in)];
-      next_run++;
-    }
   }
-  while (next_run <= J.n_runs) {
-    J.run_entry_begin_w[next_run] = J.ctr->n_entries_in;
-    next_run++;
-  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) J.run_entry_begin_w[J.n_runs] = J.ctr->n_entries_in;
 }
 
 // Decode of one block straight from global memory, one lane per restart run:
@@ -583,7 +578,7 @@ void launch_block_count(const Batch& bt, cudaStream_t st) {
                                  kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
 }
 void launch_run_bounds(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_run_bounds<<<dim3(1, bt.B), 32, 0, st>>>(bt.d);
+  note_launch(), k_run_bounds<<<dim3((bt.max_tables + 127) / 128 + 1, bt.B), 128, 0, st>>>(bt.d);
 }
 void launch_block_decode(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,

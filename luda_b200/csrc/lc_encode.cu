@@ -68,13 +68,18 @@ __device__ __forceinline__ const uint8_t* kept_key(const JobDev& J, uint64_t k, 
   return J.keys + J.e_koff[id];
 }
 
+// Entry sizes as a restart entry (k_a) and as a prefix-compressed entry
+// (k_b), the shared prefix with the previous survivor, survivor byte totals;
+// also clears the block-start flags (n + 1 of them) for the chain.
 __global__ void k_sizes(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = J.ctr->n_kept;
   unsigned long long kb = 0, vb = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) J.k_bstart[n] = 0;
   for (uint64_t k0 = (uint64_t)blockIdx.x * blockDim.x; k0 < n; k0 += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = k0 + threadIdx.x;
     if (k >= n) continue;
+    J.k_bstart[k] = 0;
     uint32_t kl;
     const uint8_t* key = kept_key(J, k, &kl);
     const uint32_t vl = J.e_vlen[J.k_ids[k]];
@@ -101,14 +106,6 @@ __global__ void k_sizes(const JobDev* __restrict__ jobs) {
     atomicAdd((unsigned long long*)&J.ctr->kept_key_bytes, kb);
     atomicAdd((unsigned long long*)&J.ctr->kept_value_bytes, vb);
   }
-}
-
-__global__ void k_zero_bstart(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  const uint64_t n = J.ctr->n_kept;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    J.k_bstart[i] = 0;
 }
 
 __device__ __forceinline__ void next_one(const JobDev& J, uint64_t s, uint64_t n) {
@@ -228,37 +225,30 @@ __global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
   }
 }
 
+// Output blocks: first survivor of each block, and the block's size (the
+// block that starts at k ends where the chain says the next one starts).
 __global__ void k_block_list(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = J.ctr->n_kept;
+  const uint32_t R = J.restart_interval;
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= n;
        k += (uint64_t)gridDim.x * blockDim.x) {
-    if (k == n) J.b_first[J.k_block[n]] = (uint32_t)n;
-    else if (J.k_bstart[k]) J.b_first[J.k_block[k]] = (uint32_t)k;
+    if (k == n) {
+      J.b_first[J.k_block[n]] = (uint32_t)n;
+    } else if (J.k_bstart[k]) {
+      const uint32_t b = J.k_block[k];
+      J.b_first[b] = (uint32_t)k;
+      const uint64_t e = J.k_next[k];
+      uint64_t sum = 0;
+      for (uint64_t j = 0; j < e - k; j++) sum += (j % R == 0) ? J.k_a[k + j] : J.k_b[k + j];
+      const uint64_t nrest = (e - k + R - 1) / R;
+      const uint32_t size = (uint32_t)(sum + 4 * nrest + 4);
+      J.b_size[b] = size;
+      J.tmp32[b] = size + kTrailer;
+    }
   }
 }
 
-__device__ __forceinline__ void block_size_one(const JobDev& J, uint64_t b) {
-  uint32_t* tmp32 = J.tmp32;
-  const uint32_t R = J.restart_interval;
-  const uint64_t s = J.b_first[b], e = J.b_first[b + 1];
-  uint64_t sum = 0;
-  for (uint64_t j = 0; j < e - s; j++) sum += (j % R == 0) ? J.k_a[s + j] : J.k_b[s + j];
-  const uint64_t nrest = (e - s + R - 1) / R;
-  const uint32_t size = (uint32_t)(sum + 4 * nrest + 4);
-  J.b_size[b] = size;
-  tmp32[b] = size + kTrailer;
-}
-
-__global__ void k_block_sizes(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  const uint64_t nb = J.ctr->n_blocks_out;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
-       b += (uint64_t)gridDim.x * blockDim.x)
-    block_size_one(J, b);
-}
-
-// Output files: size cuts at block ends, grandparent cuts at forced blocks.
 // Like the block chain, a file's end depends on where it starts: every block
 // b gets b_fnext[b], the first block of the next file if a file began at b (a
 // binary search for the size cut, and the next forced block); one thread then
@@ -307,27 +297,51 @@ __global__ void k_file_next(const JobDev* __restrict__ jobs) {
   }
 }
 
+// The file starts are the orbit of block 0 under b_fnext, which only moves
+// forward: the CTA loads a tile of b_fnext at the walk's position into shared
+// memory and thread 0 walks inside it; a step that leaves the tile reloads.
+constexpr uint32_t kFileTile = 4096;
 __global__ void k_files(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ uint32_t tile[kFileTile];
+  __shared__ uint64_t s_b;
+  __shared__ uint32_t s_f;
+  __shared__ bool s_stop;
   const uint64_t nb = J.ctr->n_blocks_out;
-  uint32_t f = 0;
-  uint64_t b = 0;
-  while (b < nb) {
-    const uint64_t end = J.b_fnext[b];
-    if (f >= J.cap_files) {
-      set_error(J.ctr, kErrLimit, 2);
-      break;
-    }
-    FileOut& F = J.files[f];
-    F.first_block = (uint32_t)b;
-    F.end_block = (uint32_t)end;
-    F.first_kept = J.b_first[b];
-    F.end_kept = J.b_first[end];
-    f++;
-    b = end;
+  if (threadIdx.x == 0) {
+    s_b = 0;
+    s_f = 0;
+    s_stop = nb == 0;
   }
-  J.ctr->n_files = f;
+  __syncthreads();
+  while (!s_stop) {
+    const uint64_t t0 = s_b;
+    for (uint64_t i = threadIdx.x; i < kFileTile && t0 + i < nb; i += blockDim.x)
+      tile[i] = J.b_fnext[t0 + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint64_t b = t0;
+      uint32_t f = s_f;
+      while (b < nb && b < t0 + kFileTile) {
+        const uint64_t end = tile[b - t0];
+        if (f >= J.cap_files) {
+          set_error(J.ctr, kErrLimit, 2);
+          b = nb;
+          break;
+        }
+        FileOut& F = J.files[f];  // first_kept / end_kept: k_block_layout
+        F.first_block = (uint32_t)b;
+        F.end_block = (uint32_t)end;
+        f++;
+        b = end;
+      }
+      s_b = b;
+      s_f = f;
+      s_stop = b >= nb;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) J.ctr->n_files = s_f;
 }
 
 __device__ __forceinline__ uint32_t file_of_block(const JobDev& J, uint64_t b) {
@@ -353,6 +367,8 @@ __global__ void k_block_layout(const JobDev* __restrict__ jobs) {
 __device__ void block_layout_one(const JobDev& J, uint64_t b) {
   const uint32_t f = file_of_block(J, b);
   const uint32_t fb0 = J.files[f].first_block, fb1 = J.files[f].end_block;
+  if (b == fb0) J.files[f].first_kept = J.b_first[b];
+  if (b + 1 == fb1) J.files[f].end_kept = J.b_first[b + 1];
   const uint64_t base = J.b_cum[fb0];
   const uint64_t off = J.b_cum[b] - base;
   J.b_file[b] = f;
@@ -933,10 +949,6 @@ inline unsigned per_job(const Batch& bt, unsigned total) {
 
 }  // namespace
 
-void launch_zero_bstart(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_zero_bstart<<<dim3(grid_x(bt.max_entries + 1, 256, per_job(bt, 148 * 8)), bt.B),
-                                 256, 0, st>>>(bt.d);
-}
 void launch_sizes(const Batch& bt, cudaStream_t st) {
   note_launch(), k_sizes<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
                            st>>>(bt.d);
@@ -957,15 +969,11 @@ void launch_block_list(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_list<<<dim3(grid_x(bt.max_entries + 1, 256, per_job(bt, 148 * 8)), bt.B), 256,
                                 0, st>>>(bt.d);
 }
-void launch_block_sizes(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_block_sizes<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
-                                 0, st>>>(bt.d);
-}
 void launch_files(const Batch& bt, cudaStream_t st) {
   note_launch(), k_forced_blocks<<<dim3((bt.max_cap_triggers + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
   note_launch(), k_file_next<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
                                st>>>(bt.d);
-  note_launch(), k_files<<<dim3(1, bt.B), 32, 0, st>>>(bt.d);
+  note_launch(), k_files<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
 }
 void launch_block_layout(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_layout<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
@@ -984,11 +992,15 @@ void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 5 * 4)),
                                         bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);
 }
-void launch_encode_rest(const Batch& bt, cudaStream_t st) {
+void launch_encode_filters(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries * 32, 256, per_job(bt, 148 * 16)), bt.B),
                                     256, 0, st>>>(bt.d);
+}
+void launch_encode_index(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_index<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 16)), bt.B), 256,
                                   0, st>>>(bt.d);
+}
+void launch_encode_meta(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_meta<<<dim3(grid_x(bt.max_cap_files, 128, 1 << 20), bt.B), 128, 0, st>>>(bt.d);
   note_launch(), k_crc_regions<<<dim3(bt.max_cap_files * 3, bt.B), 256, 0, st>>>(bt.d);
 }

@@ -455,24 +455,24 @@ void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer
     launch_kept_compact(bt, st);
     T.mark(kDrop);
   }
-  launch_zero_bstart(bt, st);
   launch_sizes(bt, st);
   launch_next(bt, st);
   launch_chain(bt, st);
   scan_batch(kScanBstart, bt, bt.max_entries, st);
   launch_block_list(bt, st);
-  launch_block_sizes(bt, st);
   scan_batch(kScanBcum, bt, bt.max_entries, st);
   launch_files(bt, st);
   launch_block_layout(bt, st);
-  scan_batch(kScanGcum, bt, bt.max_entries, st);
   scan_batch(kScanIcum, bt, bt.max_entries, st);
+  scan_batch(kScanGcum, bt, bt.max_entries, st);
   launch_file_layout(bt, st);
   T.mark(kPartition);
   launch_encode_blocks(bt, st);
   T.mark(kEncodeBlocks);
-  launch_encode_rest(bt, st);
+  launch_encode_filters(bt, st);
+  launch_encode_index(bt, st);
   launch_file_keys(bt, st);
+  launch_encode_meta(bt, st);
   T.mark(kEncodeMeta);
 }
 
@@ -542,6 +542,7 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
   J.cap_scan = N + 1;
   J.scan_scratch = A.get<uint64_t>(scan_scratch_elems(N + 1));
+  J.scan_scratch2 = A.get<uint64_t>(scan_scratch_elems(N + 1));
 }
 
 }  // namespace

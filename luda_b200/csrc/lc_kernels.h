@@ -72,18 +72,20 @@ void launch_triggers(const Batch& bt, cudaStream_t st);
 void launch_kept_compact(const Batch& bt, cudaStream_t st);
 
 // lc_encode.cu -- survivors -> output tables
-void launch_zero_bstart(const Batch& bt, cudaStream_t st);
-void launch_sizes(const Batch& bt, cudaStream_t st);
+void launch_sizes(const Batch& bt, cudaStream_t st);       // also clears the block starts
 void launch_next(const Batch& bt, cudaStream_t st);
 void launch_chain(const Batch& bt, cudaStream_t st);
-void launch_block_list(const Batch& bt, cudaStream_t st);
-void launch_block_sizes(const Batch& bt, cudaStream_t st);
+void launch_block_list(const Batch& bt, cudaStream_t st);  // also the block sizes
 void launch_files(const Batch& bt, cudaStream_t st);
 void launch_block_layout(const Batch& bt, cudaStream_t st);
 void launch_file_layout(const Batch& bt, cudaStream_t st);
+// after the layout, blocks / filters / index + file keys are independent
 void launch_encode_blocks(const Batch& bt, cudaStream_t st);
-void launch_encode_rest(const Batch& bt, cudaStream_t st);
+void launch_encode_filters(const Batch& bt, cudaStream_t st);
+void launch_encode_index(const Batch& bt, cudaStream_t st);
 void launch_file_keys(const Batch& bt, cudaStream_t st);
+// metaindex, footer, filter tails and the trailers of filter/meta/index
+void launch_encode_meta(const Batch& bt, cudaStream_t st);
 
 // grid x for a kernel over up to `items` items per job, `per` items per CTA,
 // capped at `cap` CTAs (the kernel loops over the rest)

@@ -102,6 +102,13 @@ struct ScanOf<kScanIcum> {
   static __device__ uint64_t* total(const JobDev&) { return nullptr; }
 };
 
+// Tile-sum scratch of a scan: the index-size scan runs on a side stream
+// beside the filter-size scan, so it has its own.
+template <int S>
+__device__ __forceinline__ uint64_t* scan_tiles_of(const JobDev& J) {
+  return S == kScanIcum ? J.scan_scratch2 : J.scan_scratch;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
   const int lane = threadIdx.x & 31;
@@ -143,7 +150,7 @@ __global__ void k_tile_reduce(const JobDev* __restrict__ jobs) {
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = SP::n(J);
-  TO* tile_sums = reinterpret_cast<TO*>(J.scan_scratch);
+  TO* tile_sums = reinterpret_cast<TO*>(scan_tiles_of<S>(J));
   const typename SP::TI* in = SP::in(J);
   for (uint64_t t = blockIdx.x; t * kTile <= n; t += gridDim.x) {
     const uint64_t base = t * kTile;
@@ -174,7 +181,7 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
   const uint64_t n = SP::n(J);
-  const TO* tile_sums = reinterpret_cast<const TO*>(J.scan_scratch);
+  const TO* tile_sums = reinterpret_cast<const TO*>(scan_tiles_of<S>(J));
   const uint64_t n_tiles = n / kTile + 1;
   const typename SP::TI* in = SP::in(J);
   TO* out = SP::out(J);
