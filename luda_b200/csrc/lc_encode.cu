@@ -465,27 +465,30 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
   }
 }
 
-// One warp per output data block, which is produced as the 16-byte chunks of
-// the global 16-byte grid that cover it.  Lane l takes a contiguous run of
-// chunks: for each chunk it copies the bytes of the entries' headers, key
-// deltas and values (and of the restart array) that fall in the chunk into a
-// 16-byte slot in shared memory, feeds them to its CRC32C register and stores
-// the chunk with one 16-byte store (byte stores for the partial chunks at the
-// block's two ends).  The lanes' CRC registers are combined with shifts
-// x^(8n) mod P.  The per-warp entry table (output offset, key/value sources
-// and lengths) holds up to kEncMaxEnt entries; larger blocks take the direct
-// path.
+// One warp per output data block, in three passes over a per-warp entry table
+// (output offset, key/value sources and lengths; up to kEncMaxEnt entries,
+// larger blocks take the direct path):
+//  1. lanes walk the 4-byte words of the global grid that cover the block,
+//     32 consecutive words per step; a word that lies inside one entry's key
+//     delta or value is two read-only loads, a funnel shift and one aligned
+//     store -- the bulk of the bytes, with the same work in every lane;
+//  2. one lane per entry writes, with byte stores, what step 1 left: the
+//     header varints, the bytes of the key/value words cut by a segment edge,
+//     and the restart words;
+//  3. lanes read the finished block back (from L2) in contiguous 16-byte
+//     chunks, each computing a CRC32C register over its stretch; the
+//     registers are combined with shifts x^(8n) mod P into the trailer.
 constexpr uint32_t kEncWarps = 8;
 constexpr uint32_t kEncMaxEnt = 128;
-constexpr uint32_t kEncSlot = 20;  // bytes per lane slot: 5 words, distinct banks
+constexpr uint32_t kEncBatch = 8;  // words per lane with loads in flight together
 struct EncWarp {
   uint32_t off[kEncMaxEnt + 1];  // entry output offset in the block (+ end)
+  uint32_t kbeg[kEncMaxEnt];     // offset of the key delta (after the header)
   uint32_t ksrc[kEncMaxEnt];     // key delta: offset in the key arena
   uint32_t vsrc[kEncMaxEnt];     // value: offset in the input bytes
   uint32_t kd[kEncMaxEnt];       // key delta length
   uint32_t vl[kEncMaxEnt];       // value length
   uint32_t sh[kEncMaxEnt];       // shared prefix length
-  uint8_t slot[32 * kEncSlot];
 };
 constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * sizeof(EncWarp);
 
@@ -542,28 +545,6 @@ __device__ __forceinline__ void prefetch_l1(const uint8_t* p, uint32_t n) {
   for (uintptr_t q = a; q < e; q += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
 }
 
-// Copies L <= 16 bytes from global src to slot[d, d + L) (d + L <= 16): up to
-// five independent 4-byte loads of the aligned words covering src (the
-// arenas are padded, so the words past the end are readable), funnel shifts
-// that line the bytes up, predicated byte stores.
-__device__ __forceinline__ void copy_piece(uint8_t* slot, uint32_t d, const uint8_t* src, uint32_t L) {
-  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-  const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-  const uint32_t sh = 8 * (uint32_t)(a & 3);
-  const uint32_t nw = (uint32_t)(((a & 3) + L + 3) >> 2);
-  uint32_t x0 = __ldg(w), x1 = 0, x2 = 0, x3 = 0, x4 = 0;
-  if (nw > 1) x1 = __ldg(w + 1);
-  if (nw > 2) x2 = __ldg(w + 2);
-  if (nw > 3) x3 = __ldg(w + 3);
-  if (nw > 4) x4 = __ldg(w + 4);
-  const uint32_t o[4] = {__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh),
-                         __funnelshift_r(x2, x3, sh), __funnelshift_r(x3, x4, sh)};
-  uint8_t* out = slot + d;
-#pragma unroll
-  for (uint32_t i = 0; i < 16; i++)
-    if (i < L) out[i] = (uint8_t)(o[i >> 2] >> (8 * (i & 3)));
-}
-
 // Byte i of the entry header varint(sh) varint(kd) varint(vl).
 __device__ __forceinline__ uint32_t header_byte(uint32_t sh, uint32_t kd, uint32_t vl, uint32_t i) {
   uint32_t v = sh;
@@ -582,6 +563,21 @@ __device__ __forceinline__ uint32_t header_byte(uint32_t sh, uint32_t kd, uint32
   return i + 1 < n ? (bits | 0x80) : bits;
 }
 
+// Bytes [a, b) of the block at dst, from src, except the 4-byte words of the
+// global grid that lie wholly inside [a, b) (step 1 wrote those).
+__device__ __forceinline__ void enc_edges(uint8_t* dst, uint32_t ph4, uint32_t a, uint32_t b,
+                                          const uint8_t* src) {
+  if (a >= b) return;
+  const int32_t A = (int32_t)((a + ph4 + 3) & ~3u) - (int32_t)ph4;  // first whole word's start
+  const int32_t B = (int32_t)((b + ph4) & ~3u) - (int32_t)ph4;      // last whole word's end
+  if (A + 4 <= B) {
+    for (uint32_t p = a; p < (uint32_t)A; p++) dst[p] = __ldg(src + (p - a));
+    for (uint32_t p = (uint32_t)B; p < b; p++) dst[p] = __ldg(src + (p - a));
+  } else {
+    for (uint32_t p = a; p < b; p++) dst[p] = __ldg(src + (p - a));
+  }
+}
+
 __global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t enc_smem[];
@@ -590,7 +586,6 @@ __global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* 
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem + 4096)[warp];
-  uint8_t* slot = W.slot + kEncSlot * lane;
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t R = J.restart_interval;
@@ -611,120 +606,147 @@ __global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* 
     uint32_t carry = 0;
     for (uint32_t j0 = 0; j0 < n; j0 += 32) {
       const uint32_t j = j0 + lane;
-      uint32_t size = 0;
+      uint32_t size = 0, hl = 0;
       if (j < n) {
         const uint64_t k = s + j;
         const uint32_t id = J.k_ids[k];
         const uint32_t kl = J.e_klen[id];
         const uint32_t sh = (j % R == 0) ? 0 : J.k_shared[k];
         const uint32_t kd = kl - sh, vl = J.e_vlen[id];
-        size = varint_len(sh) + varint_len(kd) + varint_len(vl) + kd + vl;
+        hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
+        size = hl + kd + vl;
         W.ksrc[j] = J.e_koff[id] + sh;
         W.vsrc[j] = J.e_voff[id];
-        // start the source lines on their way to L1 before the chunk pass
-        prefetch_l1(keys + J.e_koff[id] + sh, kd);
-        prefetch_l1(in + J.e_voff[id], vl);
         W.kd[j] = kd;
         W.vl[j] = vl;
         W.sh[j] = sh;
+        // start the source lines on their way to L1
+        prefetch_l1(keys + J.e_koff[id] + sh, kd);
+        prefetch_l1(in + J.e_voff[id], vl);
       }
       uint32_t tot;
       const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
-      if (j < n) W.off[j] = ex;
+      if (j < n) {
+        W.off[j] = ex;
+        W.kbeg[j] = ex + hl;
+      }
       carry += tot;
     }
     if (lane == 0) W.off[n] = carry;
     __syncwarp();
     const uint32_t rbase = carry;  // restart array, then the restart count
     const uint32_t nrest = (n + R - 1) / R;
-    // this lane's chunks of the global 16-byte grid
+    const uint32_t ph4 = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 3);
+    // 1. whole words inside one key delta or value, kEncBatch words per lane
+    //    at a time: every source load of the batch is in flight before the
+    //    first is used
+    {
+      uint32_t* gw = reinterpret_cast<uint32_t*>(dst - ph4);
+      const uint32_t nwords = (ph4 + rbase + 3) >> 2;
+      uint32_t j = 0;
+      for (uint32_t w0 = lane; w0 < nwords; w0 += 32 * kEncBatch) {
+        const uint32_t* s4[kEncBatch];
+        uint32_t sh8[kEncBatch];
+        bool ok[kEncBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kEncBatch; u++) {
+          const uint32_t w = w0 + 32 * u;
+          const int32_t pi = (int32_t)(4 * w) - (int32_t)ph4;
+          ok[u] = false;
+          s4[u] = nullptr;
+          sh8[u] = 0;
+          if (w < nwords && pi >= 0 && (uint32_t)pi + 4 <= rbase) {
+            const uint32_t p = (uint32_t)pi;
+            while (W.off[j + 1] <= p) j++;
+            const uint32_t kb = W.kbeg[j], kd = W.kd[j];
+            const uint8_t* src = nullptr;
+            if (p >= kb && p + 4 <= kb + kd) src = keys + W.ksrc[j] + (p - kb);
+            else if (p >= kb + kd && p + 4 <= W.off[j + 1]) src = in + W.vsrc[j] + (p - kb - kd);
+            if (src) {
+              const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
+              s4[u] = reinterpret_cast<const uint32_t*>(sa & ~uintptr_t(3));
+              sh8[u] = 8 * (uint32_t)(sa & 3);
+              ok[u] = true;
+            }
+          }
+        }
+        uint32_t x0[kEncBatch], x1[kEncBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kEncBatch; u++) {
+          x0[u] = ok[u] ? __ldg(s4[u]) : 0u;
+          x1[u] = (ok[u] && sh8[u]) ? __ldg(s4[u] + 1) : 0u;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kEncBatch; u++)
+          if (ok[u]) gw[w0 + 32 * u] = __funnelshift_r(x0[u], x1[u], sh8[u]);
+      }
+    }
+    // 2. headers, segment edges, restart words
+    for (uint32_t j = lane; j < n; j += 32) {
+      const uint32_t o = W.off[j], kb = W.kbeg[j], kd = W.kd[j], vl = W.vl[j], sh = W.sh[j];
+      for (uint32_t p = o; p < kb; p++) dst[p] = (uint8_t)header_byte(sh, kd, vl, p - o);
+      enc_edges(dst, ph4, kb, kb + kd, keys + W.ksrc[j]);
+      enc_edges(dst, ph4, kb + kd, W.off[j + 1], in + W.vsrc[j]);
+      if (j % R == 0) {
+        const uint32_t rem = n - j;
+        st_le32(dst + rbase + 4 * (j / R), (o << 8) | (rem < R ? rem : R));
+      }
+    }
+    if (lane == 0) st_le32(dst + bsz - 4, nrest);
+    __syncwarp();
+    // 3. CRC32C over the block read back, lanes over contiguous 16-byte chunks
     const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
-    uint8_t* gbase = dst - ph;
+    const uint8_t* gbase = dst - ph;
     const uint32_t nch = (ph + bsz + 15) >> 4;
     const uint32_t per = (nch + 31) >> 5;
     const uint32_t c0 = lane * per, c1 = min(nch, c0 + per);
     const int32_t pb = (int32_t)(16 * c0) - (int32_t)ph;
     const uint32_t seg_b = pb < 0 ? 0u : (uint32_t)pb;
     const uint32_t seg_e = c0 < c1 ? min(bsz, 16 * c1 - ph) : seg_b;
-    // cursor: the entry holding seg_b
-    uint32_t j = 0;
-    if (seg_b < rbase) {
-      uint32_t lo = 0, hi = n;  // last j with off[j] <= seg_b
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (W.off[mid] <= seg_b) lo = mid;
-        else hi = mid;
-      }
-      j = lo;
-    }
+    // the two shift factors x^(8n) are fetched first, to arrive meanwhile
+    const uint32_t total = bsz + 1;
+    const bool last = seg_b < seg_e && seg_e == bsz;  // this lane appends the type byte
+    const uint32_t e_end = last ? total : seg_e;
+    const uint32_t f_lane = seg_b < e_end ? crc_xpow8(J, total - e_end) : 0u;
+    const uint32_t f_init = lane == 0 ? crc_xpow8(J, total) : 0u;
     uint32_t crc = 0;
-    for (uint32_t c = c0; c < c1; c++) {
-      const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
-      const uint32_t q0 = p0 < 0 ? 0u : (uint32_t)p0;
-      const uint32_t q1 = min(bsz, (uint32_t)(p0 + 16));
-      uint32_t p = q0;
-      while (p < q1) {
-        if (p < rbase) {
-          while (W.off[j + 1] <= p) j++;
-          const uint32_t e = p - W.off[j];
-          const uint32_t sh = W.sh[j], kd = W.kd[j], vl = W.vl[j];
-          const uint32_t hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
-          const uint32_t lim = min(q1, W.off[j + 1]);
-          if (e < hl) {
-            const uint32_t m = min(lim, p + (hl - e));
-            for (uint32_t i = 0; p < m; i++, p++) slot[p - p0] = (uint8_t)header_byte(sh, kd, vl, e + i);
-          } else if (e < hl + kd) {
-            const uint32_t m = min(lim, p + (hl + kd - e));
-            copy_piece(slot, p - p0, keys + W.ksrc[j] + (e - hl), m - p);
-            p = m;
-          } else {
-            copy_piece(slot, p - p0, in + W.vsrc[j] + (e - hl - kd), lim - p);
-            p = lim;
+    for (uint32_t cb = c0; cb < c1; cb += 4) {
+      uint4 v[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; u++) {
+        const uint32_t c = cb + u;
+        const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
+        v[u] = (c < c1 && p0 >= 0 && (uint32_t)p0 + 16 <= bsz)
+                   ? __ldcg(reinterpret_cast<const uint4*>(gbase + 16 * c))
+                   : make_uint4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; u++) {
+        const uint32_t c = cb + u;
+        if (c >= c1) break;
+        const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
+        if (p0 >= 0 && (uint32_t)p0 + 16 <= bsz) {
+          const uint32_t x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            crc ^= x[i];
+            crc = tab4[768 + (crc & 0xff)] ^ tab4[512 + ((crc >> 8) & 0xff)] ^
+                  tab4[256 + ((crc >> 16) & 0xff)] ^ tab4[crc >> 24];
           }
         } else {
-          // restart words (offset << 8) | entries in the run, then their count
-          const uint32_t w = (p - rbase) >> 2, sb = 8 * ((p - rbase) & 3);
-          uint32_t val;
-          if (w < nrest) {
-            const uint32_t rem = n - w * R;
-            val = (W.off[w * R] << 8) | (rem < R ? rem : R);
-          } else {
-            val = nrest;
-          }
-          slot[p - p0] = (uint8_t)(val >> sb);
-          p++;
-        }
-      }
-      if (q0 == (uint32_t)p0 && q1 == (uint32_t)(p0 + 16)) {
-        uint32_t x[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          x[i] = *reinterpret_cast<const uint32_t*>(slot + 4 * i);
-          crc ^= x[i];
-          crc = tab4[768 + (crc & 0xff)] ^ tab4[512 + ((crc >> 8) & 0xff)] ^
-                tab4[256 + ((crc >> 16) & 0xff)] ^ tab4[crc >> 24];
-        }
-        *reinterpret_cast<uint4*>(gbase + 16 * c) = make_uint4(x[0], x[1], x[2], x[3]);
-      } else {
-        for (uint32_t q = q0; q < q1; q++) {
-          const uint8_t v = slot[q - p0];
-          crc = tab4[(crc ^ v) & 0xff] ^ (crc >> 8);
-          dst[q] = v;
+          const uint32_t q0 = p0 < 0 ? 0u : (uint32_t)p0;
+          const uint32_t q1 = min(bsz, (uint32_t)(p0 + 16));
+          for (uint32_t q = q0; q < q1; q++) crc = tab4[(crc ^ __ldcg(dst + q)) & 0xff] ^ (crc >> 8);
         }
       }
     }
     // the zero type byte closes the CRC; lanes combine their registers
-    const uint32_t total = bsz + 1;
-    uint32_t e_end = seg_e;
-    if (seg_b < seg_e && seg_e == bsz) {
-      crc = tab4[crc & 0xff] ^ (crc >> 8);
-      e_end = total;
-    }
-    uint32_t v = seg_b < e_end ? crc_shift(J, crc, total - e_end) : 0;
+    if (last) crc = tab4[crc & 0xff] ^ (crc >> 8);
+    uint32_t v = seg_b < e_end ? gf2_mulmod(f_lane, crc) : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) {
-      const uint32_t full = v ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+      const uint32_t full = v ^ gf2_mulmod(f_init, 0xffffffffu) ^ 0xffffffffu;
       dst[bsz] = 0;  // kNoCompression
       st_le32(dst + bsz + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
     }
