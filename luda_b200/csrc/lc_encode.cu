@@ -754,8 +754,13 @@ __global__ void __launch_bounds__(kEncWarps * 32) k_encode_blocks(const JobDev* 
   }
 }
 
-// One warp per filter group (at the group's first block).
-__device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b, uint32_t lane) {
+// One warp per filter group (at the group's first block).  The bloom bits are
+// set with shared-memory atomics in the warp's buffer `sbuf` (kFilterSmem
+// bytes) and written out with coalesced byte stores; larger filters are built
+// in place with global atomics.
+constexpr uint32_t kFilterSmem = 1024;
+__device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b, uint32_t lane,
+                                                    uint32_t* sbuf) {
   const FileOut& F = J.files[J.b_file[b]];
   const uint32_t fb0 = F.first_block, fb1 = F.end_block;
   uint8_t* fbase = J.out + F.out_off + F.filter_off;
@@ -765,7 +770,12 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
     uint8_t* fdst = fbase + (J.b_gcum[b] - J.b_gcum[fb0]);
     const uint32_t nbytes = gb - 1;
     const uint64_t bits = (uint64_t)nbytes * 8;
-    for (uint32_t i = lane; i < nbytes; i += 32) fdst[i] = 0;
+    const bool in_smem = nbytes <= kFilterSmem;
+    if (in_smem) {
+      for (uint32_t i = lane; i < (nbytes + 3) / 4; i += 32) sbuf[i] = 0;
+    } else {
+      for (uint32_t i = lane; i < nbytes; i += 32) fdst[i] = 0;
+    }
     __syncwarp();
     const uint64_t k0 = J.b_first[b];
     const uint32_t nk = J.b_gkeys[b];
@@ -776,14 +786,24 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
       const uint32_t delta = (h >> 17) | (h << 15);
       for (uint32_t q = 0; q < J.bloom_k; q++) {
         const uint32_t bitpos = (uint32_t)(h % bits);
-        uint8_t* byte = fdst + (bitpos >> 3);
-        const uintptr_t a = reinterpret_cast<uintptr_t>(byte);
-        unsigned int* word = reinterpret_cast<unsigned int*>(a & ~uintptr_t(3));
-        atomicOr(word, 1u << ((a & 3) * 8 + (bitpos & 7)));
+        if (in_smem) {
+          // byte bitpos/8, bit bitpos%8 = bit (bitpos & 31) of little-endian word bitpos/32
+          atomicOr(&sbuf[bitpos >> 5], 1u << (bitpos & 31));
+        } else {
+          uint8_t* byte = fdst + (bitpos >> 3);
+          const uintptr_t a = reinterpret_cast<uintptr_t>(byte);
+          unsigned int* word = reinterpret_cast<unsigned int*>(a & ~uintptr_t(3));
+          atomicOr(word, 1u << ((a & 3) * 8 + (bitpos & 7)));
+        }
         h += delta;
       }
     }
     __syncwarp();
+    if (in_smem) {
+      const uint8_t* sb = reinterpret_cast<const uint8_t*>(sbuf);
+      for (uint32_t i = lane; i < nbytes; i += 32) fdst[i] = sb[i];
+      __syncwarp();
+    }
     if (lane == 0) fdst[nbytes] = (uint8_t)J.bloom_k;
     // filter offsets of the empty indices before this group and of the group
     const uint64_t jb = J.b_off[b] >> kFilterBaseLg;
@@ -796,12 +816,13 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
 
 __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_filter[8][kFilterSmem / 4];  // blockDim 256: 8 warps
   const uint32_t lane = threadIdx.x & 31;
   if (J.bits_per_key <= 0 || J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride)
-    encode_filter_group(J, b, lane);
+    encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
 }
 
 __device__ __forceinline__ void encode_index_entry(const JobDev& J, uint64_t b) {
