@@ -346,6 +346,35 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_count(const JobDev* __
   }
 }
 
+// Entries per data block from its restart array alone (the LUDA restart word
+// holds the entry count of its run): one thread per block.  The run byte
+// ranges are checked here; the entries themselves when they are decoded.
+__global__ void k_block_restarts(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // after a footer or index error some handles are unset
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblk;
+       b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint8_t* p = J.in + J.blk_off[b];
+    const uint32_t size = J.blk_size[b];
+    bool ok = size >= 4;
+    const uint32_t nr = ok ? ld_le32(p + size - 4) : 0;
+    if (ok && (uint64_t)nr * 4 + 4 > size) ok = false;
+    const uint64_t ra = ok ? size - 4 - 4ull * nr : 0;
+    uint64_t ent = 0, prev_end = 0;
+    for (uint32_t r = 0; ok && r < nr; r++) {
+      const uint32_t w = ld_le32(p + ra + 4ull * r);
+      const uint64_t s0 = w >> 8;
+      const uint64_t e0 = (r + 1 < nr) ? (ld_le32(p + ra + 4ull * (r + 1)) >> 8) : ra;
+      if (s0 > e0 || e0 > ra || s0 < prev_end) ok = false;
+      prev_end = e0;
+      ent += w & 0xff;
+    }
+    if (!ok) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
+    J.blk_nent[b] = ok ? (uint32_t)ent : 0;
+  }
+}
+
 // Entries of merge child r start at the first block of its first table: one
 // thread per table, the first table of each run writes the run's start.
 __global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
@@ -366,7 +395,44 @@ __global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
 __device__ void decode_direct(const JobDev& J, uint64_t b, uint32_t lane) {
   BlockView v = block_view(J, b, J.in + J.blk_off[b]);
   uint64_t ent_carry = J.blk_ent_base[b];
-  uint64_t key_carry = J.blk_key_base[b];
+  uint64_t key_carry;
+  if (J.reserve_keys) {
+    // single pass: check every run and sum the block's key bytes first, then
+    // reserve them in the key arena
+    uint64_t kb = 0;
+    uint32_t maxk = 0;
+    bool ok = v.ok, sk = false;
+    for (uint32_t r = lane; ok && r < v.nr; r += 32) {
+      uint64_t s, e, rk = 0;
+      uint32_t cnt;
+      run_bounds(v, r, &s, &e, &cnt);
+      if (s > e || e > v.ra || !walk_run(v.p + s, v.p + e, cnt, &rk, &maxk, &sk)) ok = false;
+      kb += rk;
+    }
+    const bool all_ok = __all_sync(0xffffffffu, ok);
+    const bool any_short = __any_sync(0xffffffffu, sk);
+    kb = warp_sum(kb);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+    uint64_t base = 0;
+    int fail = 0;
+    if (lane == 0) {
+      fail = 1;
+      if (!all_ok) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
+      else if (any_short) set_error(J.ctr, kErrShortKey, (uint32_t)b);
+      else if (maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+      else {
+        base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
+        if (base + kb > J.cap_key_bytes) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+        else fail = 0;
+      }
+      atomicMax(&J.ctr->max_klen, maxk);
+    }
+    if (__shfl_sync(0xffffffffu, fail, 0)) return;
+    key_carry = __shfl_sync(0xffffffffu, base, 0);
+  } else {
+    key_carry = J.blk_key_base[b];
+  }
   for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
     const uint32_t r = r0 + lane;
     uint64_t s = 0, e = 0, rk = 0;
@@ -422,9 +488,14 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
   BlockView v = block_view(J, b, st);
   const uint32_t nent = J.blk_nent[b];
   if (nent > kDecMaxEnt) return false;
-  // pass 1: headers of every entry, one lane per restart run
+  // pass 1: headers of every entry, one lane per restart run; the checks of
+  // the counting walk (bounds, no shared prefix at a restart, shared prefix
+  // within the previous key, runs parsed exactly to their end, keys of at
+  // least 8 bytes) are made here too
   uint32_t carry = 0;
-  bool long_key = false;
+  bool long_key = false, bad = !v.ok, short_key = false;
+  uint64_t rk = 0;
+  uint32_t maxk = 0;
   for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
     const uint32_t r = r0 + lane;
     uint64_t s = 0, e = 0;
@@ -434,29 +505,72 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
     const uint32_t e0 = warp_excl<uint32_t>(cnt, &tot) + carry;
     carry += tot;
     if (r < v.nr) {
+      if (s > e || e > v.ra) bad = true;
       const uint8_t* p = st + s;
-      const uint8_t* lim = st + e;
-      for (uint32_t k = 0; k < cnt; k++) {
+      const uint8_t* lim = st + (e > v.ra ? v.ra : e);
+      uint32_t prev = 0;
+      for (uint32_t k = 0; k < cnt && !bad; k++) {
         uint32_t sh, ns, vl;
         const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
-        if (!q) break;
+        if (!q || (k == 0 && sh != 0) || sh > prev) {
+          bad = true;
+          break;
+        }
+        const uint32_t kl = sh + ns;
         const uint32_t idx = e0 + k;
         if (idx < kDecMaxEnt) {
           W.dpos[idx] = (uint16_t)(q - st);
           W.sh[idx] = (uint16_t)sh;
-          W.kl[idx] = (uint16_t)(sh + ns);
+          W.kl[idx] = (uint16_t)kl;
           W.vl[idx] = (uint16_t)vl;
         }
-        if (sh + ns > 0xffff) long_key = true;
+        if (kl > 0xffff) long_key = true;
+        if (kl < 8) short_key = true;
+        rk += kl;
+        maxk = max(maxk, kl);
+        prev = kl;
         p = q + ns + vl;
       }
+      if (!bad && p != lim) bad = true;
+    }
+  }
+  if (J.reserve_keys) {
+    if (__any_sync(0xffffffffu, bad)) {
+      if (lane == 0) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
+      return true;
+    }
+    if (__any_sync(0xffffffffu, short_key)) {
+      if (lane == 0) set_error(J.ctr, kErrShortKey, (uint32_t)b);
+      return true;
     }
   }
   if (__any_sync(0xffffffffu, long_key)) return false;
   __syncwarp();
   // pass 2: keys and descriptors, 32 entries at a time
   const uint64_t ebase = J.blk_ent_base[b];
-  uint64_t kbase = J.blk_key_base[b];
+  uint64_t kbase;
+  if (J.reserve_keys) {
+    // reserve this block's key bytes in the arena
+    rk = warp_sum(rk);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+    uint64_t base = 0;
+    bool retry = false;
+    if (lane == 0) {
+      atomicMax(&J.ctr->max_klen, maxk);
+      if (maxk > J.max_key_len) {
+        retry = true;
+      } else {
+        base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)rk);
+        retry = base + rk > J.cap_key_bytes;
+      }
+      if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+    }
+    if (__shfl_sync(0xffffffffu, (int)retry, 0)) return true;
+    kbase = __shfl_sync(0xffffffffu, base, 0);
+  } else {
+    kbase = J.blk_key_base[b];
+  }
   const uint32_t voff0 = (uint32_t)J.blk_off[b];  // block offset in `in`
   for (uint32_t g0 = 0; g0 < nent; g0 += 32) {
     const uint32_t i = g0 + lane;
@@ -468,7 +582,15 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
     const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
     // the rest of the block goes through the direct path (which rewrites
     // the whole block) when a group's keys overflow the buffers
-    if (__any_sync(0xffffffffu, kl > kDecLastKey) || gk + kph + 16 > kDecKeyBuf) return false;
+    if (__any_sync(0xffffffffu, kl > kDecLastKey) || gk + kph + 16 > kDecKeyBuf) {
+      // a single-pass block has reserved its key bytes already: a retry of
+      // the whole job with counting keeps the layout simple
+      if (J.reserve_keys) {
+        if (lane == 0) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+        return true;
+      }
+      return false;
+    }
     uint8_t* kb = W.keybuf + kph;
     const uint32_t cnt = min(32u, nent - g0);
     for (uint32_t e = 0; e < cnt; e++) {
@@ -576,6 +698,10 @@ void decode_kernel_attributes() {
 void launch_block_count(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_count<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
                                  kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
+}
+void launch_block_restarts(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_block_restarts<<<dim3(grid_x(bt.max_blocks_in, 256, 148 * 8), bt.B), 256, 0, st>>>(
+      bt.d);
 }
 void launch_run_bounds(const Batch& bt, cudaStream_t st) {
   note_launch(), k_run_bounds<<<dim3((bt.max_tables + 127) / 128 + 1, bt.B), 128, 0, st>>>(bt.d);

@@ -73,6 +73,7 @@ __device__ __forceinline__ const uint8_t* kept_key(const JobDev& J, uint64_t k, 
 // also clears the block-start flags (n + 1 of them) for the chain.
 __global__ void k_sizes(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t n = J.ctr->n_kept;
   unsigned long long kb = 0, vb = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) J.k_bstart[n] = 0;
@@ -139,6 +140,7 @@ __device__ __forceinline__ void next_one(const JobDev& J, uint64_t s, uint64_t n
 
 __global__ void k_next(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t n = J.ctr->n_kept;
   for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
        s += (uint64_t)gridDim.x * blockDim.x)
@@ -150,6 +152,10 @@ __global__ void k_next(const JobDev* __restrict__ jobs) {
 // survivors of the chunk.
 __global__ void k_chain_tables(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   extern __shared__ uint32_t s_next[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
@@ -171,6 +177,10 @@ __global__ void k_chain_tables(const JobDev* __restrict__ jobs) {
 
 __global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   extern __shared__ uint32_t s_tab[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
@@ -205,6 +215,10 @@ __global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
 
 __global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   extern __shared__ uint32_t s_next[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
@@ -229,6 +243,7 @@ __global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
 // block that starts at k ends where the chain says the next one starts).
 __global__ void k_block_list(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t n = J.ctr->n_kept;
   const uint32_t R = J.restart_interval;
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= n;
@@ -257,6 +272,7 @@ __global__ void k_block_list(const JobDev* __restrict__ jobs) {
 // t_blocks[i] = output block that starts at grandparent cut i (ascending).
 __global__ void k_forced_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= J.ctr->n_triggers) return;
   const uint64_t kp = J.kept_pos[J.triggers[i]];
@@ -265,6 +281,7 @@ __global__ void k_forced_blocks(const JobDev* __restrict__ jobs) {
 
 __global__ void k_file_next(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t nt = J.ctr->n_triggers;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
@@ -303,6 +320,10 @@ __global__ void k_file_next(const JobDev* __restrict__ jobs) {
 constexpr uint32_t kFileTile = 4096;
 __global__ void k_files(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   __shared__ uint32_t tile[kFileTile];
   __shared__ uint64_t s_b;
   __shared__ uint32_t s_f;
@@ -358,6 +379,7 @@ __device__ void block_layout_one(const JobDev& J, uint64_t b);
 
 __global__ void k_block_layout(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t nb = J.ctr->n_blocks_out;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
        b += (uint64_t)gridDim.x * blockDim.x)
@@ -423,6 +445,10 @@ __device__ void block_layout_one(const JobDev& J, uint64_t b) {
 
 __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   const uint32_t nf = J.ctr->n_files;
   for (uint32_t f = threadIdx.x; f < nf; f += blockDim.x) {
     FileOut& F = J.files[f];

@@ -348,6 +348,7 @@ const char* err_name(uint32_t code) {
     case kErrBadEntry: return "bad entry";
     case kErrShortKey: return "internal key shorter than 8 bytes";
     case kErrArenaOverflow: return "key arena overflow";
+    case kErrRetryExact: return "single-pass key arena too small";
     case kErrLimit: return "engine limit exceeded";
     default: return "unknown";
   }
@@ -389,7 +390,7 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.crc_xpow = e->crc_xpow;
   J.crc_xpow_n = kCrcXpowN;
   J.chunk = kChunk;
-  J.chain_smem_words = 12 * 1024;  // 48 KiB
+  J.chain_smem_words = 11 * 1024;  // 44 KiB (static shared memory takes the rest of 48)
 }
 
 uint32_t ceil_log2(uint64_t x) {
@@ -532,10 +533,12 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   // Output capacity, bounded without waiting for the layout: every survivor
   // costs at most its key, its value and 15 header bytes; every block at most
   // 4 bytes of restart word per entry, 9 bytes of count and trailer, one index
-  // entry (key + 31) and a filter share; every file 256 bytes of metaindex,
-  // footer and trailers.  The layout kernel checks the real size against it.
+  // entry (its last key + 31; the blocks' last keys are distinct survivors, so
+  // all of them together are at most the key bytes) and a filter share; every
+  // file 256 bytes of metaindex, footer and trailers.  The layout kernel
+  // checks the real size against it.
   const uint64_t bpk = J.bits_per_key > 0 ? (uint64_t)J.bits_per_key : 0;
-  J.cap_out = J.in_size + 2 * J.cap_key_bytes + N * (80 + r.max_klen + (bpk + 7) / 8) +
+  J.cap_out = J.in_size + 3 * J.cap_key_bytes + N * (80 + (bpk + 7) / 8) +
               (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
   J.out = A.own(J.cap_out);
   J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
@@ -691,7 +694,13 @@ namespace {
 
 // Runs a batch of compaction jobs (kind 0) on one slot.  Per-job failures are
 // recorded in the job; CUDA failures fail the whole batch.
-void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
+// Key arena of the single-pass decode: twice the input bytes (typical keys
+// decode to well under the table bytes), and keys of at most kFastMaxKey
+// bytes; a job beyond either is rerun with exact counting.
+constexpr uint32_t kFastMaxKey = 256;
+
+void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
+               bool exact = false) {
   if (jobs.empty()) return;
   lc_engine* e = jobs[0]->eng;
   cudaStream_t st = slot.st;
@@ -882,14 +891,21 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
     for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
     CK(cudaMemcpyAsync(slot.d_jobs, hj, sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
     T.mark(kUpload);
-    // ---- parse: index blocks, block restart runs, entry and key totals
+    // ---- parse: index blocks, then entry counts -- exact: a walk of every
+    // entry header, which also gives the key bytes; single pass: the restart
+    // words alone, the decode reserving key space itself
     if (bt.max_tables) {
       launch_table_index_count(bt, st);
       scan_batch(kScanTblBlocks, bt, bt.max_tables, st);
       launch_table_index_entries(bt, st);
-      launch_block_count(bt, st);
-      scan_batch(kScanBlkEnt, bt, bt.max_blocks_in, st);
-      scan_batch(kScanBlkKey, bt, bt.max_blocks_in, st);
+      if (exact) {
+        launch_block_count(bt, st);
+        scan_batch(kScanBlkEnt, bt, bt.max_blocks_in, st);
+        scan_batch(kScanBlkKey, bt, bt.max_blocks_in, st);
+      } else {
+        launch_block_restarts(bt, st);
+        scan_batch(kScanBlkEnt, bt, bt.max_blocks_in, st);
+      }
     }
     launch_run_bounds(bt, st);
     CK(cudaGetLastError());
@@ -918,10 +934,17 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
         any_zeroed = true;
       }
       r.N = r.failed ? 0 : hc[i].n_entries_in;
-      r.K = r.failed ? 0 : hc[i].key_bytes_in;
-      r.max_klen = std::max<uint32_t>(hc[i].max_klen, 8);
+      if (exact) {
+        r.K = r.failed ? 0 : hc[i].key_bytes_in;
+        r.max_klen = std::max<uint32_t>(hc[i].max_klen, 8);
+      } else {
+        r.K = r.failed ? 0 : std::min<uint64_t>(2 * r.J.in_size + 65536, (1ull << 32) - 1);
+        r.max_klen = kFastMaxKey;
+      }
+      r.J.reserve_keys = exact ? 0 : 1;
+      r.J.max_key_len = kFastMaxKey;
       r.j->entries_in = r.N;
-      r.j->key_bytes_in = r.K;
+      r.j->key_bytes_in = exact ? r.K : 0;
     }
     // (the zeroed counters are uploaded below, from pinned memory)
     uint32_t max_runs = 1;
@@ -1002,9 +1025,16 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       const uint64_t kb = nf ? r.koff[2ull * nf] : 0;
       memcpy(r.j->key_bytes.data(), q, std::min<uint64_t>(kb, r.j->key_bytes.size()));
     }
+    std::vector<lc_job*> retry;  // single-pass jobs whose key arena was too small
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       if (r.failed) continue;
+      if (!exact && hc[i].error == kErrRetryExact) {
+        retry.push_back(r.j);
+        r.failed = true;
+        continue;
+      }
+      if (!exact) r.j->key_bytes_in = hc[i].key_cursor;
       std::string m;
       lc_status s = counters_status(hc[i], &m);
       if (s != LC_OK) {
@@ -1064,6 +1094,12 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun) {
       if (j->d_out) keep.push_back(j->d_out);
     }
     A.release(keep);  // stream-ordered: later batches of this slot reuse the memory in order
+    if (!retry.empty()) {
+      cudaEventDestroy(ev0);
+      cudaEventDestroy(ev1);
+      run_batch(retry, slot, tun, true);
+      return;
+    }
   } catch (const CudaError& ce) {
     cudaStreamSynchronize(st);
     A.release({});

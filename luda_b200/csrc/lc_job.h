@@ -29,6 +29,8 @@ enum : uint32_t {
   kErrShortKey = 5,       // internal key shorter than 8 bytes
   kErrArenaOverflow = 6,  // decoded keys exceed the arena capacity
   kErrLimit = 7,          // an engine limit was exceeded
+  kErrRetryExact = 8,     // the single-pass decode's bounded key arena (or key length
+                          // bound) was too small: the host reruns the job with counting
 };
 
 struct Counters {
@@ -48,6 +50,7 @@ struct Counters {
   uint32_t pad;
   uint64_t kept_key_bytes;    // internal-key bytes of the survivors
   uint64_t kept_value_bytes;  // value bytes of the survivors
+  uint64_t key_cursor;        // key bytes reserved by the single-pass decode
 };
 
 struct TableDesc {
@@ -154,6 +157,9 @@ struct JobDev {
   uint32_t* chunk_entry;     // per chunk: resolved entry point
   uint32_t window;           // table width
   uint32_t chain_smem_words; // shared-memory words for staging the chunk tables
+  uint32_t reserve_keys;     // 1: decode reserves key-arena space per block (single
+                             // pass, restart counts only); 0: blk_key_base from counting
+  uint32_t max_key_len;      // 1: longest key the single-pass layout allows
 
   // output blocks
   uint32_t* b_first;         // first kept entry of block (cap_blocks_out + 1)

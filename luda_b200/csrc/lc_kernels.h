@@ -32,7 +32,7 @@ struct Batch {
   uint64_t max_blocks_in = 0, max_entries = 0;
   uint32_t merge_rounds = 0;
   uint32_t chunk = 4096;
-  uint32_t chain_smem_words = 12 * 1024;
+  uint32_t chain_smem_words = 11 * 1024;
   // tunables (chosen by the autotuner in lc_engine.cu)
   uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
   uint32_t merge_items = 8;   // outputs per thread in a merge round
@@ -60,7 +60,8 @@ void launch_crc32c_chunks(const uint8_t* data, uint64_t n, uint32_t* partials, u
 // lc_decode.cu -- input tables -> decoded entries
 void launch_table_index_count(const Batch& bt, cudaStream_t st);
 void launch_table_index_entries(const Batch& bt, cudaStream_t st);
-void launch_block_count(const Batch& bt, cudaStream_t st);
+void launch_block_count(const Batch& bt, cudaStream_t st);     // exact key counts (full walk)
+void launch_block_restarts(const Batch& bt, cudaStream_t st);  // entry counts from restart words
 void launch_run_bounds(const Batch& bt, cudaStream_t st);
 void launch_block_decode(const Batch& bt, cudaStream_t st);
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st);

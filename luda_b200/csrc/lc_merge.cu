@@ -30,6 +30,7 @@ namespace {
 
 __global__ void k_iota(const JobDev* __restrict__ jobs, uint32_t rounds) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   uint32_t* ids = (rounds & 1) ? J.m_tmp : J.m_ids;  // the buffer round 0 reads
   const uint64_t n = J.ctr->n_entries_in;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -43,6 +44,7 @@ __global__ void k_iota(const JobDev* __restrict__ jobs, uint32_t rounds) {
 __global__ void k_merge_round(const JobDev* __restrict__ jobs, uint32_t r, uint32_t rounds,
                               uint32_t items) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint32_t* __restrict__ src = ((rounds - r) & 1) ? J.m_tmp : J.m_ids;
   uint32_t* __restrict__ dst = ((rounds - r) & 1) ? J.m_ids : J.m_tmp;
   const uint32_t width = 1u << r;
@@ -151,6 +153,7 @@ __device__ __forceinline__ void drop_one(const JobDev& J, const uint32_t* __rest
 
 __global__ void k_drop(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t n = J.ctr->n_entries_in;
   for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (uint64_t)gridDim.x * blockDim.x)
@@ -161,6 +164,7 @@ __global__ void k_drop(const JobDev* __restrict__ jobs) {
 // (gp_idx is non-decreasing along the merge order).
 __global__ void k_gp_first(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   uint32_t* gp_first = J.gp_first;
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g > J.n_gp) return;
@@ -181,6 +185,10 @@ __global__ void k_gp_first(const JobDev* __restrict__ jobs) {
 // over shared-memory copies of the prefix and first-position arrays.
 __global__ void k_triggers(const JobDev* __restrict__ jobs, bool in_smem) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   const uint32_t* gp_first = J.gp_first;
   extern __shared__ uint64_t s_tr[];
   const uint64_t n = J.ctr->n_entries_in;
@@ -226,6 +234,7 @@ __global__ void k_triggers(const JobDev* __restrict__ jobs, bool in_smem) {
 
 __global__ void k_kept_compact(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint32_t* __restrict__ ids = J.m_ids;
   const uint64_t n = J.ctr->n_entries_in;
   for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
@@ -240,6 +249,7 @@ __global__ void k_kept_compact(const JobDev* __restrict__ jobs) {
 
 __global__ void k_forced(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t nk = J.kept_pos[J.ctr->n_entries_in];
   if (i == 0 && nk > 0) J.k_forced[0] = 1;
@@ -274,7 +284,7 @@ void launch_triggers(const Batch& bt, cudaStream_t st) {
   if (bt.max_gp)
     note_launch(), k_gp_first<<<dim3((bt.max_gp + 1 + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
   const size_t smem = (size_t)(bt.max_gp + 1) * 12;
-  const bool in_smem = smem <= 48 * 1024;
+  const bool in_smem = smem + 64 <= 48 * 1024;  // with the kernel's static shared memory
   note_launch(), k_triggers<<<dim3(1, bt.B), 256, in_smem ? smem : 0, st>>>(bt.d, in_smem);
 }
 

@@ -149,6 +149,10 @@ __global__ void k_tile_reduce(const JobDev* __restrict__ jobs) {
   using SP = ScanOf<S>;
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   const uint64_t n = SP::n(J);
   TO* tile_sums = reinterpret_cast<TO*>(scan_tiles_of<S>(J));
   const typename SP::TI* in = SP::in(J);
@@ -180,6 +184,10 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
   using SP = ScanOf<S>;
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
   const uint64_t n = SP::n(J);
   const TO* tile_sums = reinterpret_cast<const TO*>(scan_tiles_of<S>(J));
   const uint64_t n_tiles = n / kTile + 1;
