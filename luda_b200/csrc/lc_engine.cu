@@ -694,9 +694,9 @@ namespace {
 
 // Runs a batch of compaction jobs (kind 0) on one slot.  Per-job failures are
 // recorded in the job; CUDA failures fail the whole batch.
-// Key arena of the single-pass decode: twice the input bytes (typical keys
-// decode to well under the table bytes), and keys of at most kFastMaxKey
-// bytes; a job beyond either is rerun with exact counting.
+// Key arena of the single-pass decode: the input bytes (typical keys decode
+// to well under the table bytes), and keys of at most kFastMaxKey bytes; a job
+// beyond either is rerun with exact counting.
 constexpr uint32_t kFastMaxKey = 256;
 
 void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
@@ -938,7 +938,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         r.K = r.failed ? 0 : hc[i].key_bytes_in;
         r.max_klen = std::max<uint32_t>(hc[i].max_klen, 8);
       } else {
-        r.K = r.failed ? 0 : std::min<uint64_t>(2 * r.J.in_size + 65536, (1ull << 32) - 1);
+        r.K = r.failed ? 0 : std::min<uint64_t>(r.J.in_size + 65536, (1ull << 32) - 1);
         r.max_klen = kFastMaxKey;
       }
       r.J.reserve_keys = exact ? 0 : 1;

@@ -175,3 +175,26 @@ def test_corrupt_input_reports_corruption(engine, kind):
     ok = workloads.plain_l0_l1(seed=8, scale=0.02)
     ok.materialize(lambda e, o: oracle.build_table(e, o, "oracle"))
     assert engine.compact(ok).file_bytes() == [x[0] for x in oracle.compact(ok)]
+
+
+def test_shared_prefix_keys_rerun_with_counting(engine):
+    """Keys that share 200 bytes with their predecessor decode to about ten
+    times the table bytes: the single-pass key arena (the input size) is too
+    small, the engine reruns the job with exact counting, and the output is
+    still the reference's."""
+    from luda_b200.job import CompactionJob, FileMeta, internal_key
+    prefix = b"p" * 200
+    opts = TableOptions(max_file_size=1 << 20)
+
+    def table(number, ids, seq0):
+        keys = [internal_key(prefix + b"%012d" % i, seq0 + k, 1) for k, i in enumerate(ids)]
+        e = Entries.from_lists(keys, [b""] * len(keys))
+        return FileMeta(number == 1 and 0 or 1, number, keys[0], keys[-1], 0, e, None)
+    files = [table(1, range(0, 20000, 2), 100000), table(2, range(0, 20000, 3), 1)]
+    files[0].level = 0
+    files[1].level = 1
+    job = CompactionJob(0, files, [], 200000, opts, name="shared_prefix")
+    job.materialize(lambda e, o: oracle.build_table(e, o, "oracle"))
+    assert sum(f.entries.n for f in files) * 212 > 2 * job.input_bytes()
+    res = engine.compact(job)
+    assert res.file_bytes() == [r[0] for r in oracle.compact(job, "oracle")]
