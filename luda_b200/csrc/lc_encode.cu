@@ -890,79 +890,83 @@ __global__ void k_encode_index(const JobDev* __restrict__ jobs) {
     encode_index_entry(J, b);
 }
 
+// Metaindex, footer and the tail of the filter block's offset array (thread
+// 0), then the trailers of the filter, metaindex and index blocks, each a
+// CRC32C over the whole CTA: one CTA per output file.
 __global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= J.ctr->n_files || J.ctr->error) return;
-  const FileOut& F = J.files[f];
-  uint8_t* base = J.out + F.out_off;
-  if (J.bits_per_key > 0) {
-    uint8_t* fb = base + F.filter_off;
-    const uint64_t Ft = J.b_gcum[F.end_block] - J.b_gcum[F.first_block];
-    const uint64_t jlast = J.b_off[F.end_block - 1] >> kFilterBaseLg;
-    for (uint64_t jj = jlast + 1; jj < F.n_filters; jj++) st_le32(fb + Ft + 4 * jj, (uint32_t)Ft);
-    st_le32(fb + Ft + 4ull * F.n_filters, (uint32_t)Ft);
-    fb[Ft + 4ull * F.n_filters + 4] = (uint8_t)kFilterBaseLg;
-    uint8_t* m = base + F.meta_off;
-    m[0] = 0;
-    m[1] = (uint8_t)kFilterNameLen;
-    m[2] = (uint8_t)(varint_len(F.filter_off) + varint_len(F.filter_size));
-    for (uint32_t i = 0; i < kFilterNameLen; i++) m[3 + i] = (uint8_t)kFilterName[i];
-    uint8_t* p = m + 3 + kFilterNameLen;
-    p = put_varint(p, F.filter_off);
-    p = put_varint(p, F.filter_size);
-    st_le32(p, 1u);  // restart word (0 << 8) | 1
-    st_le32(p + 4, 1u);
-  } else {
-    uint8_t* m = base + F.meta_off;
-    st_le32(m, 0u);
-    st_le32(m + 4, 1u);
-  }
-  uint8_t* foot = base + F.size - kFooter;
-  for (int i = 0; i < 40; i++) foot[i] = 0;
-  uint8_t* p = foot;
-  p = put_varint(p, F.meta_off);
-  p = put_varint(p, F.meta_size);
-  p = put_varint(p, F.index_off);
-  p = put_varint(p, F.index_size);
-  st_le32(foot + 40, 0x8b80fb57u);
-  st_le32(foot + 44, 0xdb477524u);
-}
-
-// Trailers of the filter, metaindex and index blocks: one CTA per block.
-__global__ void k_crc_regions(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t tab[256];
   __shared__ uint32_t s_x[32];
+  __shared__ uint32_t s_skip;
+  if (threadIdx.x == 0) s_skip = J.ctr->error || blockIdx.x >= J.ctr->n_files;
   crc_table_init(tab);
   __syncthreads();
-  const uint32_t f = blockIdx.x / 3, which = blockIdx.x % 3;
-  if (f >= J.ctr->n_files || J.ctr->error) return;
-  if (which == 0 && J.bits_per_key <= 0) return;
-  const FileOut& F = J.files[f];
-  const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
-  const uint64_t len = which == 0 ? F.filter_size : (which == 1 ? F.meta_size : F.index_size);
-  uint8_t* p = J.out + F.out_off + off;
-  const uint64_t total = len + 1;
-  const uint64_t seg = (total + blockDim.x - 1) / blockDim.x;
-  const uint64_t b = (uint64_t)threadIdx.x * seg;
-  const uint64_t e = min(total, b + seg);
-  uint32_t c = 0;
-  for (uint64_t i = b; i < e; i++) {
-    const uint8_t byte = i < len ? p[i] : 0;
-    c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
-  }
-  uint32_t v = b < total ? crc_shift(J, c, total - e) : 0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) s_x[threadIdx.x >> 5] = v;
-  __syncthreads();
+  if (s_skip) return;
+  const uint32_t f = blockIdx.x;
   if (threadIdx.x == 0) {
-    uint32_t x = 0;
-    for (uint32_t w = 0; w < blockDim.x / 32; w++) x ^= s_x[w];
-    const uint32_t full = x ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
-    p[len] = 0;
-    st_le32(p + len + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
+    const FileOut& F = J.files[f];
+    uint8_t* base = J.out + F.out_off;
+    if (J.bits_per_key > 0) {
+      uint8_t* fb = base + F.filter_off;
+      const uint64_t Ft = J.b_gcum[F.end_block] - J.b_gcum[F.first_block];
+      const uint64_t jlast = J.b_off[F.end_block - 1] >> kFilterBaseLg;
+      for (uint64_t jj = jlast + 1; jj < F.n_filters; jj++) st_le32(fb + Ft + 4 * jj, (uint32_t)Ft);
+      st_le32(fb + Ft + 4ull * F.n_filters, (uint32_t)Ft);
+      fb[Ft + 4ull * F.n_filters + 4] = (uint8_t)kFilterBaseLg;
+      uint8_t* m = base + F.meta_off;
+      m[0] = 0;
+      m[1] = (uint8_t)kFilterNameLen;
+      m[2] = (uint8_t)(varint_len(F.filter_off) + varint_len(F.filter_size));
+      for (uint32_t i = 0; i < kFilterNameLen; i++) m[3 + i] = (uint8_t)kFilterName[i];
+      uint8_t* p = m + 3 + kFilterNameLen;
+      p = put_varint(p, F.filter_off);
+      p = put_varint(p, F.filter_size);
+      st_le32(p, 1u);  // restart word (0 << 8) | 1
+      st_le32(p + 4, 1u);
+    } else {
+      uint8_t* m = base + F.meta_off;
+      st_le32(m, 0u);
+      st_le32(m + 4, 1u);
+    }
+    uint8_t* foot = base + F.size - kFooter;
+    for (int i = 0; i < 40; i++) foot[i] = 0;
+    uint8_t* p = foot;
+    p = put_varint(p, F.meta_off);
+    p = put_varint(p, F.meta_size);
+    p = put_varint(p, F.index_off);
+    p = put_varint(p, F.index_size);
+    st_le32(foot + 40, 0x8b80fb57u);
+    st_le32(foot + 44, 0xdb477524u);
+  }
+  __syncthreads();
+  const FileOut& F = J.files[f];
+  for (uint32_t which = 0; which < 3; which++) {
+    if (which == 0 && J.bits_per_key <= 0) continue;
+    const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
+    const uint64_t len = which == 0 ? F.filter_size : (which == 1 ? F.meta_size : F.index_size);
+    uint8_t* p = J.out + F.out_off + off;
+    const uint64_t total = len + 1;
+    const uint64_t seg = (total + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = (uint64_t)threadIdx.x * seg;
+    const uint64_t e = min(total, b + seg);
+    uint32_t c = 0;
+    for (uint64_t i = b; i < e; i++) {
+      const uint8_t byte = i < len ? p[i] : 0;
+      c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
+    }
+    uint32_t v = b < total ? crc_shift(J, c, total - e) : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s_x[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t x = 0;
+      for (uint32_t w = 0; w < blockDim.x / 32; w++) x ^= s_x[w];
+      const uint32_t full = x ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+      p[len] = 0;
+      st_le32(p + len + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
+    }
+    __syncthreads();
   }
 }
 
@@ -1070,8 +1074,7 @@ void launch_encode_index(const Batch& bt, cudaStream_t st) {
                                   0, st>>>(bt.d);
 }
 void launch_encode_meta(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_encode_meta<<<dim3(grid_x(bt.max_cap_files, 128, 1 << 20), bt.B), 128, 0, st>>>(bt.d);
-  note_launch(), k_crc_regions<<<dim3(bt.max_cap_files * 3, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 256, 0, st>>>(bt.d);
 }
 void launch_file_keys(const Batch& bt, cudaStream_t st) {
   note_launch(), k_file_keys<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
