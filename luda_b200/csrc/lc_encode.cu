@@ -487,7 +487,9 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
       o += J.files[f].size;
     }
     J.ctr->bytes_out = o;
-    if (o > J.cap_out) set_error(J.ctr, kErrLimit, 3);
+    // a single-pass job sized its output buffer from the input: rerun it
+    // with exact counting instead of failing
+    if (o > J.cap_out) set_error(J.ctr, J.reserve_keys ? kErrRetryExact : kErrLimit, 3);
   }
 }
 

@@ -538,8 +538,16 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   // file 256 bytes of metaindex, footer and trailers.  The layout kernel
   // checks the real size against it.
   const uint64_t bpk = J.bits_per_key > 0 ? (uint64_t)J.bits_per_key : 0;
-  J.cap_out = J.in_size + 3 * J.cap_key_bytes + N * (80 + (bpk + 7) / 8) +
-              (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
+  if (J.reserve_keys) {
+    // single pass (key bytes unknown): the survivors re-encoded take about
+    // the input's bytes; a job whose layout needs more is rerun with exact
+    // counting and the bound below
+    J.cap_out = J.in_size + J.in_size / 4 + N * (64 + (bpk + 7) / 8) +
+                (uint64_t)J.cap_files * 256 + 65536;
+  } else {
+    J.cap_out = J.in_size + 3 * J.cap_key_bytes + N * (80 + (bpk + 7) / 8) +
+                (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
+  }
   J.out = A.own(J.cap_out);
   J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
@@ -1471,9 +1479,15 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     CK(cudaSetDevice(e->device));
     if (pinned_reserve && !e->pinned.add_slab(pinned_reserve))
       throw CudaError{cudaErrorMemoryAllocation, "cudaMallocHost (pinned_reserve_bytes)"};
+    // the pool keeps freed memory for reuse across jobs (trimming it at every
+    // synchronisation costs milliseconds per job) up to three quarters of the
+    // device; beyond that it is returned at synchronisation points, so that
+    // allocations of many different sizes cannot grow it without bound
     cudaMemPool_t pool;
     CK(cudaDeviceGetDefaultMemPool(&pool, e->device));
-    uint64_t thr = ~0ull;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    uint64_t thr = std::max<uint64_t>(e->budget, total_b / 4 * 3);
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     CK(cudaStreamCreateWithFlags(&e->free_st, cudaStreamNonBlocking));
     decode_kernel_attributes();
