@@ -68,7 +68,7 @@ def parse_args():
 # DRAM bytes (read + write) per launch from one ncu capture of each kernel on
 # this workload at scale 1 (profiles/k_encode_blocks_l1_l2_at_size.md,
 # profiles/k_block_decode_l1_l2_at_size.md).
-NCU_TRAFFIC = {"encode_blocks": 89.274624e6 + 30.812160e6, "decode": 68.140032e6 + 3.020800e6}
+NCU_TRAFFIC = {"encode_blocks": 88.872704e6 + 32.018688e6, "decode": 68.024832e6 + 3.235840e6}
 
 
 def measured_peak():
