@@ -356,8 +356,10 @@ def served_leg(args, local, rank, torch):
             t.copy_(torch.frombuffer(bytearray(f.data), dtype=torch.uint8))
             f.data = t.numpy()
     up = TorchUploader(local)
-    engines = {"served": Engine(local, max_inflight=4, pinned_reserve=4 << 30),
-               "plain": Engine(local, max_inflight=1, max_batch=1, pinned_reserve=4 << 30)}
+    # phase timing: per-phase CUDA events of each batch, reported for the slowest jobs
+    engines = {"served": Engine(local, max_inflight=4, pinned_reserve=4 << 30, phase_timing=True),
+               "plain": Engine(local, max_inflight=1, max_batch=1, pinned_reserve=4 << 30,
+                               phase_timing=True)}
 
     def run(mode, rate):
         eng = engines[mode]

@@ -308,6 +308,7 @@ class JobRecord:
     device_ms: float = 0.0  # the engine's device time for the batch that ran the job
     batch_jobs: int = 1  # jobs in that batch
     queue_ms: float = 0.0  # time in the engine's queue before its batch started
+    phase_ms: Optional[dict] = None  # the batch's device time per phase, when the engine times phases
     file_bytes: Optional[List[bytes]] = None  # kept when record_bytes
     job: Optional[CompactionJob] = None  # the job with host copies of its inputs
 
@@ -329,6 +330,8 @@ class ServeStats:
     host_complete_s: float = 0.0  # loop time spent collecting results and installing them
     host_result_s: float = 0.0  # ... of which reading the result
     host_install_s: float = 0.0  # ... of which installing (and releasing consumed tables)
+    host_upload_s: float = 0.0  # loop time spent copying new level-0 tables to the device
+    longest_turn_ms: float = 0.0  # the longest pass of the loop between two waits
 
     @property
     def input_bytes(self) -> int:
@@ -353,12 +356,15 @@ class ServeStats:
             "write_stall_s": self.stall_s,
             "host_submit_s": self.host_submit_s, "host_complete_s": self.host_complete_s,
             "host_result_s": self.host_result_s, "host_install_s": self.host_install_s,
+            "host_upload_s": self.host_upload_s, "longest_turn_ms": self.longest_turn_ms,
             "queue_ms_mean": float(q.mean()), "queue_ms_p99": float(np.percentile(q, 99)),
             "device_ms_mean": float(np.mean([j.device_ms for j in self.jobs])) if self.jobs else 0,
             "batch_jobs_mean": float(np.mean([j.batch_jobs for j in self.jobs])) if self.jobs else 0,
             "slowest": [{"latency_ms": j.latency_ms, "queue_ms": j.queue_ms,
                          "device_ms": j.device_ms, "batch_jobs": j.batch_jobs, "level": j.level,
-                         "input_mib": j.input_bytes / float(1 << 20), "submit_s": j.submit_s}
+                         "input_mib": j.input_bytes / float(1 << 20), "submit_s": j.submit_s,
+                         "phase_ms": ({k: round(v, 3) for k, v in j.phase_ms.items()}
+                                      if j.phase_ms else None)}
                         for j in sorted(self.jobs, key=lambda j: -j.latency_ms)[:4]],
         }
 
@@ -408,7 +414,7 @@ class Server:
         return out
 
     # -- jobs --------------------------------------------------------------
-    def _submit(self, db: SimDB, now: float):
+    def _submit(self, db: SimDB, now: Callable[[], float]):
         c = db.pick()
         if c is None:
             return None
@@ -430,7 +436,7 @@ class Server:
             f.data = bytes(f.sim.host) if self.record_bytes else None
         h = self.engine.submit_prepared(p)
         db.busy = True
-        rec = JobRecord(db.index, level, sum(f.file_size for f in tables), 0, now, 0.0,
+        rec = JobRecord(db.index, level, sum(f.file_size for f in tables), 0, now(), 0.0,
                         len(tables), resident, job=job if self.record_bytes else None)
         return h, (db, level, in0, in1, rec, p)
 
@@ -440,12 +446,15 @@ class Server:
         inflight: List = []  # (AsyncJob, context)
         records: List[JobRecord] = []
         stall = 0.0
-        t_sub = t_done = t_res = t_inst = 0.0
+        t_sub = t_done = t_res = t_inst = t_up = 0.0
+        longest = 0.0
+        since = lambda: clock() - t0  # noqa: E731
         stalled_since = {}
         i = 0
         n = len(arrivals)
         while i < n or inflight or any(d.pending for d in self.dbs):
             now = clock() - t0
+            turn0 = now
             while i < n and arrivals[i].t <= now:
                 self.dbs[arrivals[i].db].pending.append(arrivals[i])
                 i += 1
@@ -454,12 +463,14 @@ class Server:
                     f = db.pending.popleft()
                     if db.index in stalled_since:
                         stall += now - stalled_since.pop(db.index)
+                    u0 = clock()
                     db.add_l0(self._l0_table(db, f), f.last_seq)
+                    t_up += clock() - u0
                 if db.pending and db.index not in stalled_since:
                     stalled_since[db.index] = now
                 if not db.busy:
                     c0 = clock()
-                    s = self._submit(db, now)
+                    s = self._submit(db, since)
                     t_sub += clock() - c0
                     if s is not None:
                         inflight.append(s)
@@ -468,6 +479,7 @@ class Server:
                     idle_wait(max(0.0, arrivals[i].t - (clock() - t0)))
                 continue
             timeout = max(0.0, arrivals[i].t - (clock() - t0)) if i < n else -1.0
+            longest = max(longest, clock() - t0 - turn0)
             k = self.engine.wait_any([h for h, _ in inflight], timeout)
             if k is None:
                 continue
@@ -479,6 +491,7 @@ class Server:
             rec.device_ms = getattr(res, "device_ms", 0.0)
             rec.batch_jobs = getattr(res, "batch_jobs", 1)
             rec.queue_ms = getattr(res, "queue_ms", 0.0)
+            rec.phase_ms = getattr(res, "phase_ms", None)
             if self.record_bytes:
                 rec.file_bytes = res.file_bytes()
             outs = self._outputs(db, level, res)
@@ -490,7 +503,7 @@ class Server:
             records.append(rec)
             t_done += clock() - c0
         return ServeStats(self.mode, clock() - t0, records, self.h2d, self.d2h, stall, n,
-                          t_sub, t_done, t_res, t_inst)
+                          t_sub, t_done, t_res, t_inst, t_up, longest * 1e3)
 
     def close(self):
         """Releases every table still held by the databases."""
