@@ -375,9 +375,14 @@ def served_leg(args, local, rank, torch):
         s1 = eng.stats()
         out = st.summary()
         out["offered_flushes_per_s"] = rate
-        out["engine"] = {k: s1[k] - s0[k] for k in ("batches", "graph_captures", "graph_replays",
-                                                    "direct_tails")}
-        out["engine"]["pinned_mib"] = s1["pinned_bytes"] / float(1 << 20)
+        out["engine"] = {k: s1[k] - s0[k] for k in (
+            "batches", "graph_captures", "graph_replays", "direct_tails", "block_takes",
+            "block_take_us", "staging_grows", "pinned_slab_grows", "scratch_slab_grows",
+            "device_out_slab_grows", "exact_reruns")}
+        # over the engine's life so far
+        out["engine"]["setup_us_max"] = s1["setup_us_max"]
+        for k in ("pinned", "scratch", "scratch_peak", "device_out", "device_out_peak"):
+            out["engine"][k + "_mib"] = s1[k + "_bytes"] / float(1 << 20)
         return out
 
     # warm-up: graphs, memory pools, pinned slabs, at every arrival pattern

@@ -197,6 +197,17 @@ typedef struct {
   uint64_t pinned_free_bytes;/* ... of which not in use */
   uint64_t inflight_bytes;   /* device-memory estimate of the admitted jobs */
   uint64_t queued_jobs;      /* submitted jobs not yet admitted */
+  /* host-side costs, for finding stalls */
+  uint64_t block_takes;      /* scratch chunks and kept outputs taken from the device slabs */
+  uint64_t block_take_us;    /* host time in those takes (slab growth included) */
+  uint64_t staging_grows;    /* per-slot pinned staging buffers re-allocated */
+  uint64_t pinned_slab_grows;/* pinned output slabs added after creation */
+  uint64_t setup_us_max;     /* longest host set-up of a batch before its first kernel */
+  uint64_t exact_reruns;     /* jobs rerun with exact counting (single pass overflowed) */
+  /* device memory: slabs taken from the driver, their free part, the most
+   * of them in use at once, slabs added */
+  uint64_t scratch_bytes, scratch_free_bytes, scratch_peak_bytes, scratch_slab_grows;
+  uint64_t device_out_bytes, device_out_free_bytes, device_out_peak_bytes, device_out_slab_grows;
 } lc_engine_stats;
 lc_status lc_engine_get_stats(lc_engine* e, lc_engine_stats* out);
 

@@ -64,18 +64,45 @@ struct StatusError {
 
 uint64_t round16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
 
-// Pinned host memory for job outputs.  cudaMallocHost costs milliseconds
-// (page locking), far more than a small job's device time, so pinned memory
-// is taken from the driver in slabs of at least 256 MiB and handed out by
-// first fit from a free list with neighbour coalescing; it returns to the
-// driver only when the engine is destroyed.
-struct PinnedCache {
-  static constexpr uint64_t kSlab = 256ull << 20;
+// A host<->device copy as copies of at most 2 MiB.  With one job's upload and
+// another's download in flight at once (the pipelined case), one large copy
+// in one direction took most of the PCIe bandwidth from many smaller ones in
+// the other (measured on B200: 68 MB down at 50 GB/s while 33 table uploads
+// got 31 GB/s); pieces of similar size in both directions share the link
+// evenly (40 + 40 GB/s) and a pipelined job finishes ~20% sooner.
+void copy_pieces(void* dst, const void* src, uint64_t n, cudaMemcpyKind kind, cudaStream_t st) {
+  constexpr uint64_t kPiece = 2ull << 20;
+  if (kind == cudaMemcpyDeviceToDevice) {
+    CK(cudaMemcpyAsync(dst, src, n, kind, st));
+    return;
+  }
+  for (uint64_t o = 0; o < n; o += kPiece)
+    CK(cudaMemcpyAsync((uint8_t*)dst + o, (const uint8_t*)src + o, std::min(kPiece, n - o), kind, st));
+}
+
+// Memory for job outputs and scratch, pinned host memory or device memory.  Taking
+// memory from the driver costs milliseconds (page locking; device mappings,
+// which also hold up the other threads' CUDA calls), far more than a small
+// job's device time, so it is taken in slabs of at least 256 MiB and handed
+// out by first fit from a free list with neighbour coalescing; it returns to
+// the driver only when the engine is destroyed.  A returned block is free for
+// the next job at once, on any stream: the engine returns scratch and outputs
+// only after the batch that used them has completed, and a caller returns an
+// output (lc_job_release) only after its own reads of it have completed.
+// (Scratch used to come from the stream-ordered pool: a batch bigger than any
+// before made the pool map fresh memory in the middle of the batch, ~0.4 s
+// for a few GB, holding up every other thread's CUDA calls meanwhile.)
+struct SlabCache {
   static constexpr uint64_t kAlign = 4096;
+  const bool device;      // device memory (cudaMalloc) rather than pinned host memory
+  const uint64_t kSlab;   // smallest slab taken from the driver
+  SlabCache(bool dev, uint64_t min_slab) : device(dev), kSlab(min_slab) {}
   std::mutex mu;
   std::vector<std::pair<uint8_t*, uint64_t>> slabs;
   std::map<uint8_t*, uint64_t> free_blocks;  // start -> size, address order
   uint64_t total = 0;                         // bytes in slabs
+  std::atomic<uint64_t> grows{0};             // slabs added by take()
+  uint64_t in_use = 0, peak = 0;              // bytes handed out: now, at most
   uint8_t* take(uint64_t n, uint64_t* cap) {
     const uint64_t want = (std::max<uint64_t>(n, 1) + kAlign - 1) & ~(kAlign - 1);
     while (true) {
@@ -89,19 +116,27 @@ struct PinnedCache {
           free_blocks.erase(it);
           if (rest) free_blocks.emplace(p + want, rest);
           *cap = want;
+          in_use += want;
+          peak = std::max(peak, in_use);
           return p;
         }
-        // grow geometrically, so that a growing working set pins few slabs
-        grow = std::max(std::max(kSlab, want), total / 2);
+        // host: grow geometrically, so that a growing working set pins few
+        // slabs; device: by a slab at a time, device memory being scarcer
+        grow = std::max(kSlab, want);
+        if (!device) grow = std::max(grow, total / 2);
       }
-      // pinning takes milliseconds: not under the lock, so that returns
-      // (give) and other takes proceed meanwhile
+      // taking memory from the driver takes milliseconds: not under the
+      // lock, so that returns (give) and other takes proceed meanwhile
       if (!add_slab(grow)) return nullptr;
+      grows++;
     }
   }
   bool add_slab(uint64_t sz) {
     void* p = nullptr;
-    if (cudaMallocHost(&p, sz) != cudaSuccess) return false;
+    if ((device ? cudaMalloc(&p, sz) : cudaMallocHost(&p, sz)) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
     std::lock_guard<std::mutex> g(mu);
     slabs.emplace_back((uint8_t*)p, sz);
     free_blocks.emplace((uint8_t*)p, sz);
@@ -111,6 +146,7 @@ struct PinnedCache {
   void give(uint8_t* p, uint64_t cap) {
     if (!p) return;
     std::lock_guard<std::mutex> g(mu);
+    in_use -= cap;
     auto it = free_blocks.emplace(p, cap).first;
     // merge with the following block, then with the preceding one, when they
     // touch within one slab (two slabs may be adjacent in the address space,
@@ -136,7 +172,7 @@ struct PinnedCache {
   }
   void clear() {
     std::lock_guard<std::mutex> g(mu);
-    for (auto& sl : slabs) cudaFreeHost(sl.first);
+    for (auto& sl : slabs) device ? cudaFree(sl.first) : cudaFreeHost(sl.first);
     slabs.clear();
     free_blocks.clear();
     total = 0;
@@ -159,7 +195,9 @@ struct lc_engine {
   int max_inflight = 4;
   uint32_t flags = 0;
   uint32_t* crc_xpow = nullptr;
-  PinnedCache pinned;
+  SlabCache pinned{false, 256ull << 20};  // outputs' host copies
+  SlabCache dev_out{true, 256ull << 20};  // outputs kept on the device
+  SlabCache scratch{true, 1ull << 30};    // the batches' working arrays
   std::mutex mu;
   std::condition_variable cv;
   std::condition_variable admit_cv;
@@ -169,7 +207,6 @@ struct lc_engine {
   std::vector<std::thread> workers;
   bool stop = false;
   uint64_t inflight_bytes = 0;
-  cudaStream_t free_st = nullptr;  // stream-ordered frees of released outputs
   uint32_t max_batch = 64;
   uint64_t max_batch_bytes = 512ull << 20;
   bool use_graphs = true;
@@ -182,6 +219,15 @@ struct lc_engine {
   std::vector<lc_slot*> free_slots;
   // counters for lc_engine_get_stats
   std::atomic<uint64_t> n_batches{0}, n_jobs{0}, n_captures{0}, n_replays{0}, n_direct{0};
+  std::atomic<uint64_t> n_block_takes{0}, block_take_ns{0}, n_staging_grows{0}, setup_ns_max{0};
+  std::atomic<uint64_t> n_exact_reruns{0};
+  void note_setup(std::chrono::steady_clock::time_point t0) {
+    const uint64_t ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                            std::chrono::steady_clock::now() - t0).count();
+    uint64_t cur = setup_ns_max.load();
+    while (ns > cur && !setup_ns_max.compare_exchange_weak(cur, ns)) {
+    }
+  }
   lc_slot* take_slot();
   void put_slot(lc_slot* s);
   Tunables tuning() {
@@ -215,6 +261,7 @@ struct lc_job {
   uint8_t* h_out = nullptr;
   uint64_t h_out_cap = 0;
   uint8_t* d_out = nullptr;  // kept when outputs_on_device is 1 or 2
+  uint64_t d_out_cap = 0;    // its block in the engine's device slabs
   std::vector<uint64_t> file_offset, file_size, file_entries, small_off, large_off;
   std::vector<uint32_t> small_len, large_len;
   std::vector<uint8_t> key_bytes;
@@ -235,45 +282,94 @@ struct lc_job {
 
 namespace {
 
-// Device allocations of one job: a bump allocator over a few large chunks of
-// the stream-ordered pool (one cudaMallocAsync per 64 MiB instead of one per
-// array), all freed in stream order at the end.  Sub-allocations are
-// 256-byte aligned and padded so that 16-byte vector loads may run past the
-// end of an array.
+// Device allocations of one batch: a bump allocator over chunks of the
+// engine's scratch slabs (64 MiB or one array, whichever is larger), all
+// returned when the batch has completed.  Sub-allocations are 256-byte
+// aligned and padded so that 16-byte vector loads may run past the end of an
+// array.  Outputs that outlive the batch (kept on the device) come from the
+// output slabs instead: their lifetimes are the caller's.
 struct DevAlloc {
   static constexpr uint64_t kChunkBytes = 64ull << 20;
   cudaStream_t st;
-  std::vector<void*> ptrs;
+  lc_engine* eng;
+  std::vector<std::pair<uint8_t*, uint64_t>> chunks;  // from eng->scratch
+  std::vector<std::pair<uint8_t*, uint64_t>> outs;    // from eng->dev_out
   uint8_t* cur = nullptr;
   uint64_t left = 0;
-  explicit DevAlloc(cudaStream_t s) : st(s) {}
+  uint64_t n_takes = 0, take_ns = 0;  // blocks taken and the host time it took
+  DevAlloc(cudaStream_t s, lc_engine* e) : st(s), eng(e) {}
+  ~DevAlloc() {
+    release({});
+    eng->n_block_takes += n_takes;
+    eng->block_take_ns += take_ns;
+  }
+  uint8_t* take(SlabCache& c, uint64_t n, uint64_t* cap, const char* what) {
+    const auto t0 = std::chrono::steady_clock::now();
+    uint8_t* p = c.take(n, cap);
+    if (!p) {
+      // the device's stream-ordered pool may hold the memory unused (it
+      // keeps freed memory up to its release threshold): give that back and
+      // retry once
+      cudaDeviceSynchronize();
+      cudaMemPool_t def = nullptr;
+      if (cudaDeviceGetDefaultMemPool(&def, eng->device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+      p = c.take(n, cap);
+      if (!p) throw CudaError{cudaErrorMemoryAllocation, what};
+    }
+    take_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                   std::chrono::steady_clock::now() - t0).count();
+    n_takes++;
+    return p;
+  }
   template <typename T>
   T* get(uint64_t n) {
     const uint64_t bytes = (std::max<uint64_t>(n, 1) * sizeof(T) + 16 + 255) & ~uint64_t(255);
     if (bytes > left) {
-      const uint64_t c = std::max(bytes, kChunkBytes);
-      void* p = nullptr;
-      CK(cudaMallocAsync(&p, c, st));
-      ptrs.push_back(p);
-      cur = (uint8_t*)p;
-      left = c;
+      uint64_t cap = 0;
+      cur = take(eng->scratch, std::max(bytes, kChunkBytes), &cap, "cudaMalloc (scratch slab)");
+      chunks.emplace_back(cur, cap);
+      left = cap;
     }
     T* r = (T*)cur;
     cur += bytes;
     left -= bytes;
     return r;
   }
-  // a separate allocation (e.g. an output that outlives the job)
-  uint8_t* own(uint64_t bytes) {
-    void* p = nullptr;
-    CK(cudaMallocAsync(&p, std::max<uint64_t>(bytes, 16) + 64, st));
-    ptrs.push_back(p);
-    return (uint8_t*)p;
+  // a job's output: from the output slabs when it outlives the batch
+  uint8_t* output(uint64_t bytes, bool outlives) {
+    if (!outlives) return get<uint8_t>(bytes + 64);
+    uint64_t cap = 0;
+    uint8_t* p = take(eng->dev_out, std::max<uint64_t>(bytes, 16) + 64, &cap,
+                      "cudaMalloc (device output slab)");
+    outs.emplace_back(p, cap);
+    return p;
   }
+  // once the batch has completed: returns the part of output p past its
+  // first `used` bytes to the slabs and gives the capacity it keeps
+  uint64_t trim(const void* p, uint64_t used) {
+    for (auto& o : outs) {
+      if (o.first != p) continue;
+      const uint64_t keep = (used + 64 + SlabCache::kAlign - 1) & ~(SlabCache::kAlign - 1);
+      if (keep < o.second) {
+        eng->dev_out.give(o.first + keep, o.second - keep);
+        o.second = keep;
+      }
+      return o.second;
+    }
+    return 0;
+  }
+  // returns the scratch and the outputs not in `keep`, after the stream's
+  // work (already complete on the normal path; an error path may still have
+  // kernels in flight)
   void release(const std::vector<void*>& keep) {
-    for (void* p : ptrs)
-      if (std::find(keep.begin(), keep.end(), p) == keep.end()) cudaFreeAsync(p, st);
-    ptrs.clear();
+    if (chunks.empty() && outs.empty()) return;
+    cudaStreamSynchronize(st);
+    for (auto& c : chunks) eng->scratch.give(c.first, c.second);
+    chunks.clear();
+    for (auto& o : outs)
+      if (std::find(keep.begin(), keep.end(), (void*)o.first) == keep.end())
+        eng->dev_out.give(o.first, o.second);
+    outs.clear();
     cur = nullptr;
     left = 0;
   }
@@ -409,6 +505,9 @@ struct JobRun {
   lc_job* j = nullptr;
   JobDev J;
   uint64_t cap_blk = 0, N = 0, K = 0;
+  // the input's bytes (tables rounded to 16), which bound the capacities; a
+  // job reading device tables in place may span more address range than this
+  uint64_t in_bytes = 0;
   uint32_t max_klen = 8;
   bool failed = false;
   Counters hc{};
@@ -517,7 +616,7 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   J.b_cum = A.get<uint64_t>(N + 1);
   J.cap_files = (uint32_t)std::min<uint64_t>(
       N + 1, 64 + J.cap_triggers +
-                 (8 * (J.in_size + J.cap_key_bytes) + N * 64) / std::max<uint64_t>(1, J.max_file_size));
+                 (8 * (r.in_bytes + J.cap_key_bytes) + N * 64) / std::max<uint64_t>(1, J.max_file_size));
   J.files = A.get<FileOut>(J.cap_files);
   J.b_fnext = A.get<uint32_t>(N);
   J.t_blocks = A.get<uint32_t>(J.cap_triggers);
@@ -542,13 +641,13 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
     // single pass (key bytes unknown): the survivors re-encoded take about
     // the input's bytes; a job whose layout needs more is rerun with exact
     // counting and the bound below
-    J.cap_out = J.in_size + J.in_size / 4 + N * (64 + (bpk + 7) / 8) +
+    J.cap_out = r.in_bytes + r.in_bytes / 4 + N * (64 + (bpk + 7) / 8) +
                 (uint64_t)J.cap_files * 256 + 65536;
   } else {
-    J.cap_out = J.in_size + 3 * J.cap_key_bytes + N * (80 + (bpk + 7) / 8) +
-                (uint64_t)J.cap_files * 256 + (J.in_size + J.cap_key_bytes) / 256 + 65536;
+    J.cap_out = r.in_bytes + 3 * J.cap_key_bytes + N * (80 + (bpk + 7) / 8) +
+                (uint64_t)J.cap_files * 256 + (r.in_bytes + J.cap_key_bytes) / 256 + 65536;
   }
-  J.out = A.own(J.cap_out);
+  J.out = A.output(J.cap_out, r.j->outputs_on_device == 1 || r.j->outputs_on_device == 2);
   J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
   J.cap_scan = N + 1;
@@ -575,17 +674,22 @@ struct lc_slot {
   uint64_t tick = 0;
   // Pinned host staging for the slot's small copies (descriptors, counters,
   // per-file results), so that they are asynchronous DMA; it grows only at
-  // points where none of its copies is in flight.
+  // points where none of its copies is in flight, at least doubling.  An
+  // outgrown buffer is kept until the slot is destroyed: cudaFreeHost waits
+  // for the whole device, which would stall every other slot's batch.
   uint8_t* pin = nullptr;
   size_t pin_cap = 0;
+  std::vector<uint8_t*> pin_retired;
+  std::atomic<uint64_t>* grow_count = nullptr;
   uint8_t* pinned(size_t n) {
     if (n > pin_cap) {
-      if (pin) cudaFreeHost(pin);
-      pin = nullptr;
-      pin_cap = 0;
-      const size_t c = std::max<size_t>(n, std::max<size_t>(1 << 20, 2 * pin_cap));
-      CK(cudaMallocHost(&pin, c));
+      const size_t c = std::max<size_t>(n, std::max<size_t>(4 << 20, 2 * pin_cap));
+      uint8_t* q = nullptr;
+      CK(cudaMallocHost(&q, c));
+      if (pin) pin_retired.push_back(pin);
+      pin = q;
       pin_cap = c;
+      if (grow_count) (*grow_count)++;
     }
     return pin;
   }
@@ -602,6 +706,8 @@ struct lc_slot {
     }
     graphs.clear();
     if (pin) cudaFreeHost(pin);
+    for (uint8_t* q : pin_retired) cudaFreeHost(q);
+    pin_retired.clear();
     pin = nullptr;
     pin_cap = 0;
     if (d_jobs) cudaFree(d_jobs);
@@ -684,6 +790,7 @@ lc_slot* lc_engine::take_slot() {
   }
   std::unique_ptr<lc_slot> n(new lc_slot());
   n->init(device, max_batch);
+  n->grow_count = &n_staging_grows;
   slots.push_back(std::move(n));
   return slots.back().get();
 }
@@ -711,8 +818,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
                bool exact = false) {
   if (jobs.empty()) return;
   lc_engine* e = jobs[0]->eng;
+  const auto t_setup0 = std::chrono::steady_clock::now();
   cudaStream_t st = slot.st;
-  DevAlloc A(st);
+  DevAlloc A(st, e);
   PhaseTimer T((e->flags & LC_FLAG_PHASE_TIMING) != 0, st);
   const uint32_t launches0 = launches_on_this_thread();
   const uint32_t B = (uint32_t)jobs.size();
@@ -788,6 +896,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         in_total += in_size + 16;
       }
       J.in_size = in_size;
+      r.in_bytes = 0;
+      if (!r.failed)
+        for (auto& t : td) r.in_bytes += round16(t.size);
       uint64_t cap_blk = 1;
       for (auto& t : td) cap_blk += t.size / 13 + 1;
       r.cap_blk = cap_blk;
@@ -857,9 +968,8 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         J.in = d_in_all + in_base[i];
         for (uint32_t t = 0; t < J.n_tables && !r.failed; t++) {
           if (!j->tables[t].size) continue;
-          CK(cudaMemcpyAsync((uint8_t*)J.in + tds[i][t].off, j->tables[t].data, j->tables[t].size,
-                             j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                             st));
+          copy_pieces((uint8_t*)J.in + tds[i][t].off, j->tables[t].data, j->tables[t].size,
+                      j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
         }
       }
       J.in_end = J.in + J.in_size + (zero_copy[i] ? 0 : 16);
@@ -899,6 +1009,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
     CK(cudaMemcpyAsync(slot.d_jobs, hj, sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
     T.mark(kUpload);
+    e->note_setup(t_setup0);
     // ---- parse: index blocks, then entry counts -- exact: a walk of every
     // entry header, which also gives the key bytes; single pass: the restart
     // words alone, the decode reserving key space itself
@@ -946,7 +1057,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         r.K = r.failed ? 0 : hc[i].key_bytes_in;
         r.max_klen = std::max<uint32_t>(hc[i].max_klen, 8);
       } else {
-        r.K = r.failed ? 0 : std::min<uint64_t>(r.J.in_size + 65536, (1ull << 32) - 1);
+        r.K = r.failed ? 0 : std::min<uint64_t>(r.in_bytes + 65536, (1ull << 32) - 1);
         r.max_klen = kFastMaxKey;
       }
       r.J.reserve_keys = exact ? 0 : 1;
@@ -1057,7 +1168,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
           job_fail(r, LC_ERR_NO_MEMORY, "pinned host buffer");
           continue;
         }
-        CK(cudaMemcpyAsync(j->h_out, r.J.out, nbytes, cudaMemcpyDeviceToHost, st));
+        copy_pieces(j->h_out, r.J.out, nbytes, cudaMemcpyDeviceToHost, st);
       }
       const uint32_t nf = hc[i].n_files;
       j->file_offset.resize(nf);
@@ -1086,6 +1197,10 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     T.mark(kDownload);
     CK(cudaEventRecord(ev1, st));
     CK(cudaStreamSynchronize(st));
+    // outputs kept on the device hold their bytes only (the capacity was a
+    // bound taken before the layout was known)
+    for (uint32_t i = 0; i < B; i++)
+      if (jobs[i]->d_out) jobs[i]->d_out_cap = A.trim(jobs[i]->d_out, jobs[i]->bytes_out);
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     std::vector<float> ph;
@@ -1105,6 +1220,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     if (!retry.empty()) {
       cudaEventDestroy(ev0);
       cudaEventDestroy(ev1);
+      e->n_exact_reruns += retry.size();
       run_batch(retry, slot, tun, true);
       return;
     }
@@ -1134,7 +1250,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
 void run_build(lc_job* j, lc_slot& slot) {
   lc_engine* e = j->eng;
   cudaStream_t st = slot.st;
-  DevAlloc A(st);
+  DevAlloc A(st, e);
   PhaseTimer T((e->flags & LC_FLAG_PHASE_TIMING) != 0, st);
   const uint32_t launches0 = launches_on_this_thread();
   try {
@@ -1168,12 +1284,13 @@ void run_build(lc_job* j, lc_slot& slot) {
     uint8_t* d_vals = A.get<uint8_t>(vb + 16);
     uint64_t* d_ko = A.get<uint64_t>(N + 1);
     uint64_t* d_vo = A.get<uint64_t>(N + 1);
-    if (kb) CK(cudaMemcpyAsync(J.keys, j->bkeys, kb, kind, st));
-    if (vb) CK(cudaMemcpyAsync(d_vals, j->bvals, vb, kind, st));
+    if (kb) copy_pieces(J.keys, j->bkeys, kb, kind, st);
+    if (vb) copy_pieces(d_vals, j->bvals, vb, kind, st);
     CK(cudaMemcpyAsync(d_ko, j->bkoffs, (N + 1) * 8, kind, st));
     CK(cudaMemcpyAsync(d_vo, j->bvoffs, (N + 1) * 8, kind, st));
     J.in = d_vals;
     J.in_size = vb;
+    r.in_bytes = vb;
     J.in_end = d_vals + vb + 16;
     J.src_koffs = d_ko;
     J.src_voffs = d_vo;
@@ -1225,7 +1342,7 @@ void run_build(lc_job* j, lc_slot& slot) {
     if (nbytes) {
       j->h_out = e->pinned.take(nbytes, &j->h_out_cap);
       if (!j->h_out) throw StatusError{LC_ERR_NO_MEMORY, "pinned host buffer"};
-      CK(cudaMemcpyAsync(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st));
+      copy_pieces(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st);
     }
     const uint32_t nf = hc.n_files;
     j->file_offset.resize(nf);
@@ -1489,7 +1606,6 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     CK(cudaMemGetInfo(&free_b, &total_b));
     uint64_t thr = std::max<uint64_t>(e->budget, total_b / 4 * 3);
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-    CK(cudaStreamCreateWithFlags(&e->free_st, cudaStreamNonBlocking));
     decode_kernel_attributes();
     encode_kernel_attributes();
     CK(cudaGetLastError());
@@ -1500,13 +1616,15 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     for (int i = 0; i < e->max_inflight; i++) {
       std::unique_ptr<lc_slot> sl(new lc_slot());
       sl->init(e->device, e->max_batch);
+      sl->grow_count = &e->n_staging_grows;
       wslots.push_back(sl.get());
       e->slots.push_back(std::move(sl));
     }
   } catch (const CudaError& ce) {
     std::string m = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
     if (e->crc_xpow) cudaFree(e->crc_xpow);
-    if (e->free_st) cudaStreamDestroy(e->free_st);
+    e->dev_out.clear();
+    e->scratch.clear();
     e->pinned.clear();
     delete e;
     return fail(LC_ERR_CUDA, m);
@@ -1526,11 +1644,9 @@ void lc_engine_destroy(lc_engine* e) {
   e->admit_cv.notify_all();
   for (auto& w : e->workers) w.join();
   cudaSetDevice(e->device);
-  if (e->free_st) {
-    cudaStreamSynchronize(e->free_st);
-    cudaStreamDestroy(e->free_st);
-  }
   e->pinned.clear();
+  e->dev_out.clear();
+  e->scratch.clear();
   cudaFree(e->crc_xpow);
   delete e;  // destroys the slots
 }
@@ -1619,13 +1735,8 @@ lc_status lc_job_result(lc_job* j, lc_job_out* out) {
 void lc_job_release(lc_job* j) {
   if (!j) return;
   if (j->h_out) j->eng->pinned.give(j->h_out, j->h_out_cap);
-  if (j->d_out) {
-    // the job has completed; return the output to the stream-ordered pool
-    // (on the engine's own non-blocking stream: the legacy default stream
-    // would order the free after every blocking stream of the process)
-    cudaSetDevice(j->eng->device);
-    cudaFreeAsync(j->d_out, j->eng->free_st);
-  }
+  // the job has completed and the caller has finished reading its output
+  if (j->d_out) j->eng->dev_out.give(j->d_out, j->d_out_cap);
   delete j;
 }
 
@@ -1694,6 +1805,23 @@ lc_status lc_engine_get_stats(lc_engine* e, lc_engine_stats* out) {
   out->graph_captures = e->n_captures;
   out->graph_replays = e->n_replays;
   out->direct_tails = e->n_direct;
+  out->block_takes = e->n_block_takes;
+  out->block_take_us = e->block_take_ns / 1000;
+  out->staging_grows = e->n_staging_grows;
+  out->pinned_slab_grows = e->pinned.grows;
+  out->setup_us_max = e->setup_ns_max / 1000;
+  out->exact_reruns = e->n_exact_reruns;
+  auto slabs = [](SlabCache& c, uint64_t* total, uint64_t* free_b, uint64_t* peak, uint64_t* grows) {
+    std::lock_guard<std::mutex> g(c.mu);
+    *total = c.total;
+    *peak = c.peak;
+    *grows = c.grows;
+    for (auto& b : c.free_blocks) *free_b += b.second;
+  };
+  slabs(e->scratch, &out->scratch_bytes, &out->scratch_free_bytes, &out->scratch_peak_bytes,
+        &out->scratch_slab_grows);
+  slabs(e->dev_out, &out->device_out_bytes, &out->device_out_free_bytes, &out->device_out_peak_bytes,
+        &out->device_out_slab_grows);
   {
     std::lock_guard<std::mutex> g(e->pinned.mu);
     out->pinned_bytes = e->pinned.total;

@@ -43,7 +43,10 @@ class LcConfig(C.Structure):
 class LcEngineStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "batches", "jobs", "graph_captures", "graph_replays", "direct_tails", "pinned_bytes",
-        "pinned_free_bytes", "inflight_bytes", "queued_jobs")]
+        "pinned_free_bytes", "inflight_bytes", "queued_jobs", "block_takes", "block_take_us",
+        "staging_grows", "pinned_slab_grows", "setup_us_max", "exact_reruns", "scratch_bytes",
+        "scratch_free_bytes", "scratch_peak_bytes", "scratch_slab_grows", "device_out_bytes",
+        "device_out_free_bytes", "device_out_peak_bytes", "device_out_slab_grows")]
 
 
 class LcTuning(C.Structure):
