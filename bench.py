@@ -504,7 +504,7 @@ def main():
     # (lc_job_submit / lc_job_wait), at most `depth` in flight, so that one
     # job's host<->device copies overlap another job's kernels.  Every job
     # copies its own inputs in and its own outputs out.
-    depth = 3
+    depth = 4
 
     def pipelined(n):
         inflight, done, submitted, d2h = [], 0, 0, 0

@@ -166,6 +166,10 @@ lc_status lc_job_result(lc_job* j, lc_job_out* out);
  * lc_job_wait / lc_job_result. */
 lc_status lc_job_wait_any(lc_engine* e, lc_job* const* jobs, int32_t n, int64_t timeout_ns,
                           int32_t* index);
+/* Frees the job and its output buffers.  Device outputs (outputs_on_device 1
+ * or 2) go back to the engine and may be handed to the next job at once, so
+ * call it only after every kernel or copy of the caller's own that reads
+ * them has completed. */
 void lc_job_release(lc_job* j);
 
 /* Synchronous compaction on the calling thread: the drop-in for one
@@ -177,7 +181,10 @@ lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_
  * every kernel launch covers all jobs of a batch (up to max_batch_jobs; more
  * are split into several batches), and the kernel sequence after the first
  * host synchronisation is one captured CUDA graph, replayed for later batches
- * of the same shape.  Each job's output is byte-identical to lc_compact on the
+ * of the same shape.  When more than 128 MiB of the inputs are in host
+ * memory, the jobs run as about eight batches (in order) on four streams at
+ * once, so that host<->device copies overlap kernels; the call returns when
+ * all have finished.  Each job's output is byte-identical to lc_compact on the
  * same descriptor.  On return every jobs[i] is a finished handle (release each
  * with lc_job_release): lc_job_wait returns its status at once and
  * lc_job_result its output.  Returns LC_OK when every job succeeded, else the

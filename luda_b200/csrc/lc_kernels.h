@@ -63,6 +63,10 @@ void launch_table_index_entries(const Batch& bt, cudaStream_t st);
 void launch_block_count(const Batch& bt, cudaStream_t st);     // exact key counts (full walk)
 void launch_block_restarts(const Batch& bt, cudaStream_t st);  // entry counts from restart words
 void launch_run_bounds(const Batch& bt, cudaStream_t st);
+// Copies n bytes with a kernel (no copy engine); one side may be mapped
+// pinned host memory given by its device alias.  False (nothing launched)
+// unless both addresses are 16-byte aligned.
+bool launch_xfer(void* dst, const void* src, uint64_t n, cudaStream_t st);
 void launch_block_decode(const Batch& bt, cudaStream_t st);
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st);
 

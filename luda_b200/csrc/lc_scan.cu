@@ -8,6 +8,7 @@
 // host-side capacity and tiles past the count exit early.  out has n+1
 // entries: out[n] is the total, optionally also stored to a counter.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdint.h>
 
 #include "lc_kernels.h"
@@ -250,5 +251,34 @@ void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st) {
 
 // tile sums for arrays of up to n_cap elements (TO up to 8 bytes)
 uint64_t scan_scratch_elems(uint64_t n_cap) { return (n_cap + 1) / kTile + 2; }
+
+namespace {
+
+// Small control transfers (descriptors, counters, per-file results) between
+// device memory and mapped pinned host memory, done by SM loads and stores
+// over PCIe rather than by a copy engine.  A copy engine serves the streams'
+// copies in turn, so with other jobs' bulk uploads and downloads in flight a
+// few-KB cudaMemcpyAsync waited behind megabytes of them and held up its
+// job's next kernels.  16-byte words, then the last bytes.
+__global__ void k_xfer(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint64_t n) {
+  const uint64_t n16 = n / 16;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  for (uint64_t i = t; i < n16; i += stride)
+    reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+  for (uint64_t i = n16 * 16 + t; i < n; i += stride) dst[i] = src[i];
+}
+
+}  // namespace
+
+bool launch_xfer(void* dst, const void* src, uint64_t n, cudaStream_t st) {
+  if (((uintptr_t)dst | (uintptr_t)src) & 15) return false;
+  if (!n) return true;
+  const uint64_t words = n / 16 + 1;
+  const unsigned grid = (unsigned)std::min<uint64_t>((words + 255) / 256, 148);
+  note_launch(1);
+  k_xfer<<<grid, 256, 0, st>>>((uint8_t*)dst, (const uint8_t*)src, n);
+  return true;
+}
 
 }  // namespace lc

@@ -147,3 +147,25 @@ def test_continuous_batching_same_alone_and_in_mix(mix_jobs, mix_want):
         hs = [e.submit(j) for j in mix_jobs * 2]
         got = [h.wait().file_bytes() for h in hs]
     assert got == mix_want * 2
+
+
+def test_large_host_batch_split_across_slots(engine):
+    """Host inputs beyond 128 MiB in one lc_compact_batch call run as several
+    parts on several streams at once; every job still gives the bytes it
+    gives alone."""
+    jobs = [workloads.batched_job(s) for s in range(40, 63)]
+    for j in jobs:
+        j.materialize(lambda e, o: engine.build_table(e, o))
+    assert sum(j.input_bytes() for j in jobs) > 200 << 20
+    ps = [engine.prepare(j) for j in jobs]
+    alone = []
+    for p in ps:
+        r = engine.run(p)
+        alone.append(r.file_bytes())
+        r.release()
+    before = engine.stats()["batches"]
+    res = engine.run_batch(ps)
+    assert engine.stats()["batches"] - before >= 3
+    assert [r.file_bytes() for r in res] == alone
+    for r in res:
+        r.release()
