@@ -108,6 +108,14 @@ typedef struct {
                                device pointer); 2: both -- host copy in data, device
                                copy in device_data, e.g. to feed a later job's
                                inputs_on_device without crossing PCIe again */
+  int32_t verify_checksums; /* 1: check every input data block's CRC32C trailer on the
+                               device before parsing it, and fail the job with
+                               LC_ERR_CORRUPT ("block checksum mismatch") if one is
+                               wrong -- ReadOptions::verify_checksums, which LevelDB
+                               sets for compaction inputs from Options::paranoid_checks
+                               (db/version_set.cc:1239; the check is table/format.cc:
+                               86-95, switched off in the reference build).  0: no
+                               check, as the reference. */
 } lc_job_desc;
 
 /* Output of one compaction: what DoCompactionWork records in

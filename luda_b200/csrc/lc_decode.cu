@@ -375,6 +375,32 @@ __global__ void k_block_restarts(const JobDev* __restrict__ jobs) {
   }
 }
 
+// Input block checksums, for jobs that ask for them: the check ReadBlock
+// makes when ReadOptions::verify_checksums is set (table/format.cc:86-95; the
+// reference build has it switched off with `&& 0`, and LevelDB sets it for a
+// compaction's inputs from Options::paranoid_checks, db/version_set.cc:1239):
+// the fixed32 after the type byte must be Mask(crc32c(contents + type)).  One
+// warp per data block; runs before the blocks are parsed, so that a damaged
+// block reports the checksum rather than whatever its bytes break.
+__global__ void __launch_bounds__(256) k_verify_blocks(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t tab[256];
+  __shared__ uint32_t s_skip;
+  if (threadIdx.x == 0) s_skip = (!J.verify_checksums || J.ctr->error) ? 1u : 0u;
+  crc_table_init(tab);
+  __syncthreads();
+  if (s_skip) return;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
+  for (uint64_t b = (uint64_t)blockIdx.x * nw + warp; b < nblk; b += (uint64_t)gridDim.x * nw) {
+    // the index parse checked that the block and its 5-byte trailer lie in the table
+    const uint8_t* p = J.in + J.blk_off[b];
+    const uint32_t size = J.blk_size[b];
+    const uint32_t crc = warp_block_crc(J, tab, p, size, p[size]);
+    if (lane == 0 && crc != ld_le32(p + size + 1)) set_error(J.ctr, kErrChecksum, (uint32_t)b);
+  }
+}
+
 // Entries of merge child r start at the first block of its first table: one
 // thread per table, the first table of each run writes the run's start.
 __global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
@@ -701,6 +727,11 @@ void launch_block_count(const Batch& bt, cudaStream_t st) {
 }
 void launch_block_restarts(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_restarts<<<dim3(grid_x(bt.max_blocks_in, 256, 148 * 8), bt.B), 256, 0, st>>>(
+      bt.d);
+}
+void launch_verify_blocks(const Batch& bt, cudaStream_t st) {
+  if (!bt.any_verify) return;
+  note_launch(), k_verify_blocks<<<dim3(grid_x(bt.max_blocks_in, 8, 148 * 8), bt.B), 256, 0, st>>>(
       bt.d);
 }
 void launch_run_bounds(const Batch& bt, cudaStream_t st) {

@@ -210,19 +210,21 @@ __device__ __forceinline__ uint32_t crc_shift(const JobDev& J, uint32_t c, uint6
   return gf2_mulmod(crc_xpow8(J, n), c);
 }
 
-// Masked CRC32C of contents followed by a zero type byte: the block trailer
-// of table/table_builder.cc:186-189, computed cooperatively by one warp over
-// `n` bytes at `p` (the type byte is appended implicitly).
+// Masked CRC32C of contents followed by the type byte: the block trailer of
+// table/table_builder.cc:186-189, computed cooperatively by one warp over `n`
+// bytes at `p` (the type byte, 0 for an uncompressed block, is appended
+// implicitly).
 __device__ __forceinline__ uint32_t warp_block_crc(const JobDev& J, const uint32_t* tab,
-                                                   const uint8_t* p, uint32_t n) {
+                                                   const uint8_t* p, uint32_t n,
+                                                   uint8_t type = 0) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t total = n + 1;  // contents + type byte 0
+  const uint32_t total = n + 1;  // contents + type byte
   uint32_t seg = (total + 31) / 32;
   uint32_t b = lane * seg;
   uint32_t e = min(total, b + seg);
   uint32_t c = 0;
   for (uint32_t i = b; i < e; i++) {
-    uint8_t byte = i < n ? p[i] : 0;
+    uint8_t byte = i < n ? p[i] : type;
     c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
   }
   // shift each lane's raw CRC by the bytes after its segment, xor together

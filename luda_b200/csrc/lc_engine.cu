@@ -251,6 +251,7 @@ struct lc_job {
   uint64_t smallest_snapshot = 0;
   lc_table_options opt{};
   int32_t inputs_on_device = 0, outputs_on_device = 0;
+  int32_t verify_checksums = 0;
   // build-table inputs
   int64_t bn = 0;
   const uint8_t *bkeys = nullptr, *bvals = nullptr;
@@ -446,6 +447,7 @@ const char* err_name(uint32_t code) {
     case kErrArenaOverflow: return "key arena overflow";
     case kErrRetryExact: return "single-pass key arena too small";
     case kErrLimit: return "engine limit exceeded";
+    case kErrChecksum: return "block checksum mismatch";
     default: return "unknown";
   }
 }
@@ -482,6 +484,7 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.bloom_k = j->opt.bits_per_key > 0 ? bloom_k(j->opt.bits_per_key) : 0;
   J.max_file_size = j->opt.max_file_size;
   J.smallest_snapshot = j->smallest_snapshot;
+  J.verify_checksums = j->verify_checksums ? 1u : 0u;
   J.max_gp_overlap = (int64_t)(10 * j->opt.max_file_size);  // db/version_set.cc:31-33
   J.crc_xpow = e->crc_xpow;
   J.crc_xpow_n = kCrcXpowN;
@@ -1021,6 +1024,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       J.run_entry_begin_w = A.get<uint64_t>(J.n_runs + 1);
       J.run_entry_begin = J.run_entry_begin_w;
       bt.max_tables = std::max(bt.max_tables, J.n_tables);
+      bt.any_verify = bt.any_verify || (J.verify_checksums && !r.failed);
       bt.max_blocks_in = std::max(bt.max_blocks_in, cap_blk);
     }
     JobDev* hj = reinterpret_cast<JobDev*>(pin1 + o_hj);
@@ -1035,6 +1039,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       launch_table_index_count(bt, st);
       scan_batch(kScanTblBlocks, bt, bt.max_tables, st);
       launch_table_index_entries(bt, st);
+      launch_verify_blocks(bt, st);
       if (exact) {
         launch_block_count(bt, st);
         scan_batch(kScanBlkEnt, bt, bt.max_blocks_in, st);
@@ -1530,6 +1535,7 @@ lc_status copy_desc(lc_job* j, const lc_job_desc* d) {
   if (d->outputs_on_device < 0 || d->outputs_on_device > 2)
     return fail(LC_ERR_INVALID_ARG, "outputs_on_device must be 0, 1 or 2");
   j->outputs_on_device = d->outputs_on_device;
+  j->verify_checksums = d->verify_checksums;
   for (auto& t : j->tables) j->bytes_in += t.size;
   return LC_OK;
 }

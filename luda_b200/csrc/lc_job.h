@@ -31,6 +31,7 @@ enum : uint32_t {
   kErrLimit = 7,          // an engine limit was exceeded
   kErrRetryExact = 8,     // the single-pass decode's bounded key arena (or key length
                           // bound) was too small: the host reruns the job with counting
+  kErrChecksum = 9,       // a data block's stored CRC32C does not match its contents
 };
 
 struct Counters {
@@ -79,6 +80,7 @@ struct JobDev {
   uint32_t restart_interval;
   int32_t bits_per_key;  // <= 0: no filter
   uint32_t bloom_k;
+  uint32_t verify_checksums;  // check every input data block's trailer CRC
   uint64_t max_file_size;
   uint64_t smallest_snapshot;
   int64_t max_gp_overlap;  // 10 * max_file_size

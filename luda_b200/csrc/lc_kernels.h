@@ -33,6 +33,7 @@ struct Batch {
   uint32_t merge_rounds = 0;
   uint32_t chunk = 4096;
   uint32_t chain_smem_words = 11 * 1024;
+  bool any_verify = false;  // some job checks its input blocks' CRCs
   // tunables (chosen by the autotuner in lc_engine.cu)
   uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
   uint32_t merge_items = 8;   // outputs per thread in a merge round
@@ -63,6 +64,9 @@ void launch_table_index_entries(const Batch& bt, cudaStream_t st);
 void launch_block_count(const Batch& bt, cudaStream_t st);     // exact key counts (full walk)
 void launch_block_restarts(const Batch& bt, cudaStream_t st);  // entry counts from restart words
 void launch_run_bounds(const Batch& bt, cudaStream_t st);
+// Checks the CRC32C trailer of every input data block of the jobs that ask
+// for it (verify_checksums), after the block list is known.
+void launch_verify_blocks(const Batch& bt, cudaStream_t st);
 // Copies n bytes with a kernel (no copy engine); one side may be mapped
 // pinned host memory given by its device alias.  False (nothing launched)
 // unless both addresses are 16-byte aligned.

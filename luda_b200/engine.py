@@ -74,7 +74,8 @@ class LcJobDesc(C.Structure):
                 ("n_grandparents", C.c_int32), ("grandparents", C.POINTER(LcFileRange)),
                 ("n_base_files", C.c_int32), ("base_files", C.POINTER(LcFileRange)),
                 ("smallest_snapshot", C.c_uint64), ("options", LcTableOptions),
-                ("inputs_on_device", C.c_int32), ("outputs_on_device", C.c_int32)]
+                ("inputs_on_device", C.c_int32), ("outputs_on_device", C.c_int32),
+                ("verify_checksums", C.c_int32)]
 
 
 class LcJobOut(C.Structure):
@@ -245,7 +246,7 @@ def table_options(o: TableOptions) -> LcTableOptions:
 
 
 def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[int]] = None,
-              outputs_on_device: int = 0) -> LcJobDesc:
+              outputs_on_device: int = 0, verify_checksums: bool = False) -> LcJobDesc:
     """The descriptor a patched DoCompactionWork would build from its
     Compaction: runs in MakeInputIterator order, grandparents_, and every file
     at levels >= L+2 for the base-level test."""
@@ -278,7 +279,8 @@ def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[
     keep.objs += [t_arr, rc, gpa, ba]
     return LcJobDesc(job.level, len(tables), t_arr, len(runs), rc, len(gp), gpa, len(base), ba,
                      job.smallest_snapshot(), table_options(job.options),
-                     1 if device_tables is not None else 0, int(outputs_on_device))
+                     1 if device_tables is not None else 0, int(outputs_on_device),
+                     1 if verify_checksums else 0)
 
 
 def _result(out: LcJobOut, outputs_on_device) -> CompactionResult:
@@ -347,11 +349,13 @@ class Engine:
             raise LcError(st, self.lib.lc_last_error().decode())
 
     def prepare(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: int = 0) -> "PreparedJob":
-        """Builds the C descriptor once, for repeated runs of the same job."""
+                outputs_on_device: int = 0, verify_checksums: bool = False) -> "PreparedJob":
+        """Builds the C descriptor once, for repeated runs of the same job.
+        ``verify_checksums`` checks every input data block's CRC first
+        (LevelDB's paranoid_checks on compaction inputs)."""
         keep = _Keep()
-        return PreparedJob(make_desc(job, keep, device_tables, outputs_on_device), keep,
-                           outputs_on_device)
+        return PreparedJob(make_desc(job, keep, device_tables, outputs_on_device,
+                                     verify_checksums), keep, outputs_on_device)
 
     def run(self, p: "PreparedJob") -> CompactionResult:
         out = LcJobOut()
@@ -374,8 +378,8 @@ class Engine:
         self.lib.lc_job_release(jh)
 
     def compact(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: int = 0) -> CompactionResult:
-        return self.run(self.prepare(job, device_tables, outputs_on_device))
+                outputs_on_device: int = 0, verify_checksums: bool = False) -> CompactionResult:
+        return self.run(self.prepare(job, device_tables, outputs_on_device, verify_checksums))
 
     @staticmethod
     def _desc_array(prepared: Sequence["PreparedJob"]):
