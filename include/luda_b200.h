@@ -153,8 +153,10 @@ typedef struct {
                                  calls) */
 } lc_job_out;
 
-/* Engine lifetime.  An engine owns one CUDA device, its streams, a stream-
- * ordered device memory pool and a set of worker threads. */
+/* Engine lifetime.  An engine owns one CUDA device, its streams, slab caches
+ * of device memory (batch scratch, outputs kept on the device) and of pinned
+ * host memory (output copies), and a set of worker threads.  Release every
+ * job handle before destroying the engine: the outputs live in its slabs. */
 lc_status lc_engine_create(const lc_config* cfg, lc_engine** out);
 void lc_engine_destroy(lc_engine* e);
 

@@ -3,13 +3,16 @@
 // Jobs run in batches; a plain compaction is a batch of one.  Every kernel
 // launch covers all jobs of the batch (grid y = job), so a batch costs the
 // same number of launches and host synchronisations as one job:
-//   upload -> table/index parse -> block count -> [sync: entry and key totals]
+//   upload -> table/index parse -> [checksums] -> entry counts
+//   -> [sync: entry totals]
 //   -> decode -> merge rounds -> drop rule + grandparent cuts -> survivors
 //   -> entry sizes -> block chain -> blocks -> files -> layout -> encode
 //      (one captured CUDA graph, replayed for later batches of the same shape)
 //   -> [sync: file counts and output sizes] -> download -> [sync]
-// Device memory comes from the device's stream-ordered pool (cudaMallocAsync),
-// whose release threshold is raised so freed blocks are reused across jobs.
+// Device memory for a batch's working arrays and for outputs kept on the
+// device comes from engine-wide slab caches (SlabCache), reused at once
+// across the workers' streams; the CRC entry points use the stream-ordered
+// pool, whose release threshold is raised so freed blocks are reused.
 // Asynchronous jobs are served by worker threads, each with its own stream,
 // descriptor array and graph cache; a worker takes every queued job that fits
 // the device budget as one batch, so jobs that arrive while a batch runs are
