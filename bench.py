@@ -412,6 +412,20 @@ def served_leg(args, local, rank, torch):
     }
 
 
+def reduce_over_ranks(dist, device, total_ms, e2e_total, in_bytes):
+    """Whole-job figures over the ranks (replicas, one job stream per GPU):
+    the slowest rank's timed totals and the input bytes of all ranks, so that
+    value = all bytes / slowest time.  ``dist`` None: one process."""
+    if dist is None:
+        return float(total_ms), float(e2e_total), float(in_bytes)
+    import torch
+    t = torch.tensor([total_ms, e2e_total], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    b = torch.tensor([float(in_bytes)], device=device, dtype=torch.float64)
+    dist.all_reduce(b)
+    return float(t[0]), float(t[1]), float(b[0])
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -543,16 +557,7 @@ def main():
     if args.served_flushes > 0:
         served_res = served_leg(args, local, rank, torch)
 
-    # max over ranks
-    if dist is not None:
-        t = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = float(t[0]), float(t[1])
-        b = torch.tensor([float(in_bytes)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(b)
-        all_in = float(b[0])
-    else:
-        all_in = float(in_bytes)
+    total_ms, e2e_total, all_in = reduce_over_ranks(dist, "cuda", total_ms, e2e_total, in_bytes)
     value = args.steps * all_in / MiB / (total_ms / 1e3)
     e2e_value = args.steps * all_in / MiB / (e2e_total / 1e3)
 
