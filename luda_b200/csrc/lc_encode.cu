@@ -316,15 +316,19 @@ __global__ void k_file_next(const JobDev* __restrict__ jobs) {
 
 // The file starts are the orbit of block 0 under b_fnext, which only moves
 // forward: the CTA loads a tile of b_fnext at the walk's position into shared
-// memory and thread 0 walks inside it; a step that leaves the tile reloads.
+// memory, one 16-byte load per thread from the 16-byte boundary at or below
+// it, and thread 0 walks inside it; a step that leaves the tile reloads.
+// (b_fnext has N >= n_blocks_out words and 16 bytes of padding, so the last
+// vector load stays inside its allocation.)
 constexpr uint32_t kFileTile = 4096;
+constexpr uint32_t kFileThreads = kFileTile / 4;
 __global__ void k_files(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
   if (threadIdx.x == 0) s_failed = J.ctr->error;
   __syncthreads();
   if (s_failed) return;
-  __shared__ uint32_t tile[kFileTile];
+  __shared__ __align__(16) uint32_t tile[kFileTile];
   __shared__ uint64_t s_b;
   __shared__ uint32_t s_f;
   __shared__ bool s_stop;
@@ -336,12 +340,12 @@ __global__ void k_files(const JobDev* __restrict__ jobs) {
   }
   __syncthreads();
   while (!s_stop) {
-    const uint64_t t0 = s_b;
-    for (uint64_t i = threadIdx.x; i < kFileTile && t0 + i < nb; i += blockDim.x)
-      tile[i] = J.b_fnext[t0 + i];
+    const uint64_t t0 = s_b & ~uint64_t(3);
+    for (uint64_t i = threadIdx.x; 4 * i < kFileTile && t0 + 4 * i < nb; i += blockDim.x)
+      reinterpret_cast<uint4*>(tile)[i] = reinterpret_cast<const uint4*>(J.b_fnext + t0)[i];
     __syncthreads();
     if (threadIdx.x == 0) {
-      uint64_t b = t0;
+      uint64_t b = s_b;
       uint32_t f = s_f;
       while (b < nb && b < t0 + kFileTile) {
         const uint64_t end = tile[b - t0];
@@ -1051,7 +1055,7 @@ void launch_files(const Batch& bt, cudaStream_t st) {
   note_launch(), k_forced_blocks<<<dim3((bt.max_cap_triggers + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
   note_launch(), k_file_next<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256, 0,
                                st>>>(bt.d);
-  note_launch(), k_files<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_files<<<dim3(1, bt.B), kFileThreads, 0, st>>>(bt.d);
 }
 void launch_block_layout(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_layout<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
