@@ -949,6 +949,17 @@ __global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
   }
   __syncthreads();
   const FileOut& F = J.files[f];
+  // the file's smallest and largest internal keys (FileMetaData::smallest /
+  // largest) into slots 2f and 2f + 1 of fkey_stride bytes, their lengths
+  // into fkoff; every key fits a slot (a single-pass job with a longer key
+  // was rerun with exact counting, whose stride is the longest key)
+  for (uint32_t which = 0; which < 2; which++) {
+    uint32_t l;
+    const uint8_t* k = kept_key(J, which ? F.end_kept - 1 : F.first_kept, &l);
+    uint8_t* d = J.fkeys + (2ull * f + which) * J.fkey_stride;
+    for (uint32_t t = threadIdx.x; t < l; t += blockDim.x) d[t] = k[t];
+    if (threadIdx.x == 0) J.fkoff[2 * f + which] = l;
+  }
   for (uint32_t which = 0; which < 3; which++) {
     if (which == 0 && J.bits_per_key <= 0) continue;
     const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
@@ -976,52 +987,6 @@ __global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
       st_le32(p + len + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
     }
     __syncthreads();
-  }
-}
-
-// Smallest / largest internal key of every output file, packed: one CTA;
-// koff[2f], koff[2f+1] start file f's smallest and largest key.
-__global__ void k_file_keys(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  uint8_t* out = J.fkeys;
-  uint64_t* koff = J.fkoff;
-  __shared__ uint64_t s_warp[32];
-  __shared__ uint64_t s_carry;
-  const uint32_t nf = J.ctr->error ? 0 : J.ctr->n_files;
-  const uint32_t nk = 2 * nf;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  // lengths -> offsets (block-wide scan in chunks of blockDim)
-  for (uint32_t base = 0; base < nk; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    uint64_t l = 0;
-    if (i < nk) {
-      uint32_t kl;
-      kept_key(J, (i & 1) ? J.files[i >> 1].end_kept - 1 : J.files[i >> 1].first_kept, &kl);
-      l = kl;
-    }
-    uint64_t tot;
-    uint64_t ex = warp_excl<uint64_t>(l, &tot);
-    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = tot;
-    __syncthreads();
-    uint64_t before = s_carry, all = 0;
-    for (uint32_t w = 0; w < blockDim.x / 32; w++) {
-      if (w < (threadIdx.x >> 5)) before += s_warp[w];
-      all += s_warp[w];
-    }
-    if (i < nk) koff[i] = before + ex;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry += all;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) koff[nk] = s_carry;
-  __syncthreads();
-  for (uint32_t i = threadIdx.x >> 5; i < nk; i += blockDim.x >> 5) {
-    const uint32_t f = i >> 1;
-    uint32_t l;
-    const uint8_t* k = kept_key(J, (i & 1) ? J.files[f].end_kept - 1 : J.files[f].first_kept, &l);
-    uint8_t* d = out + koff[i];
-    for (uint32_t t = threadIdx.x & 31; t < l; t += 32) d[t] = k[t];
   }
 }
 
@@ -1084,9 +1049,6 @@ void launch_encode_index(const Batch& bt, cudaStream_t st) {
 }
 void launch_encode_meta(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 256, 0, st>>>(bt.d);
-}
-void launch_file_keys(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_file_keys<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
 }
 
 }  // namespace lc

@@ -577,7 +577,6 @@ void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer
   T.mark(kEncodeBlocks);
   launch_encode_filters(bt, st);
   launch_encode_index(bt, st);
-  launch_file_keys(bt, st);
   launch_encode_meta(bt, st);
   T.mark(kEncodeMeta);
 }
@@ -655,6 +654,7 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   }
   J.out = A.output(J.cap_out, r.j->outputs_on_device == 1 || r.j->outputs_on_device == 2);
   J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
+  J.fkey_stride = r.max_klen;
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
   J.cap_scan = N + 1;
   J.scan_scratch = A.get<uint64_t>(scan_scratch_elems(N + 1));
@@ -1167,7 +1167,8 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       q += (sizeof(FileOut) * r.J.cap_files + 15) & ~size_t(15);
       memcpy(r.koff.data(), q, 8 * (2ull * nf + 1));
       q += (8 * (2ull * r.J.cap_files + 1) + 15) & ~size_t(15);
-      const uint64_t kb = nf ? r.koff[2ull * nf] : 0;
+      // keys in fixed slots of max_klen bytes, their lengths in koff
+      const uint64_t kb = 2ull * nf * r.max_klen;
       memcpy(r.j->key_bytes.data(), q, std::min<uint64_t>(kb, r.j->key_bytes.size()));
     }
     std::vector<lc_job*> retry;  // single-pass jobs whose key arena was too small
@@ -1209,10 +1210,10 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         j->file_offset[f] = F.out_off;
         j->file_size[f] = F.size;
         j->file_entries[f] = F.end_kept - F.first_kept;
-        j->small_off[f] = r.koff[2 * f];
-        j->small_len[f] = (uint32_t)(r.koff[2 * f + 1] - r.koff[2 * f]);
-        j->large_off[f] = r.koff[2 * f + 1];
-        j->large_len[f] = (uint32_t)(r.koff[2 * f + 2] - r.koff[2 * f + 1]);
+        j->small_off[f] = 2ull * f * r.max_klen;
+        j->small_len[f] = (uint32_t)r.koff[2 * f];
+        j->large_off[f] = (2ull * f + 1) * r.max_klen;
+        j->large_len[f] = (uint32_t)r.koff[2 * f + 1];
       }
       j->bytes_out = nbytes;
       j->entries_out = hc[i].n_kept;
@@ -1382,10 +1383,10 @@ void run_build(lc_job* j, lc_slot& slot) {
       j->file_offset[f] = r.files[f].out_off;
       j->file_size[f] = r.files[f].size;
       j->file_entries[f] = r.files[f].end_kept - r.files[f].first_kept;
-      j->small_off[f] = r.koff[2 * f];
-      j->small_len[f] = (uint32_t)(r.koff[2 * f + 1] - r.koff[2 * f]);
-      j->large_off[f] = r.koff[2 * f + 1];
-      j->large_len[f] = (uint32_t)(r.koff[2 * f + 2] - r.koff[2 * f + 1]);
+      j->small_off[f] = 2ull * f * r.max_klen;
+      j->small_len[f] = (uint32_t)r.koff[2 * f];
+      j->large_off[f] = (2ull * f + 1) * r.max_klen;
+      j->large_len[f] = (uint32_t)r.koff[2 * f + 1];
     }
     T.mark(kDownload);
     CK(cudaStreamSynchronize(st));

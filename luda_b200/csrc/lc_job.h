@@ -191,8 +191,10 @@ struct JobDev {
   // scratch of the batched kernels
   uint32_t* gp_first;        // per grandparent count g: first merged position reaching g
   uint32_t* tmp32;           // block bytes with trailers (scan input)
-  uint8_t* fkeys;            // smallest / largest key of every file, packed
-  uint64_t* fkoff;           // 2 * cap_files + 1 offsets into fkeys
+  uint8_t* fkeys;            // smallest / largest key of file f in slots 2f, 2f + 1
+                             // of fkey_stride bytes each
+  uint64_t* fkoff;           // their lengths (2 * cap_files)
+  uint32_t fkey_stride;      // longest internal key the job can hold
   const uint64_t* src_koffs; // flush encoder: key offsets (n + 1)
   const uint64_t* src_voffs; // flush encoder: value offsets (n + 1)
   uint64_t* scan_scratch;    // tile sums of the prefix sums

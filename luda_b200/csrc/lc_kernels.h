@@ -92,7 +92,6 @@ void launch_file_layout(const Batch& bt, cudaStream_t st);
 void launch_encode_blocks(const Batch& bt, cudaStream_t st);
 void launch_encode_filters(const Batch& bt, cudaStream_t st);
 void launch_encode_index(const Batch& bt, cudaStream_t st);
-void launch_file_keys(const Batch& bt, cudaStream_t st);
 // metaindex, footer, filter tails and the trailers of filter/meta/index
 void launch_encode_meta(const Batch& bt, cudaStream_t st);
 
