@@ -658,7 +658,6 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
   J.cap_scan = N + 1;
   J.scan_scratch = A.get<uint64_t>(scan_scratch_elems(N + 1));
-  J.scan_scratch2 = A.get<uint64_t>(scan_scratch_elems(N + 1));
 }
 
 }  // namespace
@@ -974,8 +973,6 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     uint8_t* d_in_all = in_total ? A.get<uint8_t>(in_total) : nullptr;
     Counters* d_ctr = A.get<Counters>(B);
     CK(cudaMemsetAsync(d_ctr, 0, sizeof(Counters) * B, st));
-    uint64_t zero_word_off = S.h.size();  // (unused) keeps Stage layout stable
-    (void)zero_word_off;
     Batch bt;
     bt.d = slot.d_jobs;
     bt.B = B;

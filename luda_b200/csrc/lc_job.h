@@ -198,7 +198,6 @@ struct JobDev {
   const uint64_t* src_koffs; // flush encoder: key offsets (n + 1)
   const uint64_t* src_voffs; // flush encoder: value offsets (n + 1)
   uint64_t* scan_scratch;    // tile sums of the prefix sums
-  uint64_t* scan_scratch2;   // ... of a scan that runs beside another one (index sizes)
   uint64_t cap_scan;         // capacity of the arrays scanned (for the tile sums)
 
   // CRC32C shift table: x^(8m) mod P for m in [0, crc_tab_n)

@@ -103,11 +103,10 @@ struct ScanOf<kScanIcum> {
   static __device__ uint64_t* total(const JobDev&) { return nullptr; }
 };
 
-// Tile-sum scratch of a scan: the index-size scan runs on a side stream
-// beside the filter-size scan, so it has its own.
+// Tile-sum scratch of a scan (the scans of a job run one after another).
 template <int S>
 __device__ __forceinline__ uint64_t* scan_tiles_of(const JobDev& J) {
-  return S == kScanIcum ? J.scan_scratch2 : J.scan_scratch;
+  return J.scan_scratch;
 }
 
 template <typename T>
