@@ -221,15 +221,19 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
       }
       ex += vals[k];
     }
-    carry += block_sum<TO>(tile_sums, t, t + gridDim.x < n_tiles ? t + gridDim.x : n_tiles);
+    if ((t + gridDim.x) * kTile <= n)  // another tile of this CTA follows
+      carry += block_sum<TO>(tile_sums, t, t + gridDim.x < n_tiles ? t + gridDim.x : n_tiles);
   }
 }
 
 template <int S>
 void scan_sel(const Batch& bt, uint64_t n_cap, cudaStream_t st) {
   const unsigned tiles = grid_x(n_cap + 1, kTile, 148 * 8);
-  note_launch(2);
-  k_tile_reduce<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
+  // one tile (n + 1 <= kTile for every job of the batch): no tile sums to
+  // add, so the scan pass alone does it
+  const bool one_tile = n_cap + 1 <= kTile;
+  note_launch(one_tile ? 1 : 2);
+  if (!one_tile) k_tile_reduce<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
   k_tile_scan<S><<<dim3(tiles, bt.B), kScanThreads, 0, st>>>(bt.d);
 }
 
