@@ -128,8 +128,10 @@ typedef struct {
   const uint64_t* file_offset;  /* n_files, offset of file i in data */
   const uint64_t* file_size;    /* n_files */
   const uint64_t* file_entries; /* n_files, TableBuilder::NumEntries() */
-  const uint8_t* key_bytes;     /* smallest/largest internal keys, packed */
-  const uint64_t* smallest_offset; /* n_files + 0: key i at key_bytes[off, off+len) */
+  const uint8_t* key_bytes;     /* every file's smallest and largest internal keys (in
+                                   fixed-size slots; use the offsets and lengths) */
+  const uint64_t* smallest_offset; /* n_files: file i's smallest key is
+                                      key_bytes[smallest_offset[i], + smallest_len[i]) */
   const uint32_t* smallest_len;
   const uint64_t* largest_offset;
   const uint32_t* largest_len;
