@@ -47,3 +47,34 @@ def test_version_and_status_strings(lib):
 def test_library_built_for_sm100a():
     # the build passes exactly one gencode: compute_100a -> sm_100a
     assert lbuild.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_ctypes_structs_match_header_layout():
+    """Every ctypes mirror of a header struct has the C size and field offsets
+    (a small C program compiled against the header prints them)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = [("lc_config", engine.LcConfig), ("lc_engine_stats", engine.LcEngineStats),
+             ("lc_tuning", engine.LcTuning), ("lc_table", engine.LcTable),
+             ("lc_file_range", engine.LcFileRange), ("lc_table_options", engine.LcTableOptions),
+             ("lc_job_desc", engine.LcJobDesc), ("lc_job_out", engine.LcJobOut)]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "luda_b200.h"',
+             "int main(void) {"]
+    want = []
+    for cname, py in pairs:
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes.sizeof(py))
+        for f in py._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {f[0]}));')
+            want.append(getattr(py, f[0]).offset)
+    lines += ["  return 0;", "}"]
+    out_dir = os.path.join(ROOT, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "abi_layout")
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), "-x", "c", "-",
+                    "-o", exe], input="\n".join(lines).encode(), check=True)
+    got = [int(x) for x in subprocess.run([exe], capture_output=True, check=True).stdout.split()]
+    assert got == want
