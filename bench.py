@@ -364,7 +364,8 @@ def served_leg(args, local, rank, torch):
     def run(mode, rate):
         eng = engines[mode]
         if mode == "served":
-            srv = served.Server(eng, len(flushes), mode="served", upload=up.upload, free=up.free)
+            srv = served.Server(eng, len(flushes), mode="served", upload=up.upload, free=up.free,
+                                ready=up.ready)
         else:
             srv = served.Server(eng, len(flushes), mode="plain")
         s0 = eng.stats()

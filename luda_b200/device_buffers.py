@@ -1,9 +1,11 @@
 """Device copies of host table bytes for the served loop (torch allocations).
 
-``upload(data)`` copies one table to the device and returns (device address,
-handle); dropping the handle (``free``) returns the memory to torch's caching
-allocator.  The copy has finished when ``upload`` returns, so a job submitted
-on another stream may read it at once.
+``upload(data)`` starts copying one table to the device on the uploader's own
+stream and returns (device address, handle) at once; ``ready(handle)`` waits
+until that copy has finished, which the loop does before it submits the first
+job that reads the table (on another stream).  Dropping the handle (``free``)
+returns the memory to torch's caching allocator, whose stream-ordered reuse
+keeps a copy still in flight safe.
 """
 from __future__ import annotations
 
@@ -27,8 +29,16 @@ class TorchUploader:
             dst = torch.empty(max(16, a.size + 16), dtype=torch.uint8,
                               device=f"cuda:{self.device}")
             dst[:a.size].copy_(src, non_blocking=True)
-        self.stream.synchronize()
-        return dst.data_ptr(), dst
+            done = torch.cuda.Event()
+            done.record(self.stream)
+        # the source stays referenced until the copy is known to be done
+        return dst.data_ptr(), [dst, src, done]
+
+    @staticmethod
+    def ready(handle):
+        if handle[1] is not None:
+            handle[2].synchronize()
+            handle[1] = None
 
     @staticmethod
     def free(handle):

@@ -104,6 +104,7 @@ class SimTable:
     host: object = None  # table bytes in host memory (the persisted copy)
     dev: int = 0  # device address of the same bytes, 0 if not resident
     owner: object = None  # _Owner keeping host/device memory alive
+    ready: Optional[Callable[[], None]] = None  # waits until the device copy exists
 
 
 class _Owner:
@@ -373,17 +374,20 @@ class Server:
     """The request loop.  ``engine`` is a :class:`luda_b200.engine.Engine`
     (or an object with the same ``prepare`` / ``submit_prepared`` /
     ``wait_any`` methods); ``upload(bytes) -> (device address, handle)`` and
-    ``free(handle)`` move new level-0 tables to the device in served mode."""
+    ``free(handle)`` move new level-0 tables to the device in served mode, and
+    ``ready(handle)``, when given, waits until an upload that ``upload``
+    started asynchronously has finished (called before the first job that
+    reads the table is submitted)."""
 
     def __init__(self, engine, n_db: int, mode: str = "served",
                  options: Optional[TableOptions] = None, upload=None, free=None,
-                 record_bytes: bool = False, level_scale: float = 1.0):
+                 record_bytes: bool = False, level_scale: float = 1.0, ready=None):
         assert mode in ("served", "plain")
         self.engine = engine
         self.mode = mode
         self.options = options or TableOptions()
         self.dbs = [SimDB(i, self.options, level_scale) for i in range(n_db)]
-        self.upload, self.free = upload, free
+        self.upload, self.free, self.ready = upload, free, ready
         self.record_bytes = record_bytes
         self.h2d = 0
         self.d2h = 0
@@ -395,6 +399,8 @@ class Server:
             addr, handle = self.upload(f.data)
             t.dev = addr
             t.owner = _Owner(handle, 1, self.free)
+            if self.ready is not None:
+                t.ready = lambda h=handle: self.ready(h)
             self.h2d += len(f.data)
         return t
 
@@ -423,6 +429,10 @@ class Server:
         tables = job.input_tables()
         resident = sum(1 for f in tables if f.sim.dev)
         if self.mode == "served" and resident == len(tables):
+            for f in tables:
+                if f.sim.ready is not None:
+                    f.sim.ready()
+                    f.sim.ready = None
             p = self.engine.prepare(job, device_tables=[f.sim.dev for f in tables],
                                     outputs_on_device=2)
         else:

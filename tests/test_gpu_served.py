@@ -38,7 +38,8 @@ def test_served_jobs_same_alone_and_in_mix(flushes, rate):
     up = TorchUploader(0)
     with Engine(0, max_inflight=3) as eng:
         srv = served.Server(eng, len(fl), mode="served", options=opts, upload=up.upload,
-                            free=up.free, record_bytes=True, level_scale=1 / 16.0)
+                            free=up.free, ready=up.ready, record_bytes=True,
+                            level_scale=1 / 16.0)
         st = srv.run(served.schedule(fl, rate))
         assert len(st.jobs) > 0 and {j.level for j in st.jobs} >= {0, 1}
         assert any(j.resident_inputs == j.n_inputs and j.n_inputs > 0 for j in st.jobs)
