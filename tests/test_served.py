@@ -113,6 +113,42 @@ def test_served_loop_keeps_newest_values(small_flushes, mode):
     srv.close()
 
 
+def test_uploads_ready_before_a_job_reads_them(small_flushes):
+    """Level-0 uploads may still be in flight when upload() returns: the loop
+    must call ready() on every uploaded table before it hands the table's
+    device address to a job."""
+    opts, flushes = small_flushes
+    handles = {}
+
+    def upload(data):
+        addr = 4096 * (len(handles) + 1)
+        handles[addr] = {"ready": False}
+        return addr, handles[addr]
+
+    def ready(h):
+        h["ready"] = True
+
+    class DeviceOracle(OracleEngine):
+        device_jobs = 0
+
+        def prepare(self, job, device_tables=None, outputs_on_device=0):
+            if device_tables is not None:
+                assert all(handles[a]["ready"] for a in device_tables)
+                self.device_jobs += 1
+            for f in job.input_tables():
+                f.data = f.sim.host
+            return oracle.compact(job, "oracle")
+
+    eng = DeviceOracle(seed=2)
+    srv = served.Server(eng, len(flushes), mode="served", options=opts, upload=upload,
+                        free=lambda h: None, ready=ready, level_scale=1 / 128.0)
+    srv.run(served.schedule(flushes, None), idle_wait=lambda s: None)
+    assert eng.device_jobs > 0
+    for db, fl in zip(srv.dbs, flushes):
+        assert db_contents(db) == _newest([fl])
+    srv.close()
+
+
 def test_pick_follows_compaction_pointer():
     db = served.SimDB(0, TableOptions(), level_scale=1e-6)
 
