@@ -22,7 +22,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liblsm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libluda_ref.so")
-REF_ROOT = os.environ.get("LUDA_REF_ROOT", "/root/reference")
+# Location of the reference source tree, for building the reference library
+# only (the built library travels with the repository; nothing reads the
+# sources at run time).  No default: the caller names it.
+REF_ROOT = os.environ.get("LUDA_REF_ROOT")
 
 _u8p = C.POINTER(C.c_uint8)
 _u64p = C.POINTER(C.c_uint64)
@@ -62,12 +65,13 @@ class RefJob(C.Structure):
                 ("max_file_size", C.c_uint64)]
 
 
-def build(ref: bool = True) -> None:
-    """Builds the restatement and, when the reference sources are present,
-    the reference library."""
+def build(ref: bool = True, ref_root: Optional[str] = None) -> None:
+    """Builds the restatement and, when ``ref_root`` (or ``LUDA_REF_ROOT``)
+    names an existing reference source tree, the reference library."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(REF_ROOT):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"],
+    root = ref_root or REF_ROOT
+    if ref and root and os.path.isdir(root):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={root}"],
                        check=True)
 
 
