@@ -73,6 +73,9 @@ def build(ref: bool = True, ref_root: Optional[str] = None) -> None:
     if ref and root and os.path.isdir(root):
         subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={root}"],
                        check=True)
+        # the compiled drop-in and its CPU twin (needs the engine library built)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "dropin", f"REF_ROOT={root}"],
+                       check=True)
 
 
 _libs = {}
@@ -127,6 +130,23 @@ def lib(impl: str = "oracle"):
 
 def has_ref() -> bool:
     return os.path.exists(REF_SO)
+
+
+# The reference LevelDB driven through leveldb::DB by oracle/db_scenario.cc:
+# with the reference's CPU DoCompactionWork, and with the luda_b200 drop-in.
+SCENARIO_CPU = os.path.join(HERE, "_ref", "db_scenario_cpu")
+SCENARIO_DROPIN = os.path.join(HERE, "_ref", "db_scenario_luda_b200")
+
+
+def run_scenario(exe: str, db_dir: str, seed: int, timeout_s: float = 300.0) -> dict:
+    """Runs one scenario executable on a fresh DB directory; its JSON line."""
+    import json
+    r = subprocess.run([exe, db_dir, str(seed)], capture_output=True, text=True,
+                       timeout=timeout_s)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(exe)} failed ({r.returncode}): "
+                           f"{r.stdout[-500:]} {r.stderr[-500:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def _ptr(a: np.ndarray, t=_u8p):
