@@ -184,6 +184,15 @@ lc_status lc_job_wait_any(lc_engine* e, lc_job* const* jobs, int32_t n, int64_t 
  * them has completed. */
 void lc_job_release(lc_job* j);
 
+/* The device memory lc_job_submit admits a job with, against
+ * lc_config.device_budget_bytes: the input copy (host inputs), the parse
+ * arrays, the key arena, the output and the per-entry arrays, with the entry
+ * count taken as one per 40 input bytes (it is known only after the parse;
+ * a running batch then holds what it really allocated).  A job whose
+ * estimate exceeds the budget is refused with LC_ERR_BUDGET.  No counterpart
+ * in the reference, whose compactions run one at a time. */
+lc_status lc_estimate_device_bytes(const lc_job_desc* desc, uint64_t* bytes);
+
 /* Synchronous compaction on the calling thread: the drop-in for one
  * DoCompactionWork call.  *job_out must be released with lc_job_release. */
 lc_status lc_compact(lc_engine* e, const lc_job_desc* desc, lc_job_out* out, lc_job** job_out);
@@ -283,9 +292,11 @@ lc_status lc_crc32c(lc_engine* e, const uint8_t* data, uint64_t n, int32_t on_de
  * device that loads the library until the process exits), so n is limited to
  * 1 GiB; larger buffers are rejected with LC_ERR_UNSUPPORTED before anything
  * is launched.  Null pointers give LC_ERR_INVALID_ARG, runtime failures
- * LC_ERR_CUDA.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.  Every call clears the part of the array that must
+ * LC_ERR_CUDA; each failure also sets lc_last_error().  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current and keeps it; make that first call before any stream capture,
+ * and do not use the entry point across a cudaDeviceReset (the kept address
+ * belongs to the context that was reset).  Every call clears the part of the array that must
  * start at zero, but all calls share the array: calls that overlap on the GPU
  * (on different streams, or from different threads) race, so serialise them,
  * e.g. on one stream. */

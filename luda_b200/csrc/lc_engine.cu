@@ -231,6 +231,17 @@ struct lc_engine {
     while (ns > cur && !setup_ns_max.compare_exchange_weak(cur, ns)) {
     }
   }
+  // Adds delta to the device bytes admitted jobs hold (a batch trues up its
+  // admission estimate once its entry counts are known); a decrease may
+  // admit queued jobs.
+  void adjust_inflight(int64_t delta) {
+    if (!delta) return;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      inflight_bytes = (uint64_t)((int64_t)inflight_bytes + delta);
+    }
+    if (delta < 0) admit_cv.notify_all();
+  }
   lc_slot* take_slot();
   void put_slot(lc_slot* s);
   Tunables tuning() {
@@ -301,6 +312,7 @@ struct DevAlloc {
   uint8_t* cur = nullptr;
   uint64_t left = 0;
   uint64_t n_takes = 0, take_ns = 0;  // blocks taken and the host time it took
+  uint64_t used = 0;                  // bytes of scratch chunks and outputs taken
   DevAlloc(cudaStream_t s, lc_engine* e) : st(s), eng(e) {}
   ~DevAlloc() {
     release({});
@@ -333,6 +345,7 @@ struct DevAlloc {
       cur = take(eng->scratch, std::max(bytes, kChunkBytes), &cap, "cudaMalloc (scratch slab)");
       chunks.emplace_back(cur, cap);
       left = cap;
+      used += cap;
     }
     T* r = (T*)cur;
     cur += bytes;
@@ -346,6 +359,7 @@ struct DevAlloc {
     uint8_t* p = take(eng->dev_out, std::max<uint64_t>(bytes, 16) + 64, &cap,
                       "cudaMalloc (device output slab)");
     outs.emplace_back(p, cap);
+    used += cap;
     return p;
   }
   // once the batch has completed: returns the part of output p past its
@@ -837,10 +851,27 @@ namespace {
 // beyond either is rerun with exact counting.
 constexpr uint32_t kFastMaxKey = 256;
 
+// Holds the difference between a batch's admitted estimate and the device
+// memory it actually took in the engine's in-flight bytes until the batch
+// has released its scratch.
+struct InflightTrueUp {
+  lc_engine* e;
+  int64_t delta = 0;
+  explicit InflightTrueUp(lc_engine* eng) : e(eng) {}
+  void set(int64_t d) {
+    e->adjust_inflight(d - delta);
+    delta = d;
+  }
+  ~InflightTrueUp() { e->adjust_inflight(-delta); }
+};
+
+// `admitted`: the device bytes a worker charged for these jobs at admission
+// (0 for synchronous calls, which are not admitted against the budget).
 void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
-               bool exact = false) {
+               bool exact = false, uint64_t admitted = 0) {
   if (jobs.empty()) return;
   lc_engine* e = jobs[0]->eng;
+  InflightTrueUp trueup(e);
   const auto t_setup0 = std::chrono::steady_clock::now();
   cudaStream_t st = slot.st;
   DevAlloc A(st, e);
@@ -1103,6 +1134,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       bt.max_cap_triggers = std::max<uint32_t>(bt.max_cap_triggers, r.J.cap_triggers);
       bt.max_cap_files = std::max<uint32_t>(bt.max_cap_files, r.J.cap_files);
     }
+    // the batch's device memory is now known (every array is sized): the
+    // admission charge becomes what the batch holds
+    if (admitted) trueup.set((int64_t)A.used - (int64_t)admitted);
     // grid shapes in powers of two, so that batches of similar size share a
     // captured graph (the kernels loop over whatever the grid leaves)
     bt.max_entries = pow2_at_least(std::max<uint64_t>(bt.max_entries, 1));
@@ -1245,7 +1279,12 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       cudaEventDestroy(ev0);
       cudaEventDestroy(ev1);
       e->n_exact_reruns += retry.size();
-      run_batch(retry, slot, tun, true);
+      // this batch's scratch is released: the rerun holds the charge
+      trueup.set(0);
+      uint64_t readmit = 0;
+      if (admitted)
+        for (auto* j : retry) readmit += j->est_bytes;
+      run_batch(retry, slot, tun, true, readmit);
       return;
     }
   } catch (const CudaError& ce) {
@@ -1411,11 +1450,24 @@ void run_build(lc_job* j, lc_slot& slot) {
   }
 }
 
+// Device bytes a job is admitted with, from the sizes run_batch gives its
+// arrays: the input copy (host inputs), the per-block parse arrays, the key
+// arena, the output and the per-entry arrays.  The entry count is not known
+// before the parse; it is taken as one entry per kEstEntryBytes of input
+// (the at-size workloads have 67-250 bytes per entry) and the worker trues
+// the charge up to the batch's real allocation once the counts are known.
+constexpr uint64_t kEstEntryBytes = 40;
+constexpr uint64_t kEntryArrayBytes = 160;  // per-entry arrays of alloc_tail, rounded up
 uint64_t estimate_bytes(const lc_job* j) {
   uint64_t in = 0;
-  for (auto& t : j->tables) in += t.size;
-  if (j->kind == 1) in = j->bkoffs && !j->inputs_on_device ? j->bkoffs[j->bn] + j->bvoffs[j->bn] : 0;
-  return 24 * in + (64ull << 20);
+  for (auto& t : j->tables) in += round16(t.size);
+  if (j->kind == 1) in = j->bkoffs ? j->bkoffs[j->bn] + j->bvoffs[j->bn] : 0;
+  const uint64_t n_est = in / kEstEntryBytes + 1;
+  const uint64_t host_copy = j->inputs_on_device ? 0 : in + 16;
+  const uint64_t parse = (in / 13 + j->tables.size() + 1) * 48;
+  const uint64_t arena = in + 65536;
+  const uint64_t out = in + in / 4 + n_est * 66 + 65536;
+  return host_copy + parse + arena + out + n_est * kEntryArrayBytes + (8ull << 20);
 }
 
 void finish(lc_job* j) {
@@ -1479,7 +1531,7 @@ void worker_main(lc_engine* e, lc_slot* wslot) {
     } else {
       cudaSetDevice(e->device);
       if (batch.size() == 1 && batch[0]->kind == 1) run_build(batch[0], slot);
-      else run_batch(batch, slot, e->tuning());
+      else run_batch(batch, slot, e->tuning(), false, bytes);
     }
     {
       std::lock_guard<std::mutex> g(e->mu);
@@ -1585,6 +1637,12 @@ extern "C" {
 
 const char* lc_version(void) { return kVersion; }
 const char* lc_last_error(void) { return g_last_error.c_str(); }
+}  // extern "C"
+
+// The error text of entry points outside this file (lc_noalloc.cu).
+void lc::set_last_error(const std::string& msg) { g_last_error = msg; }
+
+extern "C" {
 
 const char* lc_status_string(lc_status s) {
   switch (s) {
@@ -1702,6 +1760,15 @@ lc_status lc_job_submit(lc_engine* e, const lc_job_desc* desc, lc_job** out) {
   }
   e->cv.notify_one();
   *out = j;
+  return LC_OK;
+}
+
+lc_status lc_estimate_device_bytes(const lc_job_desc* desc, uint64_t* bytes) {
+  if (!desc || !bytes) return fail(LC_ERR_INVALID_ARG, "null argument");
+  lc_job j;
+  lc_status s = copy_desc(&j, desc);
+  if (s != LC_OK) return s;
+  *bytes = estimate_bytes(&j);
   return LC_OK;
 }
 

@@ -98,7 +98,7 @@ EXPORTS = ["lc_engine_create", "lc_engine_destroy", "lc_job_submit", "lc_job_wai
            "lc_job_result", "lc_job_release", "lc_compact", "lc_build_table", "lc_last_error",
            "lc_status_string", "lc_version", "lc_crc32c", "lc_crc32c_noalloc",
            "lc_compact_batch", "lc_get_tuning", "lc_set_tuning", "lc_autotune",
-           "lc_job_wait_any", "lc_engine_get_stats"]
+           "lc_job_wait_any", "lc_engine_get_stats", "lc_estimate_device_bytes"]
 
 
 class LcError(RuntimeError):
@@ -133,6 +133,8 @@ def load_library(path: str = LIB_PATH):
     l.lc_compact.argtypes = [C.c_void_p, C.POINTER(LcJobDesc), C.POINTER(LcJobOut),
                              C.POINTER(C.c_void_p)]
     l.lc_compact.restype = C.c_int
+    l.lc_estimate_device_bytes.argtypes = [C.POINTER(LcJobDesc), C.POINTER(C.c_uint64)]
+    l.lc_estimate_device_bytes.restype = C.c_int
     l.lc_engine_get_stats.argtypes = [C.c_void_p, C.POINTER(LcEngineStats)]
     l.lc_engine_get_stats.restype = C.c_int
     l.lc_job_wait_any.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.c_int64,
@@ -420,6 +422,12 @@ class Engine:
     def compact_batch(self, jobs: Sequence[CompactionJob],
                       outputs_on_device: int = 0) -> List[CompactionResult]:
         return self.run_batch([self.prepare(j, None, outputs_on_device) for j in jobs])
+
+    def estimate_device_bytes(self, p: "PreparedJob") -> int:
+        """Device bytes the job is admitted with (``lc_estimate_device_bytes``)."""
+        v = C.c_uint64()
+        self._check(self.lib.lc_estimate_device_bytes(C.byref(p.desc), C.byref(v)))
+        return v.value
 
     def stats(self) -> dict:
         """Engine counters (``lc_engine_get_stats``)."""

@@ -78,3 +78,30 @@ def test_ctypes_structs_match_header_layout():
                     "-o", exe], input="\n".join(lines).encode(), check=True)
     got = [int(x) for x in subprocess.run([exe], capture_output=True, check=True).stdout.split()]
     assert got == want
+
+
+def test_two_gib_job_is_admitted_under_default_budget(lib):
+    """lc_estimate_device_bytes only reads the descriptor (no device work): a
+    job of 32 tables of 64 MiB (2 GiB) from host memory is admitted under the
+    default 40 GiB budget, and the estimate grows with the input."""
+    lib.lc_estimate_device_bytes.argtypes = [ctypes.POINTER(engine.LcJobDesc),
+                                             ctypes.POINTER(ctypes.c_uint64)]
+    lib.lc_estimate_device_bytes.restype = ctypes.c_int
+    dummy = ctypes.create_string_buffer(16)  # never read: only the sizes count
+
+    def estimate(n_tables, table_bytes):
+        tabs = (engine.LcTable * n_tables)()
+        for t in tabs:
+            t.data = ctypes.addressof(dummy)
+            t.size = table_bytes
+        runs = (ctypes.c_int32 * 2)(1, n_tables - 1)
+        d = engine.LcJobDesc()
+        d.level, d.n_tables, d.tables, d.n_runs, d.run_table_count = 1, n_tables, tabs, 2, runs
+        d.options = engine.LcTableOptions(4096, 16, 10, 64 << 20)
+        v = ctypes.c_uint64()
+        assert lib.lc_estimate_device_bytes(ctypes.byref(d), ctypes.byref(v)) == 0
+        return v.value
+
+    two_gib = estimate(32, 64 << 20)
+    assert 2 << 30 < two_gib < 40 << 30
+    assert estimate(16, 64 << 20) < two_gib
