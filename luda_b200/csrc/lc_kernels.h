@@ -10,9 +10,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "lc_job.h"
 
 namespace lc {
+
+// Sets the calling thread's lc_last_error() text.
+void set_last_error(const std::string& msg);
 
 // Kernel launches made by the calling thread (each batch runs on one thread).
 void note_launch(uint32_t n = 1);

@@ -10,13 +10,18 @@
 // Host code must not use the array's name as a device address (in host code
 // it is only a stand-in), so the first call on each device looks the address
 // up with cudaGetSymbolAddress while that device is current and caches it.
+// The cached address belongs to the device's current context: after a
+// cudaDeviceReset the module is loaded again, possibly elsewhere, so the
+// entry point must not be used across a device reset.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <mutex>
+#include <string>
 
 #include "../../include/luda_b200.h"
 #include "lc_crc_chunks.cuh"
+#include "lc_kernels.h"
 
 namespace {
 
@@ -37,11 +42,12 @@ __global__ void __launch_bounds__(lc::kCrcChunkThreads)
   lc::crc32c_chunks_body(data, n, scratch, scratch + kNoAllocCrcMaxChunks, out);
 }
 
-// The status alone tells the caller what went wrong (the conditions are listed
-// in the header); `what` names the failing step for a debugger.
+// Records the failing step (and the CUDA error, if any) as the calling
+// thread's lc_last_error() text, like the other entry points, and returns s.
 inline lc_status noalloc_fail(lc_status s, const char* what, cudaError_t e = cudaSuccess) {
-  (void)what;
-  (void)e;
+  std::string m(what);
+  if (e != cudaSuccess) m += std::string(": ") + cudaGetErrorString(e);
+  lc::set_last_error(m);
   return s;
 }
 

@@ -4,8 +4,11 @@
 stream and returns (device address, handle) at once; ``ready(handle)`` waits
 until that copy has finished, which the loop does before it submits the first
 job that reads the table (on another stream).  Dropping the handle (``free``)
-returns the memory to torch's caching allocator, whose stream-ordered reuse
-keeps a copy still in flight safe.
+returns the memory to torch's caching allocator, which may hand it out again
+for work on the uploader's stream at once: it knows nothing of the engine's
+streams.  So ``free(handle)`` may only be called after every job that read the
+table has completed (the served loop drops a table only after the waits of
+the jobs that read it); the copy itself is ordered on the uploader's stream.
 """
 from __future__ import annotations
 
