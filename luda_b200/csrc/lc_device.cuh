@@ -110,16 +110,18 @@ __device__ __forceinline__ uint64_t user_prefix(const uint8_t* k, uint32_t klen)
   return v;
 }
 
-// Compare two decoded entries by internal key.
-__device__ __forceinline__ int entry_cmp(const JobDev& J, uint32_t a, uint32_t b) {
-  uint64_t pa = J.e_pfx[a], pb = J.e_pfx[b];
-  if (pa != pb) return pa < pb ? -1 : 1;
-  return ikey_cmp(J.keys + J.e_koff[a], J.e_klen[a], J.keys + J.e_koff[b], J.e_klen[b]);
+// a before b in the merge (InternalKeyComparator order), given their user-key
+// prefixes: the prefixes decide unless equal.
+__device__ __forceinline__ bool entry_le(const JobDev& J, uint32_t a, uint64_t pa, uint32_t b,
+                                         uint64_t pb) {
+  if (pa != pb) return pa < pb;
+  return ikey_cmp(J.keys + J.e_koff[a], J.e_klen[a], J.keys + J.e_koff[b], J.e_klen[b]) <= 0;
 }
 
-// Same user key?
-__device__ __forceinline__ bool same_user_key(const JobDev& J, uint32_t a, uint32_t b) {
-  if (J.e_pfx[a] != J.e_pfx[b]) return false;
+// Same user key?  (pa, pb: their user-key prefixes)
+__device__ __forceinline__ bool same_user_key(const JobDev& J, uint32_t a, uint64_t pa, uint32_t b,
+                                              uint64_t pb) {
+  if (pa != pb) return false;
   uint32_t al = J.e_klen[a] - 8, bl = J.e_klen[b] - 8;
   if (al != bl) return false;
   const uint8_t* x = J.keys + J.e_koff[a];

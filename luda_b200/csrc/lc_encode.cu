@@ -63,9 +63,8 @@ __device__ __forceinline__ uint32_t bloom_bytes(uint64_t n, int bpk) {
 }
 
 __device__ __forceinline__ const uint8_t* kept_key(const JobDev& J, uint64_t k, uint32_t* len) {
-  const uint32_t id = J.k_ids[k];
-  *len = J.e_klen[id];
-  return J.keys + J.e_koff[id];
+  *len = J.k_klen[k];
+  return J.keys + J.k_koff[k];
 }
 
 // Entry sizes as a restart entry (k_a) and as a prefix-compressed entry
@@ -83,7 +82,7 @@ __global__ void k_sizes(const JobDev* __restrict__ jobs) {
     J.k_bstart[k] = 0;
     uint32_t kl;
     const uint8_t* key = kept_key(J, k, &kl);
-    const uint32_t vl = J.e_vlen[J.k_ids[k]];
+    const uint32_t vl = J.k_vlen[k];
     uint32_t shared = 0;
     if (k > 0) {
       uint32_t pl;
@@ -175,6 +174,35 @@ __global__ void k_chain_tables(const JobDev* __restrict__ jobs) {
   }
 }
 
+// Exits of groups of kChainGroup chunks for every entry point in the first
+// `window` survivors of the group's first chunk, by following the chunk
+// tables (one thread per entry point).  Only when the chunk tables do not fit
+// the resolving CTA's shared memory.
+__global__ void k_chain_groups(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;  // a failed job does no more work
+  const uint64_t n = J.ctr->n_kept;
+  const uint32_t C = J.chunk;
+  const uint32_t W = J.ctr->max_jump;
+  if (W > C || n == 0) return;
+  const uint64_t M = (n + C - 1) / C;
+  if (M * W <= J.chain_smem_words) return;  // resolved from the chunk tables directly
+  const uint64_t G = (M + kChainGroup - 1) / kChainGroup;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < G * W;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = x / W, i = x % W;
+    const uint64_t c0 = g * kChainGroup, c1 = min(M, c0 + kChainGroup);
+    uint64_t e = c0 * C + i;
+    for (uint64_t c = c0; c < c1 && e < n; c++) e = J.chunk_table[c * C + (e - c * C)];
+    J.group_table[g * C + i] = (uint32_t)e;
+  }
+}
+
+// Entry point of every chunk: the chain from survivor 0 through the chunk
+// tables.  Few chunks: one thread walks them over a shared-memory copy of the
+// tables.  Many: one thread walks the group tables (in shared memory when they
+// fit), then one thread per group walks its chunks from the group's entry
+// point.
 __global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
@@ -197,19 +225,45 @@ __global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
     return;
   }
   const uint64_t M = (n + C - 1) / C;
-  // the per-chunk tables fit in shared memory for most jobs: stage them
-  const bool staged = M * W <= J.chain_smem_words;
-  if (staged) {
+  if (M * W <= J.chain_smem_words) {
     for (uint64_t i = threadIdx.x; i < M * W; i += blockDim.x)
       s_tab[i] = J.chunk_table[(i / W) * C + (i % W)];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint64_t e = 0;
+    for (uint64_t c = 0; c < M; c++) {
+      J.chunk_entry[c] = (uint32_t)e;
+      if (e < n) e = s_tab[c * W + (e - c * C)];
+    }
+    return;
+  }
+  const uint64_t G = (M + kChainGroup - 1) / kChainGroup;
+  const bool staged = G * W + G <= J.chain_smem_words;
+  const bool entries_in_smem = G <= J.chain_smem_words;
+  uint32_t* s_entry = s_tab + (staged ? G * W : 0);  // group entry points
+  if (staged) {
+    for (uint64_t i = threadIdx.x; i < G * W; i += blockDim.x)
+      s_tab[i] = J.group_table[(i / W) * C + (i % W)];
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  uint64_t e = 0;
-  for (uint64_t c = 0; c < M; c++) {
-    J.chunk_entry[c] = (uint32_t)e;
-    const uint64_t c0 = c * C;
-    if (e < n) e = staged ? s_tab[c * W + (e - c0)] : J.chunk_table[c * C + (e - c0)];
+  if (threadIdx.x == 0) {
+    uint64_t e = 0;
+    for (uint64_t g = 0; g < G; g++) {
+      const uint64_t c0 = g * kChainGroup;
+      if (entries_in_smem) s_entry[g] = (uint32_t)e;
+      else J.chunk_entry[c0] = (uint32_t)e;
+      if (e < n)
+        e = staged ? s_tab[g * W + (e - c0 * C)] : J.group_table[g * C + (e - c0 * C)];
+    }
+  }
+  __syncthreads();
+  for (uint64_t g = threadIdx.x; g < G; g += blockDim.x) {
+    const uint64_t c0 = g * kChainGroup, c1 = min(M, c0 + kChainGroup);
+    uint64_t e = entries_in_smem ? s_entry[g] : J.chunk_entry[c0];
+    for (uint64_t c = c0; c < c1; c++) {
+      J.chunk_entry[c] = (uint32_t)e;
+      if (e < n) e = J.chunk_table[c * C + (e - c * C)];
+    }
   }
 }
 
@@ -545,10 +599,9 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab,
     const uint64_t ex = warp_excl<uint64_t>(size, &tot) + carry;
     carry += tot;
     if (valid) {
-      const uint32_t id = J.k_ids[k];
-      const uint32_t kl = J.e_klen[id], vl = J.e_vlen[id];
-      const uint8_t* key = J.keys + J.e_koff[id];
-      const uint8_t* val = J.in + J.e_voff[id];
+      const uint32_t kl = J.k_klen[k], vl = J.k_vlen[k];
+      const uint8_t* key = J.keys + J.k_koff[k];
+      const uint8_t* val = J.in + J.k_voff[k];
       const uint32_t sh = restart ? 0 : J.k_shared[k];
       uint8_t* p = dst + ex;
       p = put_varint(p, sh);
@@ -644,20 +697,20 @@ __global__ void __launch_bounds__(kEncWarps * 32, 5) k_encode_blocks(const JobDe
       uint32_t size = 0, hl = 0;
       if (j < n) {
         const uint64_t k = s + j;
-        const uint32_t id = J.k_ids[k];
-        const uint32_t kl = J.e_klen[id];
+        const uint32_t kl = J.k_klen[k];
         const uint32_t sh = (j % R == 0) ? 0 : J.k_shared[k];
-        const uint32_t kd = kl - sh, vl = J.e_vlen[id];
+        const uint32_t kd = kl - sh, vl = J.k_vlen[k];
+        const uint32_t koff = J.k_koff[k], voff = J.k_voff[k];
         hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
         size = hl + kd + vl;
-        W.ksrc[j] = J.e_koff[id] + sh;
-        W.vsrc[j] = J.e_voff[id];
+        W.ksrc[j] = koff + sh;
+        W.vsrc[j] = voff;
         W.kd[j] = kd;
         W.vl[j] = vl;
         W.sh[j] = sh;
         // start the source lines on their way to L1
-        prefetch_l1(keys + J.e_koff[id] + sh, kd);
-        prefetch_l1(in + J.e_voff[id], vl);
+        prefetch_l1(keys + koff + sh, kd);
+        prefetch_l1(in + voff, vl);
       }
       uint32_t tot;
       const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
@@ -1009,7 +1062,10 @@ void launch_chain(const Batch& bt, cudaStream_t st) {
   const size_t smem = (size_t)bt.chunk * sizeof(uint32_t);
   const unsigned g = (unsigned)std::min<uint64_t>(chunks, per_job(bt, 148 * 4));
   note_launch(), k_chain_tables<<<dim3(g, bt.B), 256, smem, st>>>(bt.d);
-  note_launch(), k_chain_resolve<<<dim3(1, bt.B), 256, (size_t)bt.chain_smem_words * 4, st>>>(bt.d);
+  if (chunks > kChainGroup)
+    note_launch(), k_chain_groups<<<dim3(grid_x(chunks / kChainGroup * bt.chunk, 256, 148 * 4), bt.B),
+                                    256, 0, st>>>(bt.d);
+  note_launch(), k_chain_resolve<<<dim3(1, bt.B), 1024, (size_t)bt.chain_smem_words * 4, st>>>(bt.d);
   note_launch(), k_chain_mark<<<dim3(g, bt.B), 128, smem, st>>>(bt.d);
 }
 void launch_block_list(const Batch& bt, cudaStream_t st) {

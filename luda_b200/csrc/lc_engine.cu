@@ -492,7 +492,7 @@ uint32_t bloom_k(int bpk) {
   return (uint32_t)k;
 }
 
-// Survivors (k_ids, counters n_kept / n_triggers set) -> encoded files.
+// Survivors (k_koff..k_vlen, counters n_kept / n_triggers set) -> encoded files.
 void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   memset(&J, 0, sizeof(J));
   J.block_size = j->opt.block_size;
@@ -609,15 +609,25 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
     J.e_voff = A.get<uint32_t>(N);
     J.e_vlen = A.get<uint32_t>(N);
     J.e_pfx = A.get<uint64_t>(N);
+    J.e_tag = A.get<uint64_t>(N);
     J.m_ids = A.get<uint32_t>(N);
     J.m_tmp = A.get<uint32_t>(N);
+    J.m_pfx = A.get<uint64_t>(N);
+    J.m_pfx_tmp = A.get<uint64_t>(N);
+    J.m_tag = A.get<uint64_t>(N);
+    J.m_tag_tmp = A.get<uint64_t>(N);
+    J.cap_merge_tiles = (uint32_t)merge_tile_capacity(N, J.n_runs);
+    J.m_split = A.get<uint32_t>(J.cap_merge_tiles);
     J.keep = A.get<uint8_t>(N);
     J.gp_idx = A.get<uint32_t>(J.n_gp ? N : 1);
     J.kept_pos = A.get<uint32_t>(N + 1);
     J.gp_first = A.get<uint32_t>(J.n_gp + 1);
-    J.k_ids = A.get<uint32_t>(N);
     J.k_forced = A.get<uint8_t>(N + 1);
   }
+  J.k_koff = A.get<uint32_t>(N);
+  J.k_klen = A.get<uint32_t>(N);
+  J.k_voff = A.get<uint32_t>(N);
+  J.k_vlen = A.get<uint32_t>(N);
   J.cap_triggers = J.n_gp + 1;
   J.triggers = A.get<uint32_t>(J.cap_triggers);
   J.k_a = A.get<uint32_t>(N);
@@ -629,6 +639,7 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   const uint64_t chunks = (N + J.chunk - 1) / J.chunk + 1;
   J.chunk_table = A.get<uint32_t>(chunks * J.chunk);
   J.chunk_entry = A.get<uint32_t>(chunks);
+  J.group_table = A.get<uint32_t>((chunks / kChainGroup + 1) * J.chunk);
   J.b_first = A.get<uint32_t>(N + 1);
   J.b_size = A.get<uint32_t>(N);
   J.tmp32 = A.get<uint32_t>(N);
@@ -765,11 +776,11 @@ struct lc_slot {
       return 0;
     }
     char key[256];
-    snprintf(key, sizeof(key), "%d|%d|%u|%u|%u|%u|%u|%llu|%llu|%u|%u|%u|%u|%u", (int)T.on,
+    snprintf(key, sizeof(key), "%d|%d|%u|%u|%u|%u|%u|%llu|%llu|%u|%u|%u|%u|%u|%u|%d", (int)T.on,
              (int)decode_merge, bt.B, bt.max_tables, bt.max_gp, bt.max_cap_triggers,
              bt.max_cap_files, (unsigned long long)bt.max_blocks_in,
              (unsigned long long)bt.max_entries, bt.merge_rounds, bt.chunk, bt.ctas_per_job,
-             bt.merge_items, bt.merge_threads);
+             bt.merge_items, bt.merge_threads, bt.max_runs, (int)bt.exact);
     auto it = graphs.find(key);
     bool fresh = false;
     if (it == graphs.end()) {
@@ -899,7 +910,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     std::vector<uint64_t> in_base(B, 0);
     std::vector<bool> zero_copy(B, false);
     struct Offs {
-      uint64_t td, gpk, gpo, gpp, lb, bk, bso, blo, bsl, bll;
+      uint64_t td, gpk, gpo, gpp, gpu, lb, bk, bso, blo, bsl, bll;
     };
     std::vector<Offs> offs(B);
     for (uint32_t i = 0; i < B; i++) {
@@ -958,12 +969,19 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       r.cap_blk = cap_blk;
       // grandparents: largest keys, offsets, size prefix
       J.n_gp = (uint32_t)j->gp_largest.size();
-      std::vector<uint64_t> gpo(J.n_gp + 1, 0), gpp(J.n_gp + 1, 0);
+      std::vector<uint64_t> gpo(J.n_gp + 1, 0), gpp(J.n_gp + 1, 0), gpu(J.n_gp + 1, 0);
       std::string gpk;
       for (uint32_t g = 0; g < J.n_gp; g++) {
-        gpk += j->gp_largest[g];
+        const std::string& k = j->gp_largest[g];
+        gpk += k;
         gpo[g + 1] = gpk.size();
         gpp[g + 1] = gpp[g] + j->gp_size[g];
+        // first 8 user-key bytes, big endian, zero padded (as the decoded
+        // entries' prefixes)
+        uint64_t v = 0;
+        for (size_t b = 0; b < 8; b++)
+          v = (v << 8) | (b + 8 < k.size() ? (uint8_t)k[b] : 0u);
+        gpu[g] = v;
       }
       // base-level files, grouped by level
       const uint32_t nb = (uint32_t)j->base_level.size();
@@ -987,6 +1005,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       o.gpk = S.put(gpk.data(), gpk.size());
       o.gpo = S.put(gpo.data(), gpo.size());
       o.gpp = S.put(gpp.data(), gpp.size());
+      o.gpu = S.put(gpu.data(), gpu.size());
       o.lb = S.put(lb.data(), lb.size());
       o.bk = S.put(bk.data(), bk.size());
       o.bso = S.put(so.data(), nb);
@@ -1011,6 +1030,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     bt.ctas_per_job = tun.ctas_per_job;
     bt.merge_items = tun.merge_items;
     bt.merge_threads = tun.merge_threads;
+    bt.exact = exact;
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       JobDev& J = r.J;
@@ -1029,6 +1049,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       J.gp_keys = d_stage + o.gpk;
       J.gp_key_off = (const uint64_t*)(d_stage + o.gpo);
       J.gp_prefix = (const uint64_t*)(d_stage + o.gpp);
+      J.gp_upfx = (const uint64_t*)(d_stage + o.gpu);
       J.base_level_begin = (const uint32_t*)(d_stage + o.lb);
       J.base_keys = d_stage + o.bk;
       J.base_small_off = (const uint64_t*)(d_stage + o.bso);
@@ -1145,6 +1166,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     bt.max_cap_triggers = (uint32_t)pow2_at_least(bt.max_cap_triggers);
     bt.max_gp = bt.max_gp ? (uint32_t)pow2_at_least(bt.max_gp + 1) - 1 : 0;
     bt.merge_rounds = ceil_log2(max_runs);
+    bt.max_runs = max_runs;
     // every job's per-file results in one device region, read back with one
     // copy: [files | key offsets | keys] per job
     std::vector<size_t> res_off(B + 1, 0);
@@ -1369,7 +1391,7 @@ void run_build(lc_job* j, lc_slot& slot) {
     J.e_voff = A.get<uint32_t>(N);
     J.e_vlen = A.get<uint32_t>(N);
     J.e_pfx = A.get<uint64_t>(N);
-    J.k_ids = A.get<uint32_t>(N);
+    J.e_tag = A.get<uint64_t>(N);
     J.k_forced = A.get<uint8_t>(N + 1);
     CK(cudaMemsetAsync(J.k_forced, 0, N + 1, st));
     J.kept_pos = A.get<uint32_t>(N + 1);
@@ -1457,7 +1479,7 @@ void run_build(lc_job* j, lc_slot& slot) {
 // (the at-size workloads have 67-250 bytes per entry) and the worker trues
 // the charge up to the batch's real allocation once the counts are known.
 constexpr uint64_t kEstEntryBytes = 40;
-constexpr uint64_t kEntryArrayBytes = 160;  // per-entry arrays of alloc_tail, rounded up
+constexpr uint64_t kEntryArrayBytes = 224;  // per-entry arrays of alloc_tail, rounded up
 uint64_t estimate_bytes(const lc_job* j) {
   uint64_t in = 0;
   for (auto& t : j->tables) in += round16(t.size);
@@ -1691,6 +1713,7 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     decode_kernel_attributes();
     encode_kernel_attributes();
+    merge_kernel_attributes();
     CK(cudaGetLastError());
     std::vector<uint32_t> t;
     host_crc_xpow(t);

@@ -101,6 +101,7 @@ struct JobDev {
   const uint8_t* gp_keys;
   const uint64_t* gp_key_off;   // n_gp + 1
   const uint64_t* gp_prefix;    // n_gp + 1, prefix sums of file sizes
+  const uint64_t* gp_upfx;      // n_gp: first 8 user-key bytes of each largest key, big endian
   // base-level files: user-key ranges per level >= L+2
   uint32_t n_base_levels;
   const uint32_t* base_level_begin;  // n_base_levels + 1, into the file list
@@ -132,11 +133,18 @@ struct JobDev {
   uint32_t* e_voff;
   uint32_t* e_vlen;
   uint64_t* e_pfx;
+  uint64_t* e_tag;           // the key's last 8 bytes: (sequence << 8) | type
   uint64_t cap_entries;
 
   // merge
   uint32_t* m_ids;           // merged order (holds the result after the last round)
   uint32_t* m_tmp;           // the other buffer of the ping-pong
+  uint64_t* m_pfx;           // e_pfx of m_ids, in merged order (result after the last round)
+  uint64_t* m_pfx_tmp;       // the other buffer of the ping-pong
+  uint64_t* m_tag;           // e_tag of m_ids, in merged order (result after the last round)
+  uint64_t* m_tag_tmp;       // the other buffer of the ping-pong
+  uint32_t* m_split;         // per merge tile: first-group elements before the tile
+  uint32_t cap_merge_tiles;  // capacity of m_split
   uint8_t* keep;             // per merged position
   uint32_t* gp_idx;          // per merged position: grandparents passed
   uint32_t* kept_pos;        // exclusive scan of keep (n+1)
@@ -144,7 +152,10 @@ struct JobDev {
   uint32_t cap_triggers;
 
   // kept entries
-  uint32_t* k_ids;
+  uint32_t* k_koff;          // survivors, in output order: key offset in the arena,
+  uint32_t* k_klen;          // key length,
+  uint32_t* k_voff;          // value offset in `in`,
+  uint32_t* k_vlen;          // value length (gathered once from the entry arrays)
   uint32_t* k_a;             // size as a restart entry
   uint32_t* k_b;             // size as a prefix-compressed entry
   uint32_t* k_shared;        // shared prefix with the previous kept key
@@ -157,6 +168,7 @@ struct JobDev {
   uint32_t chunk;            // entries per chunk
   uint32_t* chunk_table;     // per chunk: exit for each window entry
   uint32_t* chunk_entry;     // per chunk: resolved entry point
+  uint32_t* group_table;     // per group of kChainGroup chunks: exit for each window entry
   uint32_t window;           // table width
   uint32_t chain_smem_words; // shared-memory words for staging the chunk tables
   uint32_t reserve_keys;     // 1: decode reserves key-arena space per block (single

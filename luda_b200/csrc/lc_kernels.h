@@ -28,6 +28,17 @@ uint32_t launches_on_this_thread();
 // stream capture.
 void decode_kernel_attributes();
 void encode_kernel_attributes();
+void merge_kernel_attributes();
+
+// Chunks per group in the block-chain resolution.
+constexpr uint32_t kChainGroup = 64;
+
+// Largest merge tile (threads x items) and the shared memory the tile takes
+// per position.
+constexpr uint32_t kMergeMaxTile = 4096;
+constexpr uint32_t kMergeSmemPerPos = 28;
+// Entries of m_split a job needs for `entries` entries in `runs` children.
+uint64_t merge_tile_capacity(uint64_t entries, uint32_t runs);
 
 struct Batch {
   const JobDev* d = nullptr;  // device array of B job descriptors
@@ -36,9 +47,11 @@ struct Batch {
   uint32_t max_tables = 0, max_gp = 0, max_cap_triggers = 0, max_cap_files = 0;
   uint64_t max_blocks_in = 0, max_entries = 0;
   uint32_t merge_rounds = 0;
+  uint32_t max_runs = 1;
   uint32_t chunk = 4096;
   uint32_t chain_smem_words = 11 * 1024;
   bool any_verify = false;  // some job checks its input blocks' CRCs
+  bool exact = false;       // rerun with exact counting (blk_key_base from the counting walk)
   // tunables (chosen by the autotuner in lc_engine.cu)
   uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
   uint32_t merge_items = 8;   // outputs per thread in a merge round

@@ -2,9 +2,14 @@
 //
 // * Merge: the reference merges its children with MergingIterator
 //   (table/merger.cc:148, linear FindSmallest; on equal keys the earlier child
-//   wins).  Here the children are merged pairwise in rounds with merge path:
-//   each thread finds its output diagonal by binary search and merges a short
-//   stretch.  Ties go to the left (earlier) group, which keeps child order.
+//   wins).  Here the children are merged pairwise in rounds with merge path,
+//   in tiles: one thread per tile finds the tile's split by binary search,
+//   then a CTA stages the tile's two stretches (entry ids and their 8-byte
+//   user-key prefixes) in shared memory, merges them there (each thread its
+//   own diagonal) and writes ids, prefixes and tags back coalesced, so that a
+//   round reads and writes 20 bytes per entry and key bytes are read only for
+//   equal prefixes.  Ties go to the left (earlier) group, which keeps child
+//   order.  The drop rule then reads prefixes and tags in merged order.
 // * Drop rule (db/db_impl.cc:1113-1147): an entry is hidden when the previous
 //   entry has the same user key and a sequence number <= smallest_snapshot;
 //   a deletion marker is dropped when its sequence number is <=
@@ -28,64 +33,168 @@ namespace lc {
 
 namespace {
 
-__global__ void k_iota(const JobDev* __restrict__ jobs, uint32_t rounds) {
+// A single merge child (no round): the merged order is the input order.
+__global__ void k_merge_single(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   if (J.ctr->error) return;  // a failed job does no more work
-  uint32_t* ids = (rounds & 1) ? J.m_tmp : J.m_ids;  // the buffer round 0 reads
   const uint64_t n = J.ctr->n_entries_in;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    ids[i] = (uint32_t)i;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    J.m_ids[i] = (uint32_t)i;
+    J.m_pfx[i] = J.e_pfx[i];
+    J.m_tag[i] = J.e_tag[i];
+  }
 }
 
-// Round `r` of `rounds`: groups of width = 2^r merge children; pairs (2p,
-// 2p+1) merge.  Jobs with fewer children copy through, so every job of a
-// batch ends with its merged order in m_ids.
-__global__ void k_merge_round(const JobDev* __restrict__ jobs, uint32_t r, uint32_t rounds,
-                              uint32_t items) {
+// Round r of `rounds` merges groups of 2^r children pairwise: the output of
+// pair p (groups 2p and 2p+1) is cut into tiles of `tile` positions.  Round 0
+// reads the decoded entries in input order (ids are positions, prefixes and
+// tags are e_pfx / e_tag); later rounds read the previous round's arrays.
+// Jobs with fewer children copy through, so that every job of a batch ends
+// with its merged order in m_ids / m_pfx / m_tag.
+struct MergeRound {
+  const uint32_t* src_ids;  // nullptr in round 0
+  const uint64_t* src_pfx;
+  const uint64_t* src_tag;
+  uint32_t* dst_ids;
+  uint64_t* dst_pfx;
+  uint64_t* dst_tag;
+};
+
+__device__ __forceinline__ MergeRound merge_round(const JobDev& J, uint32_t r, uint32_t rounds) {
+  const bool odd = ((rounds - r) & 1) != 0;
+  MergeRound m;
+  m.src_ids = r == 0 ? nullptr : (odd ? J.m_tmp : J.m_ids);
+  m.src_pfx = r == 0 ? J.e_pfx : (odd ? J.m_pfx_tmp : J.m_pfx);
+  m.src_tag = r == 0 ? J.e_tag : (odd ? J.m_tag_tmp : J.m_tag);
+  m.dst_ids = odd ? J.m_ids : J.m_tmp;
+  m.dst_pfx = odd ? J.m_pfx : J.m_pfx_tmp;
+  m.dst_tag = odd ? J.m_tag : J.m_tag_tmp;
+  return m;
+}
+
+// Pair and tile of the job's g-th merge tile in round r; false past the last.
+struct MergeTile {
+  uint64_t a0, na, nb;  // the pair's first group [a0, a0 + na), second [a0 + na, + nb)
+  uint64_t d0, d1;      // the tile's output positions within the pair
+  bool last;            // last tile of its pair
+};
+
+__device__ __forceinline__ bool merge_tile(const JobDev& J, uint32_t r, uint64_t g, uint32_t tile,
+                                           MergeTile* t) {
+  const uint32_t width = 1u << r;
+  uint64_t acc = 0;
+  for (uint32_t r0 = 0; r0 < J.n_runs; r0 += 2 * width) {
+    const uint32_t r1 = min(r0 + width, J.n_runs), r2 = min(r0 + 2 * width, J.n_runs);
+    const uint64_t a0 = J.run_entry_begin[r0], b0 = J.run_entry_begin[r1],
+                   b1 = J.run_entry_begin[r2];
+    const uint64_t len = b1 - a0, tiles = (len + tile - 1) / tile;
+    if (g < acc + tiles) {
+      const uint64_t k = g - acc;
+      t->a0 = a0;
+      t->na = b0 - a0;
+      t->nb = b1 - b0;
+      t->d0 = k * tile;
+      t->d1 = min(len, t->d0 + tile);
+      t->last = k + 1 == tiles;
+      return true;
+    }
+    acc += tiles;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t src_id(const MergeRound& m, uint64_t i) {
+  return m.src_ids ? m.src_ids[i] : (uint32_t)i;
+}
+
+// m_split[g]: elements of the pair's first group before tile g's first
+// diagonal (merge path: the first group wins ties, which keeps the children's
+// order for equal internal keys, as MergingIterator does).  One thread per
+// tile.
+__global__ void k_merge_partition(const JobDev* __restrict__ jobs, uint32_t r, uint32_t rounds,
+                                  uint32_t tile) {
   const JobDev& J = jobs[blockIdx.y];
   if (J.ctr->error) return;  // a failed job does no more work
-  const uint32_t* __restrict__ src = ((rounds - r) & 1) ? J.m_tmp : J.m_ids;
-  uint32_t* __restrict__ dst = ((rounds - r) & 1) ? J.m_ids : J.m_tmp;
-  const uint32_t width = 1u << r;
-  const uint64_t n = J.run_entry_begin[J.n_runs];
-  for (uint64_t o0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * items; o0 < n;
-       o0 += (uint64_t)gridDim.x * blockDim.x * items) {
-    const uint64_t o1 = min(n, o0 + items);
-    uint64_t o = o0;
-    while (o < o1) {
-      // find the pair that owns output position o
-      const uint32_t pair_runs = 2 * width;
-      uint32_t r0 = 0;
-      while (true) {
-        const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
-        if (o < J.run_entry_begin[r2]) break;
-        r0 = r2;
-      }
-      const uint32_t r1 = min(r0 + width, J.n_runs);
-      const uint32_t r2 = min(r0 + pair_runs, J.n_runs);
-      const uint64_t a0 = J.run_entry_begin[r0], b0 = J.run_entry_begin[r1],
-                     b1 = J.run_entry_begin[r2];
-      const uint64_t na = b0 - a0, nb = b1 - b0;
-      const uint64_t stop = min(o1, b1);
-      if (nb == 0) {
-        for (; o < stop; o++) dst[o] = src[o];
-        continue;
-      }
-      const uint32_t* A = src + a0;
-      const uint32_t* B = src + b0;
-      const uint64_t d = o - a0;
-      uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+  const MergeRound m = merge_round(J, r, rounds);
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < J.cap_merge_tiles;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    MergeTile t;
+    if (!merge_tile(J, r, g, tile, &t)) break;
+    const uint64_t d = t.d0, a = t.a0, b = t.a0 + t.na;
+    uint64_t lo = d > t.nb ? d - t.nb : 0, hi = d < t.na ? d : t.na;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      const uint64_t ia = a + mid, ib = b + (d - 1 - mid);
+      if (entry_le(J, src_id(m, ia), m.src_pfx[ia], src_id(m, ib), m.src_pfx[ib])) lo = mid + 1;
+      else hi = mid;
+    }
+    J.m_split[g] = (uint32_t)lo;
+  }
+}
+
+// One tile per CTA step: the tile's stretches of both groups (ids and
+// prefixes) are loaded into shared memory with coalesced reads, every thread
+// finds its own diagonal there and merges `items` outputs, and the tile is
+// written back with coalesced stores; the tags follow by source position
+// (two ascending streams).  Only equal prefixes read key bytes.
+__global__ void __launch_bounds__(1024) k_merge_tile(const JobDev* __restrict__ jobs, uint32_t r,
+                                                     uint32_t rounds, uint32_t items) {
+  const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
+  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  __syncthreads();
+  if (s_failed) return;
+  const uint32_t tile = blockDim.x * items;
+  extern __shared__ __align__(16) uint8_t merge_smem[];
+  uint64_t* in_pfx = reinterpret_cast<uint64_t*>(merge_smem);
+  uint64_t* out_pfx = in_pfx + tile;
+  uint32_t* in_ids = reinterpret_cast<uint32_t*>(out_pfx + tile);
+  uint32_t* out_ids = in_ids + tile;
+  uint32_t* out_src = out_ids + tile;  // source position (in the tile) of each output
+  const MergeRound m = merge_round(J, r, rounds);
+  for (uint64_t g = blockIdx.x; g < J.cap_merge_tiles; g += gridDim.x) {
+    MergeTile t;
+    if (!merge_tile(J, r, g, tile, &t)) break;
+    const uint64_t i0 = J.m_split[g];
+    const uint64_t i1 = t.last ? t.na : J.m_split[g + 1];
+    const uint64_t j0 = t.d0 - i0, j1 = t.d1 - i1;
+    const uint32_t na = (uint32_t)(i1 - i0), nb = (uint32_t)(j1 - j0), len = na + nb;
+    __syncthreads();  // the previous tile's stores have read the buffers
+    for (uint32_t x = threadIdx.x; x < len; x += blockDim.x) {
+      const uint64_t i = x < na ? t.a0 + i0 + x : t.a0 + t.na + j0 + (x - na);
+      in_ids[x] = src_id(m, i);
+      in_pfx[x] = m.src_pfx[i];
+    }
+    __syncthreads();
+    const uint32_t k = threadIdx.x * items;
+    if (k < len) {
+      // this thread's diagonal within the tile
+      uint32_t lo = k > nb ? k - nb : 0, hi = k < na ? k : na;
       while (lo < hi) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (entry_cmp(J, A[mid], B[d - 1 - mid]) <= 0) lo = mid + 1;
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t jb = na + (k - 1 - mid);
+        if (entry_le(J, in_ids[mid], in_pfx[mid], in_ids[jb], in_pfx[jb])) lo = mid + 1;
         else hi = mid;
       }
-      uint64_t i = lo, j = d - lo;
-      for (; o < stop; o++) {
-        const bool take_a = i < na && (j >= nb || entry_cmp(J, A[i], B[j]) <= 0);
-        dst[o] = take_a ? A[i++] : B[j++];
+      uint32_t i = lo, j = k - lo;
+      const uint32_t stop = min(len, k + items);
+      for (uint32_t o = k; o < stop; o++) {
+        const bool take_a =
+            i < na && (j >= nb || entry_le(J, in_ids[i], in_pfx[i], in_ids[na + j], in_pfx[na + j]));
+        const uint32_t x = take_a ? i++ : na + j++;
+        out_ids[o] = in_ids[x];
+        out_pfx[o] = in_pfx[x];
+        out_src[o] = x;
       }
+    }
+    __syncthreads();
+    const uint64_t o0 = t.a0 + t.d0;
+    for (uint32_t x = threadIdx.x; x < len; x += blockDim.x) {
+      m.dst_ids[o0 + x] = out_ids[x];
+      m.dst_pfx[o0 + x] = out_pfx[x];
+      const uint32_t y = out_src[x];
+      m.dst_tag[o0 + x] = m.src_tag[y < na ? t.a0 + i0 + y : t.a0 + t.na + j0 + (y - na)];
     }
   }
 }
@@ -110,11 +219,11 @@ __device__ __forceinline__ bool is_base_level(const JobDev& J, const uint8_t* uk
 }
 
 __device__ __forceinline__ void drop_one(const JobDev& J, const uint32_t* __restrict__ ids,
-                                         uint64_t p) {
+                                         const uint64_t* __restrict__ pfx,
+                                         const uint64_t* __restrict__ tags, uint64_t p) {
   const uint32_t id = ids[p];
-  const uint8_t* key = J.keys + J.e_koff[id];
-  const uint32_t klen = J.e_klen[id];
-  const uint64_t tag = ld_le64(key + klen - 8);
+  const uint64_t upfx = pfx[p];
+  const uint64_t tag = tags[p];
   const uint32_t type = (uint32_t)(tag & 0xff);
   const uint64_t seq = tag >> 8;
   bool drop = false;
@@ -122,29 +231,36 @@ __device__ __forceinline__ void drop_one(const JobDev& J, const uint32_t* __rest
     bool first = true;
     uint64_t pseq = 0;
     if (p > 0) {
-      const uint32_t pid = ids[p - 1];
-      const uint8_t* pkey = J.keys + J.e_koff[pid];
-      const uint64_t ptag = ld_le64(pkey + J.e_klen[pid] - 8);
-      if ((ptag & 0xff) <= 1 && same_user_key(J, pid, id)) {
+      const uint64_t ptag = tags[p - 1];
+      if ((ptag & 0xff) <= 1 && same_user_key(J, ids[p - 1], pfx[p - 1], id, upfx)) {
         first = false;
         pseq = ptag >> 8;
       }
     }
     if (!first && pseq <= J.smallest_snapshot) {
       drop = true;
-    } else if (type == 0 && seq <= J.smallest_snapshot && is_base_level(J, key, klen - 8)) {
+    } else if (type == 0 && seq <= J.smallest_snapshot &&
+               is_base_level(J, J.keys + J.e_koff[id], J.e_klen[id] - 8)) {
       drop = true;
     }
   }
   J.keep[p] = drop ? 0 : 1;
   if (J.n_gp) {
-    // grandparents passed: count of g with key > largest[g]
+    // grandparents passed: count of g with key > largest[g] (internal-key
+    // order); the user-key prefixes decide unless equal
     uint32_t lo = 0, hi = J.n_gp;
     while (lo < hi) {
-      uint32_t mid = (lo + hi) >> 1;
-      const uint64_t go = J.gp_key_off[mid];
-      const uint32_t gl = (uint32_t)(J.gp_key_off[mid + 1] - go);
-      if (ikey_cmp(key, klen, J.gp_keys + go, gl) > 0) lo = mid + 1;
+      const uint32_t mid = (lo + hi) >> 1;
+      const uint64_t gp = J.gp_upfx[mid];
+      bool after;
+      if (gp != upfx) {
+        after = upfx > gp;
+      } else {
+        const uint64_t go = J.gp_key_off[mid];
+        const uint32_t gl = (uint32_t)(J.gp_key_off[mid + 1] - go);
+        after = ikey_cmp(J.keys + J.e_koff[id], J.e_klen[id], J.gp_keys + go, gl) > 0;
+      }
+      if (after) lo = mid + 1;
       else hi = mid;
     }
     J.gp_idx[p] = lo;
@@ -157,7 +273,7 @@ __global__ void k_drop(const JobDev* __restrict__ jobs) {
   const uint64_t n = J.ctr->n_entries_in;
   for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (uint64_t)gridDim.x * blockDim.x)
-    drop_one(J, J.m_ids, p);
+    drop_one(J, J.m_ids, J.m_pfx, J.m_tag, p);
 }
 
 // gp_first[g] = first merged position whose grandparent count reaches g
@@ -241,7 +357,11 @@ __global__ void k_kept_compact(const JobDev* __restrict__ jobs) {
        p += (uint64_t)gridDim.x * blockDim.x) {
     if (J.keep[p]) {
       const uint32_t k = J.kept_pos[p];
-      J.k_ids[k] = ids[p];
+      const uint32_t id = ids[p];
+      J.k_koff[k] = J.e_koff[id];
+      J.k_klen[k] = J.e_klen[id];
+      J.k_voff[k] = J.e_voff[id];
+      J.k_vlen[k] = J.e_vlen[id];
       J.k_forced[k] = 0;
     }
   }
@@ -266,14 +386,42 @@ static unsigned flat_ctas(const Batch& bt, uint64_t items, unsigned per) {
   return grid_x(items, per, cap);
 }
 
+// Merge tile (threads x items, at most kMergeMaxTile) and the shared memory
+// it takes: ids and prefixes of the tile's input and output and each output's
+// source position.
+static uint32_t merge_items_of(const Batch& bt) {
+  uint32_t items = std::max<uint32_t>(1, bt.merge_items);
+  while ((uint64_t)bt.merge_threads * items > kMergeMaxTile && items > 1) items >>= 1;
+  return items;
+}
+
+void merge_kernel_attributes() {
+  cudaFuncSetAttribute(k_merge_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(kMergeSmemPerPos * kMergeMaxTile));
+}
+
+uint64_t merge_tile_capacity(uint64_t entries, uint32_t runs) {
+  // tiles of at least 64 positions, one partial tile per pair
+  return entries / 64 + runs + 2;
+}
+
 void launch_merge(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_iota<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(
-      bt.d, bt.merge_rounds);
-  const uint32_t items = bt.merge_items;
+  if (bt.merge_rounds == 0) {
+    note_launch(), k_merge_single<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(
+        bt.d);
+    return;
+  }
+  const uint32_t items = merge_items_of(bt);
   const uint32_t threads = bt.merge_threads;
-  for (uint32_t r = 0; r < bt.merge_rounds; r++)
-    note_launch(), k_merge_round<<<dim3(flat_ctas(bt, (bt.max_entries + items - 1) / items, threads),
-                                        bt.B), threads, 0, st>>>(bt.d, r, bt.merge_rounds, items);
+  const uint32_t tile = threads * items;
+  const uint64_t tiles = bt.max_entries / tile + bt.max_runs + 1;
+  for (uint32_t r = 0; r < bt.merge_rounds; r++) {
+    note_launch(), k_merge_partition<<<dim3(grid_x(tiles, 128, 148 * 16), bt.B), 128, 0, st>>>(
+        bt.d, r, bt.merge_rounds, tile);
+    note_launch(), k_merge_tile<<<dim3(flat_ctas(bt, tiles, 1), bt.B), threads,
+                                  kMergeSmemPerPos * (size_t)tile, st>>>(bt.d, r, bt.merge_rounds,
+                                                                         items);
+  }
 }
 
 void launch_drop(const Batch& bt, cudaStream_t st) {
