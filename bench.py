@@ -408,7 +408,7 @@ def job_leg(name, args, eng, eng_ph, flush, torch, steps, warmup, clocks=None, p
         flush.zero_()
         torch.cuda.synchronize()
         r = eng_ph.run(prep_ph)
-        phases.append(r.phases)
+        phases.append(r.phase_ms)
         ph_ms.append(r.device_ms)
         stats_r = r
         r.release()
@@ -468,7 +468,7 @@ def job_leg(name, args, eng, eng_ph, flush, torch, steps, warmup, clocks=None, p
             h2d.append(a.elapsed_time(b))
             dh.append(b.elapsed_time(c))
         r = eng_ph.run(eng_ph.prepare(job))
-        up_ms, down_ms = r.phases["upload"], r.phases["download"]
+        up_ms, down_ms = r.phase_ms["upload"], r.phase_ms["download"]
         r.release()
         link = {"h2d_gbs": src.numel() / (min(h2d) / 1e3) / 1e9,
                 "d2h_gbs": d2h / (min(dh) / 1e3) / 1e9,
@@ -713,7 +713,8 @@ class RefLoopEngine:
     def __init__(self):
         self.pending = []
 
-    def prepare(self, job, device_tables=None, outputs_on_device=0):
+    def prepare(self, job, device_tables=None, outputs_on_device=0, keep_decoded=False,
+                decoded=None):
         # the loop drops its references to the input buffers after this call
         assert device_tables is None
         return job, [(f, f.data) for f in job.input_tables()]

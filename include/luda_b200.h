@@ -39,6 +39,10 @@ typedef enum {
 
 typedef struct lc_engine lc_engine;
 typedef struct lc_job lc_job;
+/* The decoded entries of one output table, kept in device memory by the job
+ * that wrote the table (lc_job_desc.keep_decoded) and valid until that job is
+ * released.  Opaque. */
+typedef struct lc_decoded lc_decoded;
 
 typedef struct {
   int32_t device;               /* CUDA device ordinal */
@@ -116,6 +120,20 @@ typedef struct {
                                (db/version_set.cc:1239; the check is table/format.cc:
                                86-95, switched off in the reference build).  0: no
                                check, as the reference. */
+  int32_t keep_decoded;     /* 1 (with outputs_on_device 1 or 2): also keep every output
+                               table's decoded entries in device memory
+                               (lc_job_out.decoded), so that a later job reading that
+                               table from device memory can skip parsing and decoding
+                               it.  LUDA's nearest counterpart keeps a level-0 flush's
+                               decoded entries in host memory for the compaction that
+                               reads that file next (cuda/cuda_common.h:253-255, 339-355;
+                               db/db_impl.cc:146-149). */
+  const lc_decoded* const* decoded; /* NULL, or n_tables entries: for table i, the
+                               decoded form of that same table (an lc_job_out.decoded
+                               entry of the job that wrote it; NULL where none).  The
+                               table must then be read from device memory
+                               (inputs_on_device) and have the size the decoded form
+                               was made for.  The output is byte-identical either way. */
 } lc_job_desc;
 
 /* Output of one compaction: what DoCompactionWork records in
@@ -153,6 +171,10 @@ typedef struct {
                                  kernel_launches are the batch's) */
   double queue_ms;            /* lc_job_submit -> start of its batch (0 for synchronous
                                  calls) */
+  const lc_decoded* const* decoded; /* keep_decoded: n_files entries, the decoded entries
+                                 of each output table (valid until lc_job_release);
+                                 else NULL */
+  uint32_t decoded_inputs;    /* input tables read from their decoded form */
 } lc_job_out;
 
 /* Engine lifetime.  An engine owns one CUDA device, its streams, slab caches

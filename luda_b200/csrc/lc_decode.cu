@@ -85,6 +85,11 @@ __global__ void k_table_index_count(const JobDev* __restrict__ jobs) {
   const uint32_t t = blockIdx.x;
   if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
+  if (T.cached) {  // read from its decoded form: pseudo blocks of kDecRunBlock entries
+    if (threadIdx.x == 0)
+      J.tbl_nblocks[t] = (uint32_t)((J.dec_runs[t].n + kDecRunBlock - 1) / kDecRunBlock);
+    return;
+  }
   const uint8_t* base = J.in + T.off;
   __shared__ uint64_t s_ioff, s_isize;
   __shared__ uint32_t s_nr, s_ok;
@@ -126,6 +131,15 @@ __global__ void k_table_index_entries(const JobDev* __restrict__ jobs) {
   const uint32_t t = blockIdx.x;
   if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
+  if (T.cached) {
+    const uint64_t out_base = J.tbl_block_base[t], out_end = J.tbl_block_base[t + 1];
+    for (uint64_t o = out_base + threadIdx.x; o < out_end && o < J.cap_blocks_in; o += blockDim.x) {
+      J.blk_off[o] = ((uint64_t)t << 32) | ((o - out_base) * kDecRunBlock);
+      J.blk_size[o] = kPseudoBlock;
+      J.blk_run[o] = T.run;
+    }
+    return;
+  }
   const uint8_t* base = J.in + T.off;
   uint64_t io, is;
   if (!parse_footer(base, T.size, &io, &is)) return;  // error already recorded
@@ -195,6 +209,67 @@ __global__ void k_table_index_entries(const JobDev* __restrict__ jobs) {
       if (!ok) set_error(J.ctr, kErrBadIndex, t);
     }
     __syncthreads();
+  }
+}
+
+// A pseudo block: entries [*j0, *j1) of the decoded run of table *t.
+__device__ __forceinline__ const DecRun& pseudo_block(const JobDev& J, uint64_t b, uint32_t* t,
+                                                      uint64_t* j0, uint64_t* j1) {
+  const uint64_t o = J.blk_off[b];
+  *t = (uint32_t)(o >> 32);
+  const DecRun& R = J.dec_runs[*t];
+  *j0 = o & 0xffffffffull;
+  *j1 = min(R.n, *j0 + kDecRunBlock);
+  return R;
+}
+
+// Entry descriptors of a pseudo block (key lengths, value places and
+// lengths); its key bytes, one lane per entry.  Returns the key bytes and
+// the longest key; false if a key is shorter than 8 bytes or a value lies
+// outside its table.
+__device__ __forceinline__ bool pseudo_entries(const JobDev& J, uint64_t b, uint64_t ebase,
+                                               uint32_t lane, uint32_t lanes, uint64_t* kbytes,
+                                               uint32_t* maxk) {
+  uint32_t t;
+  uint64_t j0, j1;
+  const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
+  const TableDesc T = J.tables[t];
+  bool ok = true;
+  uint32_t mk = 0;
+  for (uint64_t j = j0 + lane; j < j1; j += lanes) {
+    const uint64_t e = ebase + (j - j0);
+    const uint32_t kl = (uint32_t)(R.kcum[j + 1] - R.kcum[j]);
+    const uint32_t vl = R.vlen[j], vp = R.vpos[j];
+    if (kl < 8 || (uint64_t)vp + vl > T.size || e >= J.cap_entries) {
+      ok = false;
+      continue;
+    }
+    J.e_klen[e] = kl;
+    J.e_vlen[e] = vl;
+    J.e_voff[e] = (uint32_t)(T.off + vp);
+    mk = max(mk, kl);
+  }
+  *kbytes = R.kcum[j1] - R.kcum[j0];
+  *maxk = mk;
+  return ok;
+}
+
+// Key bytes (one contiguous copy), key offsets, prefixes and tags of a
+// pseudo block, by one warp; its keys start at kbase in the arena.
+__device__ __forceinline__ void pseudo_keys(const JobDev& J, uint64_t b, uint64_t ebase,
+                                            uint64_t kbase, uint32_t lane) {
+  uint32_t t;
+  uint64_t j0, j1;
+  const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
+  const uint64_t k0 = R.kcum[j0], kn = R.kcum[j1] - k0;
+  const uint8_t* src = R.keys + k0;
+  uint8_t* dst = J.keys + kbase;
+  for (uint64_t x = lane; x < kn; x += 32) dst[x] = src[x];
+  for (uint64_t j = j0 + lane; j < j1; j += 32) {
+    const uint64_t e = ebase + (j - j0);
+    J.e_koff[e] = (uint32_t)(kbase + (R.kcum[j] - k0));
+    J.e_pfx[e] = R.pfx[j];
+    J.e_tag[e] = R.tag[j];
   }
 }
 
@@ -340,6 +415,21 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_count(const JobDev* __
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
        b += (uint64_t)gridDim.x * kDecWarps) {
+    if (J.blk_size[b] == kPseudoBlock) {
+      uint32_t t;
+      uint64_t j0, j1;
+      const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
+      uint32_t mk = 0;
+      for (uint64_t j = j0 + lane; j < j1; j += 32) mk = max(mk, (uint32_t)(R.kcum[j + 1] - R.kcum[j]));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+      if (lane == 0) {
+        J.blk_nent[b] = (uint32_t)(j1 - j0);
+        J.blk_kbytes[b] = R.kcum[j1] - R.kcum[j0];
+        atomicMax(&J.ctr->max_klen, mk);
+      }
+      continue;
+    }
     const uint8_t* st = stage_block(J, b, W.stage, lane);
     block_count_one(J, b, lane, st ? st : J.in + J.blk_off[b]);
     __syncwarp();
@@ -355,8 +445,15 @@ __global__ void k_block_restarts(const JobDev* __restrict__ jobs) {
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblk;
        b += (uint64_t)gridDim.x * blockDim.x) {
-    const uint8_t* p = J.in + J.blk_off[b];
     const uint32_t size = J.blk_size[b];
+    if (size == kPseudoBlock) {
+      uint32_t t;
+      uint64_t j0, j1;
+      pseudo_block(J, b, &t, &j0, &j1);
+      J.blk_nent[b] = (uint32_t)(j1 - j0);
+      continue;
+    }
+    const uint8_t* p = J.in + J.blk_off[b];
     bool ok = size >= 4;
     const uint32_t nr = ok ? ld_le32(p + size - 4) : 0;
     if (ok && (uint64_t)nr * 4 + 4 > size) ok = false;
@@ -394,8 +491,9 @@ __global__ void __launch_bounds__(256) k_verify_blocks(const JobDev* __restrict_
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * nw + warp; b < nblk; b += (uint64_t)gridDim.x * nw) {
     // the index parse checked that the block and its 5-byte trailer lie in the table
-    const uint8_t* p = J.in + J.blk_off[b];
     const uint32_t size = J.blk_size[b];
+    if (size == kPseudoBlock) continue;  // a decoded form: no block bytes to check
+    const uint8_t* p = J.in + J.blk_off[b];
     const uint32_t crc = warp_block_crc(J, tab, p, size, p[size]);
     if (lane == 0 && crc != ld_le32(p + size + 1)) set_error(J.ctr, kErrChecksum, (uint32_t)b);
   }
@@ -672,6 +770,16 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* _
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
   for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
        b += (uint64_t)gridDim.x * kDecWarps) {
+    if (J.blk_size[b] == kPseudoBlock) {
+      uint64_t kb;
+      uint32_t mk;
+      if (!__all_sync(0xffffffffu, pseudo_entries(J, b, J.blk_ent_base[b], lane, 32, &kb, &mk))) {
+        if (lane == 0) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
+        continue;
+      }
+      pseudo_keys(J, b, J.blk_ent_base[b], J.blk_key_base[b], lane);
+      continue;
+    }
     const uint8_t* st = stage_block(J, b, W.stage, lane);
     if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
     __syncwarp();
@@ -717,7 +825,12 @@ __global__ void __launch_bounds__(256) k_block_walk(const JobDev* __restrict__ j
     uint64_t kb = 0;
     uint32_t maxk = 0;
     bool bad = false, short_key = false;
-    if (active) {
+    if (active && J.blk_size[b] == kPseudoBlock) {
+      if (!pseudo_entries(J, b, J.blk_ent_base[b], 0, 1, &kb, &maxk)) bad = true;
+      if (bad) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
+      else if (maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+      atomicMax(&J.ctr->max_klen, maxk);
+    } else if (active) {
       const uint8_t* p = J.in + J.blk_off[b];
       const uint32_t size = J.blk_size[b];
       const uint32_t nr = ld_le32(p + size - 4);  // checked by k_block_restarts
@@ -795,6 +908,10 @@ __global__ void __launch_bounds__(kKeysWarps * 32) k_block_keys(const JobDev* __
     const uint64_t ebase = J.blk_ent_base[b];
     const uint32_t nent = J.blk_nent[b];
     uint64_t kbase = J.blk_key_base[b];
+    if (J.blk_size[b] == kPseudoBlock) {
+      pseudo_keys(J, b, ebase, kbase, lane);
+      continue;
+    }
     for (uint32_t g0 = 0; g0 < nent; g0 += 32) {
       const uint32_t i = g0 + lane;
       const bool valid = i < nent;

@@ -607,6 +607,8 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab,
       p = put_varint(p, sh);
       p = put_varint(p, kl - sh);
       p = put_varint(p, vl);
+      if (J.dec_vpos)  // the value's place in its file, for the decoded form
+        J.dec_vpos[k] = (uint32_t)(J.b_off[b] + (uint64_t)(p - dst) + (kl - sh));
       for (uint32_t i = sh; i < kl; i++) *p++ = key[i];
       for (uint32_t i = 0; i < vl; i++) *p++ = val[i];
       if (restart) {
@@ -717,6 +719,8 @@ __global__ void __launch_bounds__(kEncWarps * 32, 5) k_encode_blocks(const JobDe
       if (j < n) {
         W.off[j] = ex;
         W.kbeg[j] = ex + hl;
+        if (J.dec_vpos)  // the value's place in its file, for the decoded form
+          J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + W.kd[j]);
       }
       carry += tot;
     }
@@ -839,6 +843,35 @@ __global__ void __launch_bounds__(kEncWarps * 32, 5) k_encode_blocks(const JobDe
       st_le32(dst + bsz + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
     }
     __syncwarp();
+  }
+}
+
+// The survivors' decoded form for later jobs (keep_decoded): key bytes at
+// dec_kcum (a scan of the key lengths), value lengths, prefixes and tags; the
+// value places were written by k_encode_blocks.  One warp per 32 survivors,
+// lanes over the group's key bytes.
+__global__ void k_emit_decoded(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error || !J.dec_keys) return;
+  const uint64_t n = J.ctr->n_kept;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g * 32 < n; g += warps) {
+    const uint64_t k = g * 32 + lane;
+    if (k < n) {
+      uint32_t kl;
+      const uint8_t* key = kept_key(J, k, &kl);
+      J.dec_vlen[k] = J.k_vlen[k];
+      J.dec_pfx[k] = user_prefix(key, kl);
+      J.dec_tag[k] = ld_le64(key + kl - 8);
+    }
+    const uint64_t k1 = min(n, g * 32 + 32);
+    for (uint64_t j = g * 32; j < k1; j++) {
+      uint32_t kl;
+      const uint8_t* key = kept_key(J, j, &kl);
+      uint8_t* d = J.dec_keys + J.dec_kcum[j];
+      for (uint32_t t = lane; t < kl; t += 32) d[t] = key[t];
+    }
   }
 }
 
@@ -1094,6 +1127,12 @@ void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
   // shared out among the jobs
   note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 5 * 4)),
                                         bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);
+}
+void launch_emit_decoded(const Batch& bt, cudaStream_t st) {
+  if (!bt.any_keep_decoded) return;
+  scan_batch(kScanDecKey, bt, bt.max_entries, st);
+  note_launch(), k_emit_decoded<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B), 256,
+                                  0, st>>>(bt.d);
 }
 void launch_encode_filters(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries * 32, 256, per_job(bt, 148 * 16)), bt.B),

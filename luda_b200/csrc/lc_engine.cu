@@ -251,6 +251,13 @@ struct lc_engine {
   ~lc_engine();
 };
 
+// A table's decoded entries, kept in device memory by the job that wrote the
+// table (a view into that job's decoded buffer); released with that job.
+struct lc_decoded {
+  DecRun run;
+  uint64_t table_size;
+};
+
 struct lc_job {
   lc_engine* eng = nullptr;
   int kind = 0;  // 0 compaction, 1 build table
@@ -266,6 +273,13 @@ struct lc_job {
   lc_table_options opt{};
   int32_t inputs_on_device = 0, outputs_on_device = 0;
   int32_t verify_checksums = 0;
+  int32_t keep_decoded = 0;
+  std::vector<const lc_decoded*> in_dec;  // per input table, or empty (none)
+  uint8_t* d_dec = nullptr;               // the survivors' decoded form (keep_decoded)
+  uint64_t d_dec_cap = 0;
+  std::vector<lc_decoded> out_dec;        // per output file: views into d_dec
+  std::vector<const lc_decoded*> out_dec_ptrs;
+  uint32_t decoded_inputs = 0;
   // build-table inputs
   int64_t bn = 0;
   const uint8_t *bkeys = nullptr, *bvals = nullptr;
@@ -393,7 +407,6 @@ struct DevAlloc {
   }
 };
 
-void check_launch() { CK(cudaGetLastError()); }
 
 // Phases of a job, timed with CUDA events on the job's stream when the engine
 // was created with LC_FLAG_PHASE_TIMING.
@@ -469,21 +482,6 @@ const char* err_name(uint32_t code) {
   }
 }
 
-void check_counters(const Counters& c) {
-  if (c.error) {
-    lc_status s = (c.error == kErrLimit || c.error == kErrArenaOverflow) ? LC_ERR_UNSUPPORTED
-                                                                         : LC_ERR_CORRUPT;
-    throw StatusError{s, std::string(err_name(c.error)) + " (detail " +
-                             std::to_string(c.error_detail) + ")"};
-  }
-}
-
-void read_counters(Counters* h, const Counters* d, cudaStream_t st) {
-  CK(cudaMemcpyAsync(h, d, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  check_counters(*h);
-}
-
 uint32_t bloom_k(int bpk) {
   // util/bloom.cc:20-24
   size_t k = static_cast<size_t>(bpk * 0.69);
@@ -533,6 +531,8 @@ struct JobRun {
   Counters hc{};
   std::vector<FileOut> files;
   std::vector<uint64_t> koff;
+  uint8_t* dec_block = nullptr;  // keep_decoded: the decoded buffer (device output slab)
+  uint64_t dec_cap = 0;
 };
 
 void job_fail(JobRun& r, lc_status s, const std::string& m) {
@@ -588,6 +588,7 @@ void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer
   launch_file_layout(bt, st);
   T.mark(kPartition);
   launch_encode_blocks(bt, st);
+  launch_emit_decoded(bt, st);
   T.mark(kEncodeBlocks);
   launch_encode_filters(bt, st);
   launch_encode_index(bt, st);
@@ -678,6 +679,22 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
                 (uint64_t)J.cap_files * 256 + (r.in_bytes + J.cap_key_bytes) / 256 + 65536;
   }
   J.out = A.output(J.cap_out, r.j->outputs_on_device == 1 || r.j->outputs_on_device == 2);
+  if (r.j->keep_decoded && !r.failed) {
+    // the survivors' decoded form, kept with the outputs: keys (at most the
+    // arena), key offsets, value lengths and places, prefixes, tags
+    const uint64_t kcap = (J.cap_key_bytes + 16 + 255) & ~uint64_t(255);
+    const uint64_t n8 = ((N + 1) * 8 + 255) & ~uint64_t(255), n4 = (N * 4 + 255) & ~uint64_t(255);
+    const uint64_t bytes = kcap + 3 * n8 + 2 * n4;
+    uint8_t* q = A.output(bytes, true);
+    r.dec_block = q;
+    r.dec_cap = A.outs.back().second;
+    J.dec_keys = q;
+    J.dec_kcum = reinterpret_cast<uint64_t*>(q + kcap);
+    J.dec_pfx = reinterpret_cast<uint64_t*>(q + kcap + n8);
+    J.dec_tag = reinterpret_cast<uint64_t*>(q + kcap + 2 * n8);
+    J.dec_vlen = reinterpret_cast<uint32_t*>(q + kcap + 3 * n8);
+    J.dec_vpos = reinterpret_cast<uint32_t*>(q + kcap + 3 * n8 + n4);
+  }
   J.fkeys = A.get<uint8_t>(2ull * J.cap_files * r.max_klen + 1);
   J.fkey_stride = r.max_klen;
   J.fkoff = A.get<uint64_t>(2ull * J.cap_files + 1);
@@ -780,7 +797,8 @@ struct lc_slot {
              (int)decode_merge, bt.B, bt.max_tables, bt.max_gp, bt.max_cap_triggers,
              bt.max_cap_files, (unsigned long long)bt.max_blocks_in,
              (unsigned long long)bt.max_entries, bt.merge_rounds, bt.chunk, bt.ctas_per_job,
-             bt.merge_items, bt.merge_threads, bt.max_runs, (int)bt.exact);
+             bt.merge_items, bt.merge_threads, bt.max_runs,
+             (int)bt.exact | ((int)bt.any_keep_decoded << 1));
     auto it = graphs.find(key);
     bool fresh = false;
     if (it == graphs.end()) {
@@ -910,7 +928,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     std::vector<uint64_t> in_base(B, 0);
     std::vector<bool> zero_copy(B, false);
     struct Offs {
-      uint64_t td, gpk, gpo, gpp, gpu, lb, bk, bso, blo, bsl, bll;
+      uint64_t td, dec, gpk, gpo, gpp, gpu, lb, bk, bso, blo, bsl, bll;
     };
     std::vector<Offs> offs(B);
     for (uint32_t i = 0; i < B; i++) {
@@ -930,6 +948,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         }
         td[t].run = run;
         td[t].size = j->tables[t].size;
+        td[t].cached = (!j->in_dec.empty() && j->in_dec[t]) ? 1u : 0u;
         in_run++;
       }
       J.n_tables = nt;
@@ -1002,6 +1021,13 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       J.n_base_levels = nb ? (uint32_t)lb.size() - 1 : 0;
       Offs& o = offs[i];
       o.td = S.put(td.data(), nt);
+      {
+        std::vector<DecRun> dr(nt);
+        memset(dr.data(), 0, sizeof(DecRun) * nt);
+        for (uint32_t t = 0; t < nt; t++)
+          if (td[t].cached) dr[t] = j->in_dec[t]->run;
+        o.dec = S.put(dr.data(), nt);
+      }
       o.gpk = S.put(gpk.data(), gpk.size());
       o.gpo = S.put(gpo.data(), gpo.size());
       o.gpp = S.put(gpp.data(), gpp.size());
@@ -1046,6 +1072,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       }
       J.in_end = J.in + J.in_size + (zero_copy[i] ? 0 : 16);
       J.tables = (const TableDesc*)(d_stage + o.td);
+      J.dec_runs = (const DecRun*)(d_stage + o.dec);
       J.gp_keys = d_stage + o.gpk;
       J.gp_key_off = (const uint64_t*)(d_stage + o.gpo);
       J.gp_prefix = (const uint64_t*)(d_stage + o.gpp);
@@ -1077,6 +1104,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       J.run_entry_begin = J.run_entry_begin_w;
       bt.max_tables = std::max(bt.max_tables, J.n_tables);
       bt.any_verify = bt.any_verify || (J.verify_checksums && !r.failed);
+      bt.any_keep_decoded = bt.any_keep_decoded || (j->keep_decoded && !r.failed);
       bt.max_blocks_in = std::max(bt.max_blocks_in, cap_blk);
     }
     JobDev* hj = reinterpret_cast<JobDev*>(pin1 + o_hj);
@@ -1273,6 +1301,26 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       j->kept_key_bytes = hc[i].kept_key_bytes;
       j->kept_value_bytes = hc[i].kept_value_bytes;
       if (j->outputs_on_device == 1 || j->outputs_on_device == 2) j->d_out = r.J.out;
+      if (r.J.dec_keys) {
+        // every output file's decoded entries: views into the job's buffer
+        j->d_dec = r.dec_block;
+        j->d_dec_cap = r.dec_cap;
+        j->out_dec.resize(nf);
+        j->out_dec_ptrs.resize(nf);
+        for (uint32_t f = 0; f < nf; f++) {
+          const uint64_t k0 = r.files[f].first_kept;
+          lc_decoded& x = j->out_dec[f];
+          x.run.n = r.files[f].end_kept - k0;
+          x.run.keys = r.J.dec_keys;
+          x.run.kcum = r.J.dec_kcum + k0;
+          x.run.vlen = r.J.dec_vlen + k0;
+          x.run.vpos = r.J.dec_vpos + k0;
+          x.run.pfx = r.J.dec_pfx + k0;
+          x.run.tag = r.J.dec_tag + k0;
+          x.table_size = r.files[f].size;
+          j->out_dec_ptrs[f] = &x;
+        }
+      }
     }
     T.mark(kDownload);
     CK(cudaEventRecord(ev1, st));
@@ -1295,6 +1343,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       j->batch_jobs = B;
       if (!runs[i].failed) j->status = LC_OK;
       if (j->d_out) keep.push_back(j->d_out);
+      if (j->d_dec) keep.push_back(j->d_dec);
     }
     A.release(keep);  // the batch has completed: its scratch serves the next one at once
     if (!retry.empty()) {
@@ -1314,6 +1363,8 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     A.release({});
     for (auto* j : jobs) {
       j->d_out = nullptr;
+      j->d_dec = nullptr;
+      j->out_dec_ptrs.clear();
       j->status = LC_ERR_CUDA;
       j->err = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
     }
@@ -1322,6 +1373,8 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     A.release({});
     for (auto* j : jobs) {
       j->d_out = nullptr;
+      j->d_dec = nullptr;
+      j->out_dec_ptrs.clear();
       j->status = se.s;
       j->err = se.msg;
     }
@@ -1489,7 +1542,8 @@ uint64_t estimate_bytes(const lc_job* j) {
   const uint64_t parse = (in / 13 + j->tables.size() + 1) * 48;
   const uint64_t arena = in + 65536;
   const uint64_t out = in + in / 4 + n_est * 66 + 65536;
-  return host_copy + parse + arena + out + n_est * kEntryArrayBytes + (8ull << 20);
+  const uint64_t dec = j->keep_decoded ? arena + n_est * 32 : 0;
+  return host_copy + parse + arena + out + dec + n_est * kEntryArrayBytes + (8ull << 20);
 }
 
 void finish(lc_job* j) {
@@ -1611,6 +1665,21 @@ lc_status copy_desc(lc_job* j, const lc_job_desc* d) {
     return fail(LC_ERR_INVALID_ARG, "outputs_on_device must be 0, 1 or 2");
   j->outputs_on_device = d->outputs_on_device;
   j->verify_checksums = d->verify_checksums;
+  if (d->keep_decoded && d->outputs_on_device != 1 && d->outputs_on_device != 2)
+    return fail(LC_ERR_INVALID_ARG, "keep_decoded needs outputs kept on the device");
+  j->keep_decoded = d->keep_decoded ? 1 : 0;
+  if (d->decoded) {
+    j->in_dec.assign(d->decoded, d->decoded + d->n_tables);
+    for (int32_t t = 0; t < d->n_tables; t++) {
+      const lc_decoded* x = d->decoded[t];
+      if (!x) continue;
+      if (!d->inputs_on_device)
+        return fail(LC_ERR_INVALID_ARG, "a decoded table must be read from device memory");
+      if (x->table_size != d->tables[t].size)
+        return fail(LC_ERR_INVALID_ARG, "decoded form of another table (size differs)");
+      j->decoded_inputs++;
+    }
+  }
   for (auto& t : j->tables) j->bytes_in += t.size;
   return LC_OK;
 }
@@ -1642,6 +1711,8 @@ void fill_out(lc_job* j, lc_job_out* o) {
   o->device_data = j->d_out;
   o->batch_jobs = j->batch_jobs;
   o->queue_ms = j->queue_ms;
+  o->decoded = j->keep_decoded && !j->out_dec_ptrs.empty() ? j->out_dec_ptrs.data() : nullptr;
+  o->decoded_inputs = j->decoded_inputs;
 }
 
 void host_crc_xpow(std::vector<uint32_t>& t) {
@@ -1852,6 +1923,7 @@ void lc_job_release(lc_job* j) {
   if (j->h_out) j->eng->pinned.give(j->h_out, j->h_out_cap);
   // the job has completed and the caller has finished reading its output
   if (j->d_out) j->eng->dev_out.give(j->d_out, j->d_out_cap);
+  if (j->d_dec) j->eng->dev_out.give(j->d_dec, j->d_dec_cap);
   delete j;
 }
 

@@ -58,8 +58,26 @@ struct TableDesc {
   uint64_t off;   // in `in`
   uint64_t size;
   uint32_t run;
-  uint32_t pad;
+  uint32_t cached;  // 1: read from its decoded form (JobDev::dec_runs[t]), not parsed
 };
+
+// The decoded entries of one table, kept by the job that wrote it: entry j
+// has the key keys[kcum[j], kcum[j+1]) and its value at byte vpos[j] of the
+// table, vlen[j] bytes long; pfx and tag as e_pfx / e_tag.
+struct DecRun {
+  uint64_t n;
+  const uint8_t* keys;
+  const uint64_t* kcum;  // n + 1, absolute in `keys`
+  const uint32_t* vlen;
+  const uint32_t* vpos;
+  const uint64_t* pfx;
+  const uint64_t* tag;
+};
+
+// Entries per pseudo block of a table read from its decoded form.
+constexpr uint32_t kDecRunBlock = 256;
+// blk_size of a pseudo block; its blk_off is (table << 32) | first entry.
+constexpr uint32_t kPseudoBlock = 0xffffffffu;
 
 struct FileOut {       // per output file
   uint64_t out_off;    // offset of the file in `out`
@@ -90,6 +108,7 @@ struct JobDev {
   uint64_t in_size;
   const uint8_t* in_end;  // end of memory that may be read with 16-byte loads
   const TableDesc* tables;
+  const DecRun* dec_runs;    // per table (n = 0 where the table is parsed)
   uint32_t n_tables;
   uint32_t n_runs;
   const uint64_t* run_entry_begin;  // filled after decode: entries of run r are
@@ -156,6 +175,14 @@ struct JobDev {
   uint32_t* k_klen;          // key length,
   uint32_t* k_voff;          // value offset in `in`,
   uint32_t* k_vlen;          // value length (gathered once from the entry arrays)
+
+  // the survivors' decoded form, kept for later jobs (keep_decoded; else null)
+  uint8_t* dec_keys;         // keys in survivor order
+  uint64_t* dec_kcum;        // n_kept + 1: key offsets in dec_keys
+  uint32_t* dec_vlen;
+  uint32_t* dec_vpos;        // value offset within its output file (by k_encode_blocks)
+  uint64_t* dec_pfx;
+  uint64_t* dec_tag;
   uint32_t* k_a;             // size as a restart entry
   uint32_t* k_b;             // size as a prefix-compressed entry
   uint32_t* k_shared;        // shared prefix with the previous kept key

@@ -52,6 +52,7 @@ struct Batch {
   uint32_t chain_smem_words = 11 * 1024;
   bool any_verify = false;  // some job checks its input blocks' CRCs
   bool exact = false;       // rerun with exact counting (blk_key_base from the counting walk)
+  bool any_keep_decoded = false;  // some job keeps its outputs' decoded form
   // tunables (chosen by the autotuner in lc_engine.cu)
   uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
   uint32_t merge_items = 8;   // outputs per thread in a merge round
@@ -68,6 +69,7 @@ enum ScanSel : int {
   kScanBcum,           // tmp32 -> b_cum
   kScanGcum,           // b_gbytes -> b_gcum
   kScanIcum,           // b_isize -> b_icum
+  kScanDecKey,         // k_klen -> dec_kcum (jobs that keep their decoded form)
 };
 void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st);
 uint64_t scan_scratch_elems(uint64_t n_cap);
@@ -109,6 +111,8 @@ void launch_file_layout(const Batch& bt, cudaStream_t st);
 // after the layout, blocks / filters / index + file keys are independent
 void launch_encode_blocks(const Batch& bt, cudaStream_t st);
 void launch_encode_filters(const Batch& bt, cudaStream_t st);
+// the decoded form of the survivors, for jobs with keep_decoded
+void launch_emit_decoded(const Batch& bt, cudaStream_t st);
 void launch_encode_index(const Batch& bt, cudaStream_t st);
 // metaindex, footer, filter tails and the trailers of filter/meta/index
 void launch_encode_meta(const Batch& bt, cudaStream_t st);

@@ -103,6 +103,16 @@ struct ScanOf<kScanIcum> {
   static __device__ uint64_t* total(const JobDev&) { return nullptr; }
 };
 
+template <>
+struct ScanOf<kScanDecKey> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.k_klen; }
+  static __device__ TO* out(const JobDev& J) { return J.dec_kcum; }  // null: job skipped
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_kept; }
+  static __device__ uint64_t* total(const JobDev&) { return nullptr; }
+};
+
 // Tile-sum scratch of a scan (the scans of a job run one after another).
 template <int S>
 __device__ __forceinline__ uint64_t* scan_tiles_of(const JobDev& J) {
@@ -150,7 +160,7 @@ __global__ void k_tile_reduce(const JobDev* __restrict__ jobs) {
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
-  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  if (threadIdx.x == 0) s_failed = J.ctr->error || SP::out(J) == nullptr;
   __syncthreads();
   if (s_failed) return;
   const uint64_t n = SP::n(J);
@@ -185,7 +195,7 @@ __global__ void k_tile_scan(const JobDev* __restrict__ jobs) {
   using TO = typename SP::TO;
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
-  if (threadIdx.x == 0) s_failed = J.ctr->error;
+  if (threadIdx.x == 0) s_failed = J.ctr->error || SP::out(J) == nullptr;
   __syncthreads();
   if (s_failed) return;
   const uint64_t n = SP::n(J);
@@ -249,6 +259,7 @@ void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st) {
     case kScanBcum: scan_sel<kScanBcum>(bt, n_cap, st); break;
     case kScanGcum: scan_sel<kScanGcum>(bt, n_cap, st); break;
     case kScanIcum: scan_sel<kScanIcum>(bt, n_cap, st); break;
+    case kScanDecKey: scan_sel<kScanDecKey>(bt, n_cap, st); break;
   }
 }
 

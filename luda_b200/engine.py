@@ -75,7 +75,8 @@ class LcJobDesc(C.Structure):
                 ("n_base_files", C.c_int32), ("base_files", C.POINTER(LcFileRange)),
                 ("smallest_snapshot", C.c_uint64), ("options", LcTableOptions),
                 ("inputs_on_device", C.c_int32), ("outputs_on_device", C.c_int32),
-                ("verify_checksums", C.c_int32)]
+                ("verify_checksums", C.c_int32), ("keep_decoded", C.c_int32),
+                ("decoded", C.POINTER(C.c_void_p))]
 
 
 class LcJobOut(C.Structure):
@@ -88,7 +89,8 @@ class LcJobOut(C.Structure):
                 ("phase_name", C.POINTER(C.c_char_p)), ("phase_ms", C.POINTER(C.c_float)),
                 ("key_bytes_in", C.c_uint64), ("value_bytes_out", C.c_uint64),
                 ("key_bytes_out", C.c_uint64), ("device_data", C.c_void_p),
-                ("batch_jobs", C.c_uint32), ("queue_ms", C.c_double)]
+                ("batch_jobs", C.c_uint32), ("queue_ms", C.c_double),
+                ("decoded", C.POINTER(C.c_void_p)), ("decoded_inputs", C.c_uint32)]
 
 LC_FLAG_PHASE_TIMING = 1
 LC_FLAG_NO_GRAPHS = 2
@@ -172,6 +174,7 @@ class OutputFile:
     smallest: bytes
     largest: bytes
     entries: int
+    decoded: Optional[int] = None  # lc_decoded handle (keep_decoded), valid while the result lives
 
 
 @dataclasses.dataclass
@@ -192,6 +195,7 @@ class CompactionResult:
     batch_jobs: int = 1
     queue_ms: float = 0.0
     _handle: object = None
+    decoded_inputs: int = 0  # input tables read from their decoded form
 
     def release(self):
         """Frees the job's output buffers (host pinned or device)."""
@@ -248,10 +252,14 @@ def table_options(o: TableOptions) -> LcTableOptions:
 
 
 def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[int]] = None,
-              outputs_on_device: int = 0, verify_checksums: bool = False) -> LcJobDesc:
+              outputs_on_device: int = 0, verify_checksums: bool = False,
+              keep_decoded: bool = False, decoded: Optional[Sequence[Optional[int]]] = None
+              ) -> LcJobDesc:
     """The descriptor a patched DoCompactionWork would build from its
     Compaction: runs in MakeInputIterator order, grandparents_, and every file
-    at levels >= L+2 for the base-level test."""
+    at levels >= L+2 for the base-level test.  ``decoded``: per input table (in
+    the same order as ``device_tables``) the ``lc_decoded`` handle of its
+    decoded form, or None."""
     runs = job.runs()
     tables = [f for r in runs for f in r]
     t_arr = (LcTable * max(1, len(tables)))()
@@ -279,10 +287,15 @@ def make_desc(job: CompactionJob, keep: _Keep, device_tables: Optional[Sequence[
     gp, base = job.grandparents(), job.base_files()
     gpa, ba = ranges(gp), ranges(base)
     keep.objs += [t_arr, rc, gpa, ba]
+    dec = None
+    if decoded is not None and any(decoded):
+        dec = (C.c_void_p * max(1, len(tables)))(*[d or None for d in decoded])
+        keep.objs.append(dec)
     return LcJobDesc(job.level, len(tables), t_arr, len(runs), rc, len(gp), gpa, len(base), ba,
                      job.smallest_snapshot(), table_options(job.options),
                      1 if device_tables is not None else 0, int(outputs_on_device),
-                     1 if verify_checksums else 0)
+                     1 if verify_checksums else 0, 1 if keep_decoded else 0,
+                     C.cast(dec, C.POINTER(C.c_void_p)) if dec is not None else None)
 
 
 def _result(out: LcJobOut, outputs_on_device) -> CompactionResult:
@@ -301,13 +314,14 @@ def _result(out: LcJobOut, outputs_on_device) -> CompactionResult:
                          out.smallest_len[i])
         lg = C.string_at(C.addressof(out.key_bytes.contents) + out.largest_offset[i],
                          out.largest_len[i])
-        files.append(OutputFile(data, sm, lg, int(out.file_entries[i])))
+        dec = out.decoded[i] if out.decoded else None
+        files.append(OutputFile(data, sm, lg, int(out.file_entries[i]), dec))
     phases = {out.phase_name[i].decode(): out.phase_ms[i] for i in range(out.n_phases)}
     return CompactionResult(files, out.bytes_in, out.bytes_out, out.entries_in, out.entries_out,
                             out.device_ms, out.device_data, offs,
                             out.kernel_launches, phases or None, out.key_bytes_in,
                             out.value_bytes_out, out.key_bytes_out, out.batch_jobs,
-                            out.queue_ms)
+                            out.queue_ms, decoded_inputs=out.decoded_inputs)
 
 
 class Engine:
@@ -351,13 +365,18 @@ class Engine:
             raise LcError(st, self.lib.lc_last_error().decode())
 
     def prepare(self, job: CompactionJob, device_tables: Optional[Sequence[int]] = None,
-                outputs_on_device: int = 0, verify_checksums: bool = False) -> "PreparedJob":
+                outputs_on_device: int = 0, verify_checksums: bool = False,
+                keep_decoded: bool = False,
+                decoded: Optional[Sequence[Optional[int]]] = None) -> "PreparedJob":
         """Builds the C descriptor once, for repeated runs of the same job.
         ``verify_checksums`` checks every input data block's CRC first
-        (LevelDB's paranoid_checks on compaction inputs)."""
+        (LevelDB's paranoid_checks on compaction inputs).  ``keep_decoded``
+        keeps the outputs' decoded entries on the device (``OutputFile.decoded``);
+        ``decoded`` gives, per device table, such a handle or None."""
         keep = _Keep()
         return PreparedJob(make_desc(job, keep, device_tables, outputs_on_device,
-                                     verify_checksums), keep, outputs_on_device)
+                                     verify_checksums, keep_decoded, decoded), keep,
+                           outputs_on_device)
 
     def run(self, p: "PreparedJob") -> CompactionResult:
         out = LcJobOut()

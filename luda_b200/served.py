@@ -105,6 +105,7 @@ class SimTable:
     dev: int = 0  # device address of the same bytes, 0 if not resident
     owner: object = None  # _Owner keeping host/device memory alive
     ready: Optional[Callable[[], None]] = None  # waits until the device copy exists
+    dec: Optional[int] = None  # handle of its decoded entries on the device (outputs of jobs)
 
 
 class _Owner:
@@ -306,6 +307,7 @@ class JobRecord:
     done_s: float
     n_inputs: int
     resident_inputs: int
+    decoded_inputs: int = 0  # inputs read from their decoded form (no parse, no decode)
     device_ms: float = 0.0  # the engine's device time for the batch that ran the job
     batch_jobs: int = 1  # jobs in that batch
     queue_ms: float = 0.0  # time in the engine's queue before its batch started
@@ -350,6 +352,8 @@ class ServeStats:
             "mean_ms": float(lat.mean()),
             "jobs_by_level": {str(l): sum(1 for j in self.jobs if j.level == l)
                               for l in sorted(set(j.level for j in self.jobs))},
+            "decoded_resident_fraction": (sum(j.decoded_inputs for j in self.jobs) /
+                                          max(1, sum(j.n_inputs for j in self.jobs))),
             "resident_input_fraction": (sum(j.resident_inputs for j in self.jobs) /
                                         max(1, sum(j.n_inputs for j in self.jobs))),
             "h2d_mib": self.h2d_bytes / float(1 << 20),
@@ -381,8 +385,12 @@ class Server:
 
     def __init__(self, engine, n_db: int, mode: str = "served",
                  options: Optional[TableOptions] = None, upload=None, free=None,
-                 record_bytes: bool = False, level_scale: float = 1.0, ready=None):
+                 record_bytes: bool = False, level_scale: float = 1.0, ready=None,
+                 keep_decoded: bool = True):
         assert mode in ("served", "plain")
+        # served mode: outputs kept on the device also keep their decoded
+        # entries, so that the next level's job skips parsing and decoding them
+        self.keep_decoded = keep_decoded and mode == "served"
         self.engine = engine
         self.mode = mode
         self.options = options or TableOptions()
@@ -415,7 +423,8 @@ class Server:
             if self.mode == "served" and res.device_ptr:
                 dev = int(res.device_ptr) + int(res.file_offsets[i])
             out.append(SimTable(db.new_number(), level + 1, f.smallest, f.largest, len(f.data),
-                                host=f.data, dev=dev, owner=owner))
+                                host=f.data, dev=dev, owner=owner,
+                                dec=getattr(f, "decoded", None) if dev else None))
         self.d2h += res.bytes_out
         return out
 
@@ -433,13 +442,19 @@ class Server:
                 if f.sim.ready is not None:
                     f.sim.ready()
                     f.sim.ready = None
+            decoded = [f.sim.dec for f in tables]
             p = self.engine.prepare(job, device_tables=[f.sim.dev for f in tables],
-                                    outputs_on_device=2)
+                                    outputs_on_device=2, keep_decoded=self.keep_decoded,
+                                    decoded=decoded if self.keep_decoded else None)
+            n_decoded = sum(1 for d in decoded if d) if self.keep_decoded else 0
         else:
             for f in tables:
                 f.data = f.sim.host
-            p = self.engine.prepare(job, outputs_on_device=2 if self.mode == "served" else 0)
+            served_mode = self.mode == "served"
+            p = self.engine.prepare(job, outputs_on_device=2 if served_mode else 0,
+                                    keep_decoded=served_mode and self.keep_decoded)
             resident = 0
+            n_decoded = 0
             self.h2d += sum(f.file_size for f in tables)
         for f in tables:
             # host copy of the inputs for the record (the live buffers are reused)
@@ -447,7 +462,8 @@ class Server:
         h = self.engine.submit_prepared(p)
         db.busy = True
         rec = JobRecord(db.index, level, sum(f.file_size for f in tables), 0, now(), 0.0,
-                        len(tables), resident, job=job if self.record_bytes else None)
+                        len(tables), resident, job=job if self.record_bytes else None,
+                        decoded_inputs=n_decoded)
         return h, (db, level, in0, in1, rec, p)
 
     def run(self, arrivals: Sequence[Flush], clock=time.perf_counter,

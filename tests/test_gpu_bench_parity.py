@@ -50,6 +50,8 @@ def test_served_bench_scale_matches_oracle(engine):
         st = srv.run(served.schedule(fl, None))
         assert {j.level for j in st.jobs} >= {0, 1}
         assert any(j.resident_inputs == j.n_inputs and j.n_inputs > 0 for j in st.jobs)
+        # outputs of earlier jobs are read from their decoded form
+        assert any(j.decoded_inputs > 0 for j in st.jobs)
         for rec in st.jobs:
             assert [o[0] for o in oracle.compact(rec.job, "oracle")] == rec.file_bytes
         for db, f in zip(srv.dbs, fl):

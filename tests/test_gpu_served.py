@@ -3,7 +3,8 @@ the mix.
 
 Several simulated databases run their compactions through one engine with
 continuous batching, device-resident level-0 uploads and outputs kept on the
-device for the next level's jobs.  Each job the loop ran is then compacted
+device, with their decoded entries, for the next level's jobs (which then read
+those inputs without parsing or decoding them).  Each job the loop ran is then compacted
 again alone from host copies of its inputs (lc_compact) and by the CPU
 restatement; all three must be byte-identical, and every database must end up
 holding the newest value of every key written.
@@ -43,6 +44,8 @@ def test_served_jobs_same_alone_and_in_mix(flushes, rate):
         st = srv.run(served.schedule(fl, rate))
         assert len(st.jobs) > 0 and {j.level for j in st.jobs} >= {0, 1}
         assert any(j.resident_inputs == j.n_inputs and j.n_inputs > 0 for j in st.jobs)
+        # outputs of earlier jobs are read from their decoded form
+        assert any(j.decoded_inputs > 0 for j in st.jobs)
         for rec in st.jobs:
             alone = eng.compact(rec.job)
             assert alone.file_bytes() == rec.file_bytes

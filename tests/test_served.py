@@ -46,7 +46,8 @@ class OracleEngine:
         self.rng = np.random.default_rng(seed)
         self.jobs = 0
 
-    def prepare(self, job, device_tables=None, outputs_on_device=0):
+    def prepare(self, job, device_tables=None, outputs_on_device=0, keep_decoded=False,
+                decoded=None):
         # the real engine takes the table pointers here; the host may drop
         # its references to the job's buffers right after
         assert device_tables is None
@@ -131,7 +132,8 @@ def test_uploads_ready_before_a_job_reads_them(small_flushes):
     class DeviceOracle(OracleEngine):
         device_jobs = 0
 
-        def prepare(self, job, device_tables=None, outputs_on_device=0):
+        def prepare(self, job, device_tables=None, outputs_on_device=0, keep_decoded=False,
+                decoded=None):
             if device_tables is not None:
                 assert all(handles[a]["ready"] for a in device_tables)
                 self.device_jobs += 1
