@@ -777,190 +777,33 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* _
         if (lane == 0) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
         continue;
       }
-      pseudo_keys(J, b, J.blk_ent_base[b], J.blk_key_base[b], lane);
+      uint64_t kbase = 0;
+      if (J.reserve_keys) {
+        // single pass: reserve the block's key bytes in the arena
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+        int retry = 0;
+        if (lane == 0) {
+          atomicMax(&J.ctr->max_klen, mk);
+          if (mk > J.max_key_len) {
+            retry = 1;
+          } else {
+            kbase = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
+            retry = kbase + kb > J.cap_key_bytes;
+          }
+          if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+        }
+        if (__shfl_sync(0xffffffffu, retry, 0)) continue;
+        kbase = __shfl_sync(0xffffffffu, kbase, 0);
+      } else {
+        kbase = J.blk_key_base[b];
+      }
+      pseudo_keys(J, b, J.blk_ent_base[b], kbase, lane);
       continue;
     }
     const uint8_t* st = stage_block(J, b, W.stage, lane);
     if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
     __syncwarp();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Single-pass decode without staging the blocks (jobs with reserve_keys):
-//
-// 1. k_block_walk, one thread per data block: walks every restart run's
-//    entry headers straight from global memory -- only the header bytes are
-//    touched, never the values -- checking each (bounds, no shared prefix at
-//    a restart, shared prefix within the previous key, keys of at least 8
-//    bytes, runs parsed exactly to their ends) and writing each entry's key
-//    length, value place and length, plus (in scratch that the merge and the
-//    partition overwrite later) its key delta's place and shared-prefix
-//    length.  The blocks' key bytes are reserved in the key arena with one
-//    atomic add per warp.
-// 2. k_block_keys, one warp per data block: rebuilds the keys in entry order
-//    in shared memory (lanes over bytes; the shared prefix is the front of the
-//    previous key, the rest is the delta read from global memory), writes them
-//    with 16-byte stores, and writes the entries' key offsets, prefixes and
-//    tags.
-// The delta places live in m_tmp and the shared lengths in k_a.
-constexpr uint32_t kKeysWarps = 8;
-constexpr uint32_t kKeysBuf = 32 * 256 + 32;  // 32 keys of at most 256 bytes, 16-byte phase
-
-__global__ void __launch_bounds__(256) k_block_walk(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  if (J.ctr->error) return;  // after a footer or index error some handles are unset
-  uint32_t* __restrict__ d_dpos = J.m_tmp;  // key delta place in `in`
-  uint32_t* __restrict__ d_sh = J.k_a;      // shared prefix length
-  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  const uint32_t lane = threadIdx.x & 31;
-  // every lane of a warp takes part in the warp's reservation, so all lanes
-  // run the loop the same number of times
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t b_first = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t w_first = b_first - lane;
-  const uint64_t trips = nblk > w_first ? (nblk - w_first + stride - 1) / stride : 0;
-  for (uint64_t it = 0, b = b_first; it < trips; it++, b += stride) {
-    const bool active = b < nblk;
-    uint64_t kb = 0;
-    uint32_t maxk = 0;
-    bool bad = false, short_key = false;
-    if (active && J.blk_size[b] == kPseudoBlock) {
-      if (!pseudo_entries(J, b, J.blk_ent_base[b], 0, 1, &kb, &maxk)) bad = true;
-      if (bad) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
-      else if (maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-      atomicMax(&J.ctr->max_klen, maxk);
-    } else if (active) {
-      const uint8_t* p = J.in + J.blk_off[b];
-      const uint32_t size = J.blk_size[b];
-      const uint32_t nr = ld_le32(p + size - 4);  // checked by k_block_restarts
-      const uint64_t ra = size - 4 - 4ull * nr;
-      uint64_t e = J.blk_ent_base[b];
-      const uint64_t e_end = e + J.blk_nent[b];
-      for (uint32_t r = 0; r < nr && !bad; r++) {
-        const uint32_t w = ld_le32(p + ra + 4ull * r);
-        const uint32_t cnt = w & 0xff;
-        const uint8_t* q = p + (w >> 8);
-        const uint8_t* lim = p + ((r + 1 < nr) ? (ld_le32(p + ra + 4ull * (r + 1)) >> 8) : ra);
-        uint32_t prev = 0;
-        for (uint32_t k = 0; k < cnt; k++) {
-          uint32_t sh, ns, vl;
-          const uint8_t* d = entry_header(q, lim, &sh, &ns, &vl);
-          if (!d || (k == 0 && sh != 0) || sh > prev || e >= e_end || e >= J.cap_entries) {
-            bad = true;
-            break;
-          }
-          const uint32_t kl = sh + ns;
-          if (kl < 8) short_key = true;
-          J.e_klen[e] = kl;
-          J.e_vlen[e] = vl;
-          J.e_voff[e] = (uint32_t)((d + ns) - J.in);
-          d_dpos[e] = (uint32_t)(d - J.in);
-          d_sh[e] = sh;
-          kb += kl;
-          maxk = max(maxk, kl);
-          prev = kl;
-          q = d + ns + vl;
-          e++;
-        }
-        if (!bad && q != lim) bad = true;
-      }
-      if (!bad && e != e_end) bad = true;
-      if (bad) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
-      else if (short_key) set_error(J.ctr, kErrShortKey, (uint32_t)b);
-      else if (maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-      atomicMax(&J.ctr->max_klen, maxk);
-    }
-    // key arena: one reservation per warp, each block its own span
-    const uint64_t need = (active && !bad && !short_key) ? kb : 0;
-    uint64_t tot;
-    const uint64_t ex = warp_excl<uint64_t>(need, &tot);
-    uint64_t base = 0;
-    if (lane == 0 && tot)
-      base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)tot);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (active) {
-      if (base + tot > J.cap_key_bytes) {
-        if (need) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-      } else {
-        J.blk_key_base[b] = base + ex;
-      }
-    }
-  }
-}
-
-struct KeysWarpSmem {
-  uint8_t keybuf[kKeysBuf];
-  uint8_t lastkey[kDecLastKey];  // last key of the previous group of 32 entries
-};
-
-__global__ void __launch_bounds__(kKeysWarps * 32) k_block_keys(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  extern __shared__ __align__(16) uint8_t keys_smem[];
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  KeysWarpSmem& W = reinterpret_cast<KeysWarpSmem*>(keys_smem)[warp];
-  if (J.ctr->error) return;
-  const uint32_t* __restrict__ d_dpos = J.m_tmp;
-  const uint32_t* __restrict__ d_sh = J.k_a;
-  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  for (uint64_t b = (uint64_t)blockIdx.x * kKeysWarps + warp; b < nblk;
-       b += (uint64_t)gridDim.x * kKeysWarps) {
-    const uint64_t ebase = J.blk_ent_base[b];
-    const uint32_t nent = J.blk_nent[b];
-    uint64_t kbase = J.blk_key_base[b];
-    if (J.blk_size[b] == kPseudoBlock) {
-      pseudo_keys(J, b, ebase, kbase, lane);
-      continue;
-    }
-    for (uint32_t g0 = 0; g0 < nent; g0 += 32) {
-      const uint32_t i = g0 + lane;
-      const bool valid = i < nent;
-      const uint64_t e = ebase + i;
-      const uint32_t kl = valid ? J.e_klen[e] : 0;
-      const uint32_t esh = valid ? d_sh[e] : 0;
-      const uint32_t edp = valid ? d_dpos[e] : 0;
-      uint32_t gk;
-      const uint32_t kofs = warp_excl<uint32_t>(kl, &gk);
-      uint8_t* gdst = J.keys + kbase;
-      const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
-      uint8_t* kb = W.keybuf + kph;
-      const uint32_t cnt = min(32u, nent - g0);
-      for (uint32_t x = 0; x < cnt; x++) {
-        const uint32_t xsh = __shfl_sync(0xffffffffu, esh, x);
-        const uint32_t xkl = __shfl_sync(0xffffffffu, kl, x);
-        const uint32_t xdp = __shfl_sync(0xffffffffu, edp, x);
-        const uint32_t xofs = __shfl_sync(0xffffffffu, kofs, x);
-        const uint32_t pofs = __shfl_sync(0xffffffffu, kofs, (x + 31) & 31);
-        const uint8_t* prev = x == 0 ? W.lastkey : kb + pofs;
-        const uint8_t* src = J.in + xdp - xsh;
-        uint8_t* d = kb + xofs;
-        for (uint32_t t = lane; t < xkl; t += 32) d[t] = t < xsh ? prev[t] : __ldg(src + t);
-        __syncwarp();
-      }
-      {
-        // the group's last key is the next group's first prefix
-        const uint32_t lofs = __shfl_sync(0xffffffffu, kofs, cnt - 1);
-        const uint32_t lkl = __shfl_sync(0xffffffffu, kl, cnt - 1);
-        for (uint32_t t = lane; t < lkl; t += 32) W.lastkey[t] = kb[lofs + t];
-      }
-      __syncwarp();
-      // keys out: head bytes, 16-byte body, tail
-      const uint32_t head = (16 - kph) & 15;
-      const uint32_t h = head < gk ? head : gk;
-      if (lane < h) gdst[lane] = kb[lane];
-      const uint32_t body = (gk - h) & ~15u;
-      const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
-      uint4* dv = reinterpret_cast<uint4*>(gdst + h);
-      for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
-      for (uint32_t t = h + body + lane; t < gk; t += 32) gdst[t] = kb[t];
-      if (valid) {
-        J.e_koff[e] = (uint32_t)(kbase + kofs);
-        J.e_pfx[e] = user_prefix(kb + kofs, kl);
-        J.e_tag[e] = ld_le64(kb + kofs + kl - 8);
-      }
-      kbase += gk;
-      __syncwarp();
-    }
   }
 }
 
@@ -990,10 +833,10 @@ __global__ void k_entries_from_offsets(const JobDev* __restrict__ jobs) {
 }  // namespace
 
 void launch_table_index_count(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_table_index_count<<<dim3(bt.max_tables, bt.B), 128, 0, st>>>(bt.d);
+  note_launch(), k_table_index_count<<<dim3(bt.max_tables, bt.B), 1024, 0, st>>>(bt.d);
 }
 void launch_table_index_entries(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_table_index_entries<<<dim3(bt.max_tables, bt.B), 128, 0, st>>>(bt.d);
+  note_launch(), k_table_index_entries<<<dim3(bt.max_tables, bt.B), 1024, 0, st>>>(bt.d);
 }
 
 static void dec_smem_attr(const void* fn) {
@@ -1011,8 +854,6 @@ static unsigned dec_ctas(const Batch& bt) {
 void decode_kernel_attributes() {
   dec_smem_attr((const void*)k_block_count);
   dec_smem_attr((const void*)k_block_decode);
-  cudaFuncSetAttribute(k_block_keys, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(kKeysWarps * sizeof(KeysWarpSmem)));
 }
 
 void launch_block_count(const Batch& bt, cudaStream_t st) {
@@ -1032,17 +873,8 @@ void launch_run_bounds(const Batch& bt, cudaStream_t st) {
   note_launch(), k_run_bounds<<<dim3((bt.max_tables + 127) / 128 + 1, bt.B), 128, 0, st>>>(bt.d);
 }
 void launch_block_decode(const Batch& bt, cudaStream_t st) {
-  if (bt.exact) {
-    // rerun with exact counting: blocks staged whole, keys placed by the scan
-    note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
-                                    kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
-    return;
-  }
-  const uint64_t cap = std::max<uint64_t>(1, bt.ctas_per_job ? bt.ctas_per_job : 148 * 8 / bt.B);
-  note_launch(), k_block_walk<<<dim3(grid_x(bt.max_blocks_in, 256, 4 * cap), bt.B), 256, 0, st>>>(
-      bt.d);
-  note_launch(), k_block_keys<<<dim3(grid_x(bt.max_blocks_in, kKeysWarps, 3 * cap), bt.B),
-                                kKeysWarps * 32, kKeysWarps * sizeof(KeysWarpSmem), st>>>(bt.d);
+  note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
+                                  kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
 }
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st) {
   note_launch(), k_entries_from_offsets<<<dim3(grid_x(bt.max_entries, 256, 148 * 8), bt.B), 256, 0,

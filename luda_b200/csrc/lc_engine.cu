@@ -798,7 +798,7 @@ struct lc_slot {
              bt.max_cap_files, (unsigned long long)bt.max_blocks_in,
              (unsigned long long)bt.max_entries, bt.merge_rounds, bt.chunk, bt.ctas_per_job,
              bt.merge_items, bt.merge_threads, bt.max_runs,
-             (int)bt.exact | ((int)bt.any_keep_decoded << 1));
+             (int)bt.any_keep_decoded);
     auto it = graphs.find(key);
     bool fresh = false;
     if (it == graphs.end()) {
@@ -1056,7 +1056,6 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     bt.ctas_per_job = tun.ctas_per_job;
     bt.merge_items = tun.merge_items;
     bt.merge_threads = tun.merge_threads;
-    bt.exact = exact;
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       JobDev& J = r.J;

@@ -51,7 +51,6 @@ struct Batch {
   uint32_t chunk = 4096;
   uint32_t chain_smem_words = 11 * 1024;
   bool any_verify = false;  // some job checks its input blocks' CRCs
-  bool exact = false;       // rerun with exact counting (blk_key_base from the counting walk)
   bool any_keep_decoded = false;  // some job keeps its outputs' decoded form
   // tunables (chosen by the autotuner in lc_engine.cu)
   uint32_t ctas_per_job = 0;  // grid x of the grid-stride kernels; 0 = from the sizes
