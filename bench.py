@@ -467,7 +467,9 @@ def job_leg(name, args, eng, eng_ph, flush, torch, steps, warmup, clocks=None, p
             torch.cuda.synchronize()
             h2d.append(a.elapsed_time(b))
             dh.append(b.elapsed_time(c))
-        r = eng_ph.run(eng_ph.prepare(job))
+        p_host = eng_ph.prepare(job)
+        eng_ph.run(p_host).release()  # pinned output memory taken once, outside the figure
+        r = eng_ph.run(p_host)
         up_ms, down_ms = r.phase_ms["upload"], r.phase_ms["download"]
         r.release()
         link = {"h2d_gbs": src.numel() / (min(h2d) / 1e3) / 1e9,
