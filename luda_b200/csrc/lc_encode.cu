@@ -551,25 +551,28 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
   }
 }
 
-// One warp per output data block, in three passes over a per-warp entry table
-// (output offset, key/value sources and lengths; up to kEncMaxEnt entries,
-// larger blocks take the direct path):
-//  1. lanes walk the 4-byte words of the global grid that cover the block,
-//     32 consecutive words per step; a word that lies inside one entry's key
-//     delta or value is two read-only loads, a funnel shift and one aligned
-//     store -- the bulk of the bytes, with the same work in every lane;
-//  2. one lane per entry writes, with byte stores, what step 1 left: the
-//     header varints, the bytes of the key/value words cut by a segment edge,
-//     and the restart words;
-//  3. lanes read the finished block back (from L2) in contiguous 16-byte
-//     chunks, each computing a CRC32C register over its stretch; the
-//     registers are combined with shifts x^(8n) mod P into the trailer.
+// One warp per output data block, assembled in the warp's shared-memory stage
+// (which has the block's own 16-byte phase in global memory), in five steps:
+//  1. entry table, one lane per entry: output offsets, key/value sources and
+//     lengths, and the 16-byte chunks of the stage that lie wholly inside a
+//     long (>= kEncLong bytes) key delta or value;
+//  2. one lane per entry writes its header varints, its short stretches and
+//     the cut edges of its long ones byte by byte, and its restart word;
+//  3. the long stretches' chunks as one flat list over the warp: a chunk is
+//     five 4-byte read-only loads and four funnel shifts at any source
+//     alignment, then one 16-byte shared store; kEncChunks chunks per lane
+//     are loaded before any is stored;
+//  4. CRC32C of the block plus its type byte from the stage, lanes over
+//     contiguous stretches (slicing-by-4 tables), combined by x^(8n) shifts;
+//  5. the stage -- block, type byte and CRC -- to global memory with 16-byte
+//     stores (byte stores for the two partial chunks at the ends).
+// Blocks with more than kEncMaxEnt entries, or too large for the stage, take
+// the direct path.
 constexpr uint32_t kEncWarps = 8;
 constexpr uint32_t kEncMaxEnt = 128;
-// Words per lane with loads in flight together.  4 with five CTAs (40 warps)
-// per SM beat 8 with four (registers capped the occupancy): encode_blocks on
-// the 65.6 MiB L1->L2 job 0.135 ms vs 0.148 ms on B200; six CTAs spilled.
-constexpr uint32_t kEncBatch = 4;
+constexpr uint32_t kEncStage = 8448;  // block + 5-byte trailer + 16-byte phase
+constexpr uint32_t kEncLong = 32;     // stretches at least this long are copied in chunks
+constexpr uint32_t kEncChunks = 4;    // chunks in flight per lane
 struct EncWarp {
   uint32_t off[kEncMaxEnt + 1];  // entry output offset in the block (+ end)
   uint32_t kbeg[kEncMaxEnt];     // offset of the key delta (after the header)
@@ -578,6 +581,8 @@ struct EncWarp {
   uint32_t kd[kEncMaxEnt];       // key delta length
   uint32_t vl[kEncMaxEnt];       // value length
   uint32_t sh[kEncMaxEnt];       // shared prefix length
+  uint32_t cc[kEncMaxEnt + 1];   // chunks of the long stretches before the entry
+  __align__(16) uint8_t stage[kEncStage];
 };
 constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * sizeof(EncWarp);
 
@@ -627,48 +632,32 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab,
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
-// Prefetch into L1 the 128-byte lines of [p, p + n).
-__device__ __forceinline__ void prefetch_l1(const uint8_t* p, uint32_t n) {
-  if (!n) return;
-  const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127);
-  const uintptr_t e = reinterpret_cast<uintptr_t>(p) + n;
-  for (uintptr_t q = a; q < e; q += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+// Full 16-byte chunks of stage stretch [a, b) (stage offsets): first chunk
+// offset and count.
+__device__ __forceinline__ uint32_t chunks_in(uint32_t a, uint32_t b, uint32_t* first) {
+  const uint32_t a0 = (a + 15) & ~15u, b0 = b & ~15u;
+  *first = a0;
+  return b0 > a0 ? (b0 - a0) >> 4 : 0;
 }
 
-// Byte i of the entry header varint(sh) varint(kd) varint(vl).
-__device__ __forceinline__ uint32_t header_byte(uint32_t sh, uint32_t kd, uint32_t vl, uint32_t i) {
-  uint32_t v = sh;
-  uint32_t n = varint_len(sh);
-  if (i >= n) {
-    i -= n;
-    v = kd;
-    n = varint_len(kd);
-    if (i >= n) {
-      i -= n;
-      v = vl;
-      n = varint_len(vl);
+// Bytes [a, b) of the stage from src, except the full chunks of a long
+// stretch (step 3 writes those).
+__device__ __forceinline__ void stretch_bytes(uint8_t* st, uint32_t a, uint32_t b,
+                                              const uint8_t* src, bool chunked) {
+  uint32_t c0 = b, c1 = b;
+  if (chunked) {
+    uint32_t first;
+    const uint32_t nq = chunks_in(a, b, &first);
+    if (nq) {
+      c0 = first;
+      c1 = first + 16 * nq;
     }
   }
-  const uint32_t bits = (v >> (7 * i)) & 0x7f;
-  return i + 1 < n ? (bits | 0x80) : bits;
+  for (uint32_t p = a; p < c0; p++) st[p] = __ldg(src + (p - a));
+  for (uint32_t p = c1; p < b; p++) st[p] = __ldg(src + (p - a));
 }
 
-// Bytes [a, b) of the block at dst, from src, except the 4-byte words of the
-// global grid that lie wholly inside [a, b) (step 1 wrote those).
-__device__ __forceinline__ void enc_edges(uint8_t* dst, uint32_t ph4, uint32_t a, uint32_t b,
-                                          const uint8_t* src) {
-  if (a >= b) return;
-  const int32_t A = (int32_t)((a + ph4 + 3) & ~3u) - (int32_t)ph4;  // first whole word's start
-  const int32_t B = (int32_t)((b + ph4) & ~3u) - (int32_t)ph4;      // last whole word's end
-  if (A + 4 <= B) {
-    for (uint32_t p = a; p < (uint32_t)A; p++) dst[p] = __ldg(src + (p - a));
-    for (uint32_t p = (uint32_t)B; p < b; p++) dst[p] = __ldg(src + (p - a));
-  } else {
-    for (uint32_t p = a; p < b; p++) dst[p] = __ldg(src + (p - a));
-  }
-}
-
-__global__ void __launch_bounds__(kEncWarps * 32, 5) k_encode_blocks(const JobDev* __restrict__ jobs) {
+__global__ void __launch_bounds__(kEncWarps * 32, 2) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t enc_smem[];
   uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
@@ -688,159 +677,140 @@ __global__ void __launch_bounds__(kEncWarps * 32, 5) k_encode_blocks(const JobDe
     const uint32_t bsz = J.b_size[b];
     const uint64_t s = J.b_first[b];
     const uint32_t n = (uint32_t)(J.b_first[b + 1] - s);
-    if (n > kEncMaxEnt) {
+    const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+    if (n > kEncMaxEnt || ph + bsz + kTrailer + 16 > kEncStage) {
       enc_direct(J, tab4, b, dst, lane);
       continue;
     }
-    // entry table
-    uint32_t carry = 0;
+    uint8_t* st = W.stage;
+    // 1. entry table
+    uint32_t carry = 0, ccarry = 0;
     for (uint32_t j0 = 0; j0 < n; j0 += 32) {
       const uint32_t j = j0 + lane;
-      uint32_t size = 0, hl = 0;
+      uint32_t size = 0, hl = 0, kd = 0, vl = 0;
       if (j < n) {
         const uint64_t k = s + j;
         const uint32_t kl = J.k_klen[k];
         const uint32_t sh = (j % R == 0) ? 0 : J.k_shared[k];
-        const uint32_t kd = kl - sh, vl = J.k_vlen[k];
-        const uint32_t koff = J.k_koff[k], voff = J.k_voff[k];
+        kd = kl - sh;
+        vl = J.k_vlen[k];
         hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
         size = hl + kd + vl;
-        W.ksrc[j] = koff + sh;
-        W.vsrc[j] = voff;
+        W.ksrc[j] = J.k_koff[k] + sh;
+        W.vsrc[j] = J.k_voff[k];
         W.kd[j] = kd;
         W.vl[j] = vl;
         W.sh[j] = sh;
-        // start the source lines on their way to L1
-        prefetch_l1(keys + koff + sh, kd);
-        prefetch_l1(in + voff, vl);
       }
       uint32_t tot;
       const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
+      uint32_t nq = 0;
       if (j < n) {
         W.off[j] = ex;
         W.kbeg[j] = ex + hl;
+        uint32_t first;
+        if (kd >= kEncLong) nq += chunks_in(ph + ex + hl, ph + ex + hl + kd, &first);
+        if (vl >= kEncLong) nq += chunks_in(ph + ex + hl + kd, ph + ex + size, &first);
         if (J.dec_vpos)  // the value's place in its file, for the decoded form
-          J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + W.kd[j]);
+          J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + kd);
       }
+      uint32_t ctot;
+      const uint32_t cx = warp_excl<uint32_t>(nq, &ctot) + ccarry;
+      if (j < n) W.cc[j] = cx;
       carry += tot;
+      ccarry += ctot;
     }
-    if (lane == 0) W.off[n] = carry;
+    if (lane == 0) {
+      W.off[n] = carry;
+      W.cc[n] = ccarry;
+    }
     __syncwarp();
     const uint32_t rbase = carry;  // restart array, then the restart count
     const uint32_t nrest = (n + R - 1) / R;
-    const uint32_t ph4 = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 3);
-    // 1. whole words inside one key delta or value, kEncBatch words per lane
-    //    at a time: every source load of the batch is in flight before the
-    //    first is used
-    {
-      uint32_t* gw = reinterpret_cast<uint32_t*>(dst - ph4);
-      const uint32_t nwords = (ph4 + rbase + 3) >> 2;
-      uint32_t j = 0;
-      for (uint32_t w0 = lane; w0 < nwords; w0 += 32 * kEncBatch) {
-        const uint32_t* s4[kEncBatch];
-        uint32_t sh8[kEncBatch];
-        bool ok[kEncBatch];
-#pragma unroll
-        for (uint32_t u = 0; u < kEncBatch; u++) {
-          const uint32_t w = w0 + 32 * u;
-          const int32_t pi = (int32_t)(4 * w) - (int32_t)ph4;
-          ok[u] = false;
-          s4[u] = nullptr;
-          sh8[u] = 0;
-          if (w < nwords && pi >= 0 && (uint32_t)pi + 4 <= rbase) {
-            const uint32_t p = (uint32_t)pi;
-            while (W.off[j + 1] <= p) j++;
-            const uint32_t kb = W.kbeg[j], kd = W.kd[j];
-            const uint8_t* src = nullptr;
-            if (p >= kb && p + 4 <= kb + kd) src = keys + W.ksrc[j] + (p - kb);
-            else if (p >= kb + kd && p + 4 <= W.off[j + 1]) src = in + W.vsrc[j] + (p - kb - kd);
-            if (src) {
-              const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
-              s4[u] = reinterpret_cast<const uint32_t*>(sa & ~uintptr_t(3));
-              sh8[u] = 8 * (uint32_t)(sa & 3);
-              ok[u] = true;
-            }
-          }
-        }
-        uint32_t x0[kEncBatch], x1[kEncBatch];
-#pragma unroll
-        for (uint32_t u = 0; u < kEncBatch; u++) {
-          x0[u] = ok[u] ? __ldg(s4[u]) : 0u;
-          x1[u] = (ok[u] && sh8[u]) ? __ldg(s4[u] + 1) : 0u;
-        }
-#pragma unroll
-        for (uint32_t u = 0; u < kEncBatch; u++)
-          if (ok[u]) gw[w0 + 32 * u] = __funnelshift_r(x0[u], x1[u], sh8[u]);
-      }
-    }
-    // 2. headers, segment edges, restart words
+    // 2. headers, short stretches, edges, restart words
     for (uint32_t j = lane; j < n; j += 32) {
-      const uint32_t o = W.off[j], kb = W.kbeg[j], kd = W.kd[j], vl = W.vl[j], sh = W.sh[j];
-      for (uint32_t p = o; p < kb; p++) dst[p] = (uint8_t)header_byte(sh, kd, vl, p - o);
-      enc_edges(dst, ph4, kb, kb + kd, keys + W.ksrc[j]);
-      enc_edges(dst, ph4, kb + kd, W.off[j + 1], in + W.vsrc[j]);
+      const uint32_t o = W.off[j], kb = W.kbeg[j], kd = W.kd[j], vl = W.vl[j];
+      uint8_t* p = st + ph + o;
+      p = put_varint(p, W.sh[j]);
+      p = put_varint(p, kd);
+      put_varint(p, vl);
+      stretch_bytes(st, ph + kb, ph + kb + kd, keys + W.ksrc[j], kd >= kEncLong);
+      stretch_bytes(st, ph + kb + kd, ph + kb + kd + vl, in + W.vsrc[j], vl >= kEncLong);
       if (j % R == 0) {
         const uint32_t rem = n - j;
-        st_le32(dst + rbase + 4 * (j / R), (o << 8) | (rem < R ? rem : R));
+        st_le32(st + ph + rbase + 4 * (j / R), (o << 8) | (rem < R ? rem : R));
       }
     }
-    if (lane == 0) st_le32(dst + bsz - 4, nrest);
-    __syncwarp();
-    // 3. CRC32C over the block read back, lanes over contiguous 16-byte chunks
-    const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
-    const uint8_t* gbase = dst - ph;
-    const uint32_t nch = (ph + bsz + 15) >> 4;
-    const uint32_t per = (nch + 31) >> 5;
-    const uint32_t c0 = lane * per, c1 = min(nch, c0 + per);
-    const int32_t pb = (int32_t)(16 * c0) - (int32_t)ph;
-    const uint32_t seg_b = pb < 0 ? 0u : (uint32_t)pb;
-    const uint32_t seg_e = c0 < c1 ? min(bsz, 16 * c1 - ph) : seg_b;
-    // the two shift factors x^(8n) are fetched first, to arrive meanwhile
-    const uint32_t total = bsz + 1;
-    const bool last = seg_b < seg_e && seg_e == bsz;  // this lane appends the type byte
-    const uint32_t e_end = last ? total : seg_e;
-    const uint32_t f_lane = seg_b < e_end ? crc_xpow8(J, total - e_end) : 0u;
-    const uint32_t f_init = lane == 0 ? crc_xpow8(J, total) : 0u;
-    uint32_t crc = 0;
-    for (uint32_t cb = c0; cb < c1; cb += 4) {
-      uint4 v[4];
+    if (lane == 0) {
+      st_le32(st + ph + bsz - 4, nrest);
+      st[ph + bsz] = 0;  // kNoCompression
+    }
+    // 3. the long stretches' chunks
+    const uint32_t nchunks = W.cc[n];
+    for (uint32_t c0 = lane; c0 < nchunks; c0 += 32 * kEncChunks) {
+      uint32_t w[kEncChunks][5];
+      uint32_t sh8[kEncChunks], at[kEncChunks];
 #pragma unroll
-      for (uint32_t u = 0; u < 4; u++) {
-        const uint32_t c = cb + u;
-        const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
-        v[u] = (c < c1 && p0 >= 0 && (uint32_t)p0 + 16 <= bsz)
-                   ? __ldcg(reinterpret_cast<const uint4*>(gbase + 16 * c))
-                   : make_uint4(0, 0, 0, 0);
-      }
-#pragma unroll
-      for (uint32_t u = 0; u < 4; u++) {
-        const uint32_t c = cb + u;
-        if (c >= c1) break;
-        const int32_t p0 = (int32_t)(16 * c) - (int32_t)ph;
-        if (p0 >= 0 && (uint32_t)p0 + 16 <= bsz) {
-          const uint32_t x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            crc ^= x[i];
-            crc = tab4[768 + (crc & 0xff)] ^ tab4[512 + ((crc >> 8) & 0xff)] ^
-                  tab4[256 + ((crc >> 16) & 0xff)] ^ tab4[crc >> 24];
+      for (uint32_t u = 0; u < kEncChunks; u++) {
+        const uint32_t c = c0 + 32 * u;
+        at[u] = 0xffffffffu;
+        if (c < nchunks) {
+          // the entry holding chunk c: last j with cc[j] <= c
+          uint32_t lo = 0, hi = n;
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (W.cc[mid] <= c) lo = mid;
+            else hi = mid;
           }
-        } else {
-          const uint32_t q0 = p0 < 0 ? 0u : (uint32_t)p0;
-          const uint32_t q1 = min(bsz, (uint32_t)(p0 + 16));
-          for (uint32_t q = q0; q < q1; q++) crc = tab4[(crc ^ __ldcg(dst + q)) & 0xff] ^ (crc >> 8);
+          const uint32_t j = lo, kb = W.kbeg[j], kd = W.kd[j];
+          uint32_t q = c - W.cc[j], first, nq = 0;
+          if (kd >= kEncLong) nq = chunks_in(ph + kb, ph + kb + kd, &first);
+          const uint8_t* src;
+          if (q < nq) {
+            src = keys + W.ksrc[j] + (first + 16 * q - (ph + kb));
+          } else {
+            q -= nq;
+            chunks_in(ph + kb + kd, ph + kb + kd + W.vl[j], &first);
+            src = in + W.vsrc[j] + (first + 16 * q - (ph + kb + kd));
+          }
+          at[u] = first + 16 * q;
+          const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+          const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+          sh8[u] = 8 * (uint32_t)(a & 3);
+#pragma unroll
+          for (int i = 0; i < 4; i++) w[u][i] = __ldg(base + i);
+          // the fifth word holds needed bytes only when the source is not
+          // word aligned (never read past the stretch)
+          w[u][4] = sh8[u] ? __ldg(base + 4) : 0u;
         }
       }
-    }
-    // the zero type byte closes the CRC; lanes combine their registers
-    if (last) crc = tab4[crc & 0xff] ^ (crc >> 8);
-    uint32_t v = seg_b < e_end ? gf2_mulmod(f_lane, crc) : 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) {
-      const uint32_t full = v ^ gf2_mulmod(f_init, 0xffffffffu) ^ 0xffffffffu;
-      dst[bsz] = 0;  // kNoCompression
-      st_le32(dst + bsz + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
+      for (uint32_t u = 0; u < kEncChunks; u++) {
+        if (at[u] == 0xffffffffu) continue;
+        uint4 v;
+        v.x = __funnelshift_r(w[u][0], w[u][1], sh8[u]);
+        v.y = __funnelshift_r(w[u][1], w[u][2], sh8[u]);
+        v.z = __funnelshift_r(w[u][2], w[u][3], sh8[u]);
+        v.w = __funnelshift_r(w[u][3], w[u][4], sh8[u]);
+        *reinterpret_cast<uint4*>(st + at[u]) = v;
+      }
+    }
+    __syncwarp();
+    // 4. CRC32C of the block and its type byte
+    const uint32_t crc = warp_block_crc_smem(J, tab4, st + ph, bsz);
+    if (lane == 0) st_le32(st + ph + bsz + 1, crc);
+    __syncwarp();
+    // 5. block and trailer out
+    const uint32_t end = ph + bsz + kTrailer;
+    uint8_t* gbase = dst - ph;
+    const uint32_t nch = (end + 15) >> 4;
+    for (uint32_t c = lane; c < nch; c += 32) {
+      const uint32_t a = 16 * c;
+      if (a >= ph && a + 16 <= end) {
+        *reinterpret_cast<uint4*>(gbase + a) = *reinterpret_cast<const uint4*>(st + a);
+      } else {
+        for (uint32_t x = max(a, ph); x < min(a + 16, end); x++) gbase[x] = st[x];
+      }
     }
     __syncwarp();
   }
@@ -988,13 +958,13 @@ __global__ void k_encode_index(const JobDev* __restrict__ jobs) {
 // Metaindex, footer and the tail of the filter block's offset array (thread
 // 0), then the trailers of the filter, metaindex and index blocks, each a
 // CRC32C over the whole CTA: one CTA per output file.
-__global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
+__global__ void __launch_bounds__(1024) k_encode_meta(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
-  __shared__ uint32_t tab[256];
+  __shared__ uint32_t tab4[4 * 256];
   __shared__ uint32_t s_x[32];
   __shared__ uint32_t s_skip;
   if (threadIdx.x == 0) s_skip = J.ctr->error || blockIdx.x >= J.ctr->n_files;
-  crc_table_init(tab);
+  crc_tables4_init(tab4);
   __syncthreads();
   if (s_skip) return;
   const uint32_t f = blockIdx.x;
@@ -1052,13 +1022,16 @@ __global__ void k_encode_meta(const JobDev* __restrict__ jobs) {
     const uint64_t len = which == 0 ? F.filter_size : (which == 1 ? F.meta_size : F.index_size);
     uint8_t* p = J.out + F.out_off + off;
     const uint64_t total = len + 1;
-    const uint64_t seg = (total + blockDim.x - 1) / blockDim.x;
+    // contiguous stretches of whole words per thread (the last thread also
+    // takes the type byte, which is 0 for these blocks)
+    const uint64_t seg = ((total + blockDim.x - 1) / blockDim.x + 3) & ~uint64_t(3);
     const uint64_t b = (uint64_t)threadIdx.x * seg;
     const uint64_t e = min(total, b + seg);
     uint32_t c = 0;
-    for (uint64_t i = b; i < e; i++) {
-      const uint8_t byte = i < len ? p[i] : 0;
-      c = tab[(c ^ byte) & 0xff] ^ (c >> 8);
+    if (b < e) {
+      const uint64_t e_data = min(e, len);
+      if (e_data > b) c = crc_raw4(tab4, 0, p + b, (uint32_t)(e_data - b));
+      if (e > len) c = tab4[c & 0xff] ^ (c >> 8);  // the type byte
     }
     uint32_t v = b < total ? crc_shift(J, c, total - e) : 0;
 #pragma unroll
@@ -1125,7 +1098,7 @@ void encode_kernel_attributes() {
 void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
   // grid-stride over the device-side block count: 5 CTAs per SM x 4 waves,
   // shared out among the jobs
-  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 5 * 4)),
+  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 2 * 4)),
                                         bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);
 }
 void launch_emit_decoded(const Batch& bt, cudaStream_t st) {
@@ -1143,7 +1116,7 @@ void launch_encode_index(const Batch& bt, cudaStream_t st) {
                                   0, st>>>(bt.d);
 }
 void launch_encode_meta(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 1024, 0, st>>>(bt.d);
 }
 
 }  // namespace lc
