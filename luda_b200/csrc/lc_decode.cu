@@ -761,6 +761,191 @@ __device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const 
   return true;
 }
 
+// One block (warp per block): a decoded-run pseudo block, or a staged block,
+// or, when it does not fit the stage, the direct path.
+__device__ __forceinline__ void decode_one(const JobDev& J, uint64_t b, uint32_t lane,
+                                           DecWarpSmem& W) {
+  if (J.blk_size[b] == kPseudoBlock) {
+    uint64_t kb;
+    uint32_t mk;
+    if (!__all_sync(0xffffffffu, pseudo_entries(J, b, J.blk_ent_base[b], lane, 32, &kb, &mk))) {
+      if (lane == 0) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
+      return;
+    }
+    uint64_t kbase = 0;
+    if (J.reserve_keys) {
+      // single pass: reserve the block's key bytes in the arena
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+      int retry = 0;
+      if (lane == 0) {
+        atomicMax(&J.ctr->max_klen, mk);
+        if (mk > J.max_key_len) {
+          retry = 1;
+        } else {
+          kbase = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
+          retry = kbase + kb > J.cap_key_bytes;
+        }
+        if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+      }
+      if (__shfl_sync(0xffffffffu, retry, 0)) return;
+      kbase = __shfl_sync(0xffffffffu, kbase, 0);
+    } else {
+      kbase = J.blk_key_base[b];
+    }
+    pseudo_keys(J, b, J.blk_ent_base[b], kbase, lane);
+    return;
+  }
+  const uint8_t* st = stage_block(J, b, W.stage, lane);
+  if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
+  __syncwarp();
+}
+
+// Sparse blocks: few entries with long values (the job's blocks average at
+// most kSparseEnt entries, the block at most 64 KiB).  Staging them would
+// move every value byte for a few header and key bytes, so a warp takes
+// kSparseGroup consecutive blocks: each lane walks its block's restart runs
+// straight from global memory (headers only), recording every entry in the
+// warp's arrays; one atomic reserves all their key spans; then the warp
+// rebuilds each block's keys (shared prefix from the previous key, delta
+// from global memory) and writes keys and descriptors.  Blocks that are not
+// sparse in such a group go through decode_one.
+constexpr uint32_t kSparseEnt = 8;
+constexpr uint32_t kSparseGroup = 32;
+
+__device__ __forceinline__ bool sparse_block(const JobDev& J, uint64_t b) {
+  const uint32_t size = J.blk_size[b], nent = J.blk_nent[b];
+  return size != kPseudoBlock && size <= 0xffff && nent > 0 && nent <= kSparseEnt &&
+         size >= 128u * nent;
+}
+
+__device__ void decode_sparse_group(const JobDev& J, uint64_t g0, uint64_t nblk, uint32_t lane,
+                                    DecWarpSmem& W) {
+  const uint64_t b = g0 + lane;
+  const bool mine = b < nblk && sparse_block(J, b);
+  const unsigned mask = __ballot_sync(0xffffffffu, mine);
+  // 1. one lane per sparse block: headers from global memory
+  bool bad = false, short_key = false;
+  uint32_t kb = 0, maxk = 0, nent = 0;
+  if (mine) {
+    const uint8_t* p = J.in + J.blk_off[b];
+    const uint32_t size = J.blk_size[b];
+    const uint32_t nr = ld_le32(p + size - 4);  // checked by k_block_restarts
+    const uint32_t ra = size - 4 - 4 * nr;
+    nent = J.blk_nent[b];
+    uint32_t e = 0;
+    for (uint32_t r = 0; r < nr && !bad; r++) {
+      const uint32_t w = ld_le32(p + ra + 4 * r);
+      const uint32_t cnt = w & 0xff;
+      const uint8_t* q = p + (w >> 8);
+      const uint8_t* lim = p + ((r + 1 < nr) ? (ld_le32(p + ra + 4 * (r + 1)) >> 8) : ra);
+      uint32_t prev = 0;
+      for (uint32_t k = 0; k < cnt; k++) {
+        uint32_t sh, ns, vl;
+        const uint8_t* d = entry_header(q, lim, &sh, &ns, &vl);
+        if (!d || (k == 0 && sh != 0) || sh > prev || e >= nent) {
+          bad = true;
+          break;
+        }
+        const uint32_t kl = sh + ns;
+        if (kl < 8) short_key = true;
+        const uint32_t x = lane * kSparseEnt + e;
+        W.dpos[x] = (uint16_t)(d - p);
+        W.sh[x] = (uint16_t)sh;
+        W.kl[x] = (uint16_t)kl;
+        W.vl[x] = (uint16_t)vl;
+        kb += kl;
+        maxk = max(maxk, kl);
+        prev = kl;
+        q = d + ns + vl;
+        e++;
+      }
+      if (!bad && q != lim) bad = true;
+    }
+    if (!bad && e != nent) bad = true;
+    if (bad) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
+    else if (short_key) set_error(J.ctr, kErrShortKey, (uint32_t)b);
+    else if (J.reserve_keys && maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
+    atomicMax(&J.ctr->max_klen, maxk);
+  }
+  // 2. key spans: one reservation for the group (single pass), else the scan's
+  const bool ok = mine && !bad && !short_key && (!J.reserve_keys || maxk <= J.max_key_len);
+  const uint32_t need = ok ? kb : 0;
+  uint64_t kbase = 0;
+  if (J.reserve_keys) {
+    uint32_t tot;
+    const uint32_t ex = warp_excl<uint32_t>(need, &tot);
+    uint64_t base = 0;
+    if (lane == 0 && tot)
+      base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)tot);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (tot && base + tot > J.cap_key_bytes) {
+      if (lane == 0) set_error(J.ctr, kErrRetryExact, (uint32_t)g0);
+      return;
+    }
+    kbase = base + ex;
+  } else if (mine) {
+    kbase = J.blk_key_base[b];
+  }
+  __syncwarp();
+  // 3. per sparse block: keys rebuilt in entry order, descriptors
+  const unsigned done = __ballot_sync(0xffffffffu, ok);
+  for (unsigned m = done; m; m &= m - 1) {
+    const uint32_t L = __ffs(m) - 1;
+    const uint64_t bb = g0 + L;
+    const uint32_t n = __shfl_sync(0xffffffffu, nent, L);
+    const uint64_t kb0 = __shfl_sync(0xffffffffu, kbase, L);
+    const uint8_t* p = J.in + J.blk_off[bb];
+    const uint32_t voff0 = (uint32_t)J.blk_off[bb];
+    const uint64_t ebase = J.blk_ent_base[bb];
+    uint8_t* kbuf = W.keybuf;  // at most kSparseEnt keys of at most 256 bytes (single pass)
+    uint32_t kofs = 0, pofs = 0;
+    const bool fits = __shfl_sync(0xffffffffu, kb, L) <= kDecKeyBuf;
+    uint8_t* gdst = J.keys + kb0;
+    for (uint32_t x = 0; x < n; x++) {
+      const uint32_t i = L * kSparseEnt + x;
+      const uint32_t esh = W.sh[i], ekl = W.kl[i], edp = W.dpos[i];
+      if (fits) {
+        uint8_t* d = kbuf + kofs;
+        for (uint32_t t = lane; t < ekl; t += 32)
+          d[t] = t < esh ? kbuf[pofs + t] : __ldg(p + edp + t - esh);
+      } else {
+        // longer keys (exact reruns): built in place in the arena, one key at a time
+        uint8_t* d = gdst + kofs;
+        for (uint32_t t = lane; t < ekl; t += 32) d[t] = t < esh ? gdst[pofs + t] : p[edp + t - esh];
+      }
+      __syncwarp();
+      if (lane == 0) {
+        const uint64_t e = ebase + x;
+        J.e_koff[e] = (uint32_t)(kb0 + kofs);
+        J.e_klen[e] = ekl;
+        J.e_voff[e] = voff0 + edp + (ekl - esh);
+        J.e_vlen[e] = W.vl[i];
+      }
+      pofs = kofs;
+      kofs += ekl;
+    }
+    __syncwarp();
+    if (fits) {
+      for (uint32_t t = lane; t < kofs; t += 32) gdst[t] = kbuf[t];
+    }
+    // prefixes and tags, one lane per entry
+    if (lane < n) {
+      const uint32_t i = L * kSparseEnt + lane;
+      uint32_t o = 0;
+      for (uint32_t x = 0; x < lane; x++) o += W.kl[L * kSparseEnt + x];
+      const uint8_t* k = fits ? kbuf + o : gdst + o;
+      const uint32_t kl = W.kl[i];
+      J.e_pfx[ebase + lane] = user_prefix(k, kl);
+      J.e_tag[ebase + lane] = ld_le64(k + kl - 8);
+    }
+    __syncwarp();
+  }
+  // 4. the group's other blocks
+  const unsigned rest = __ballot_sync(0xffffffffu, b < nblk && !mine);
+  for (unsigned m = rest; m; m &= m - 1) decode_one(J, g0 + (__ffs(m) - 1), lane, W);
+}
+
 __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t dec_smem[];
@@ -768,43 +953,15 @@ __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* _
   DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
   if (J.ctr->error) return;
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
-       b += (uint64_t)gridDim.x * kDecWarps) {
-    if (J.blk_size[b] == kPseudoBlock) {
-      uint64_t kb;
-      uint32_t mk;
-      if (!__all_sync(0xffffffffu, pseudo_entries(J, b, J.blk_ent_base[b], lane, 32, &kb, &mk))) {
-        if (lane == 0) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
-        continue;
-      }
-      uint64_t kbase = 0;
-      if (J.reserve_keys) {
-        // single pass: reserve the block's key bytes in the arena
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
-        int retry = 0;
-        if (lane == 0) {
-          atomicMax(&J.ctr->max_klen, mk);
-          if (mk > J.max_key_len) {
-            retry = 1;
-          } else {
-            kbase = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
-            retry = kbase + kb > J.cap_key_bytes;
-          }
-          if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-        }
-        if (__shfl_sync(0xffffffffu, retry, 0)) continue;
-        kbase = __shfl_sync(0xffffffffu, kbase, 0);
-      } else {
-        kbase = J.blk_key_base[b];
-      }
-      pseudo_keys(J, b, J.blk_ent_base[b], kbase, lane);
-      continue;
-    }
-    const uint8_t* st = stage_block(J, b, W.stage, lane);
-    if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
-    __syncwarp();
+  if (J.sparse_blocks) {
+    for (uint64_t g = (uint64_t)blockIdx.x * kDecWarps + warp; g * kSparseGroup < nblk;
+         g += (uint64_t)gridDim.x * kDecWarps)
+      decode_sparse_group(J, g * kSparseGroup, nblk, lane, W);
+    return;
   }
+  for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
+       b += (uint64_t)gridDim.x * kDecWarps)
+    decode_one(J, b, lane, W);
 }
 
 __global__ void k_entries_from_offsets(const JobDev* __restrict__ jobs) {

@@ -108,42 +108,69 @@ __global__ void k_sizes(const JobDev* __restrict__ jobs) {
   }
 }
 
-__device__ __forceinline__ void next_one(const JobDev& J, uint64_t s, uint64_t n) {
+// TableBuilder's size estimate of a block [s, e] (buffer + 4 per restart +
+// 4): the prefix-compressed sizes (k_pb, a prefix sum of k_b) plus, at every
+// restart s + mR, the difference between the entry's restart size and its
+// compressed size, plus the restart words.  `D` is that difference summed
+// over the restarts up to segment m (the segment holding e).
+__device__ __forceinline__ uint64_t block_est(const JobDev& J, uint64_t s, uint64_t e, uint64_t D,
+                                              uint64_t m) {
+  return J.k_pb[e + 1] - J.k_pb[s] + D + 4 * (m + 1) + 4;
+}
+
+// next(s): the first survivor of the block after the one that starts at s.
+// The block ends after the first e whose estimate reaches block_size
+// (TableBuilder::Add, table/table_builder.cc:120-123), or before the first
+// grandparent cut after s, or at the end.  Restart segments (R survivors)
+// are stepped through, then the segment that reaches block_size is binary
+// searched: O(block / R + log R) loads instead of a walk over the block.
+__device__ __forceinline__ uint64_t next_of(const JobDev& J, uint64_t s, uint64_t n) {
   const uint32_t R = J.restart_interval;
   const uint64_t bs = J.block_size;
-  uint64_t buf = 0;
-  uint64_t e = s;
-  uint32_t j = 0;
-  uint64_t nxt;
-  while (true) {
-    if (e >= n) {
-      nxt = n;
-      break;
-    }
-    if (j > 0 && J.k_forced[e]) {
-      nxt = e;
-      break;
-    }
-    buf += (j % R == 0) ? J.k_a[e] : J.k_b[e];
-    const uint64_t est = buf + 4ull * (1 + j / R) + 4;
-    if (est >= bs) {
-      nxt = e + 1;
-      break;
-    }
-    j++;
-    e++;
+  uint32_t lo = 0, hi = J.ctr->n_triggers;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (J.t_kept[mid] <= s) lo = mid + 1;
+    else hi = mid;
   }
-  J.k_next[s] = (uint32_t)nxt;
-  atomicMax(&J.ctr->max_jump, (uint32_t)(nxt - s));
+  const uint64_t limit = lo < J.ctr->n_triggers ? min(n, (uint64_t)J.t_kept[lo]) : n;
+  uint64_t D = 0;
+  for (uint64_t m = 0;; m++) {
+    const uint64_t a = s + m * R;
+    if (a >= limit) return limit;
+    D += J.k_a[a] - J.k_b[a];
+    const uint64_t z = min(a + R, limit);  // segment [a, z)
+    if (block_est(J, s, z - 1, D, m) >= bs) {
+      uint64_t l = a, h = z - 1;
+      while (l < h) {
+        const uint64_t mid = (l + h) >> 1;
+        if (block_est(J, s, mid, D, m) >= bs) h = mid;
+        else l = mid + 1;
+      }
+      return l + 1;
+    }
+  }
 }
 
 __global__ void k_next(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   if (J.ctr->error) return;  // a failed job does no more work
   const uint64_t n = J.ctr->n_kept;
-  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (uint64_t)gridDim.x * blockDim.x)
-    next_one(J, s, n);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t s0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t w0 = s0 - (threadIdx.x & 31);
+  const uint64_t trips = n > w0 ? (n - w0 + stride - 1) / stride : 0;
+  uint32_t jump = 0;
+  for (uint64_t it = 0, s = s0; it < trips; it++, s += stride) {
+    if (s < n) {
+      const uint64_t nxt = next_of(J, s, n);
+      J.k_next[s] = (uint32_t)nxt;
+      jump = max(jump, (uint32_t)(nxt - s));
+    }
+  }
+  // the longest block, one atomic per warp
+  jump = __reduce_max_sync(0xffffffffu, jump);
+  if ((threadIdx.x & 31) == 0 && jump) atomicMax(&J.ctr->max_jump, jump);
 }
 
 
@@ -308,10 +335,10 @@ __global__ void k_block_list(const JobDev* __restrict__ jobs) {
       const uint32_t b = J.k_block[k];
       J.b_first[b] = (uint32_t)k;
       const uint64_t e = J.k_next[k];
-      uint64_t sum = 0;
-      for (uint64_t j = 0; j < e - k; j++) sum += (j % R == 0) ? J.k_a[k + j] : J.k_b[k + j];
+      uint64_t D = 0;
+      for (uint64_t a = k; a < e; a += R) D += J.k_a[a] - J.k_b[a];
       const uint64_t nrest = (e - k + R - 1) / R;
-      const uint32_t size = (uint32_t)(sum + 4 * nrest + 4);
+      const uint32_t size = (uint32_t)(J.k_pb[e] - J.k_pb[k] + D + 4 * nrest + 4);
       J.b_size[b] = size;
       J.tmp32[b] = size + kTrailer;
     }
@@ -905,15 +932,60 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
   }
 }
 
+// A filter group whose filter has at most kFilterLocal bytes, by one thread:
+// the bits in a thread-local array, then byte stores.
+constexpr uint32_t kFilterLocal = 128;
+__device__ __forceinline__ void filter_group_thread(const JobDev& J, uint64_t b, uint32_t gb) {
+  const FileOut& F = J.files[J.b_file[b]];
+  const uint32_t fb0 = F.first_block, fb1 = F.end_block;
+  uint8_t* fbase = J.out + F.out_off + F.filter_off;
+  const uint64_t Ft = J.b_gcum[fb1] - J.b_gcum[fb0];
+  uint8_t* fdst = fbase + (J.b_gcum[b] - J.b_gcum[fb0]);
+  const uint32_t nbytes = gb - 1;
+  const uint32_t bits = nbytes * 8;
+  uint32_t w[kFilterLocal / 4];
+#pragma unroll
+  for (uint32_t i = 0; i < kFilterLocal / 4; i++) w[i] = 0;
+  const uint64_t k0 = J.b_first[b];
+  const uint32_t nk = J.b_gkeys[b];
+  for (uint32_t i = 0; i < nk; i++) {
+    uint32_t kl;
+    const uint8_t* key = kept_key(J, k0 + i, &kl);
+    uint32_t h = leveldb_hash(key, kl - 8, 0xbc9f1d34u);
+    const uint32_t delta = (h >> 17) | (h << 15);
+    for (uint32_t q = 0; q < J.bloom_k; q++) {
+      const uint32_t bitpos = h % bits;
+      w[bitpos >> 5] |= 1u << (bitpos & 31);  // byte bitpos/8, bit bitpos%8
+      h += delta;
+    }
+  }
+  for (uint32_t i = 0; i < nbytes; i++) fdst[i] = (uint8_t)(w[i >> 2] >> (8 * (i & 3)));
+  fdst[nbytes] = (uint8_t)J.bloom_k;
+  // filter offsets of the empty indices before this group and of the group
+  const uint64_t jb = J.b_off[b] >> kFilterBaseLg;
+  const int64_t jprev = (b == fb0) ? -1 : (int64_t)(J.b_off[b - 1] >> kFilterBaseLg);
+  const uint32_t val = (uint32_t)(J.b_gcum[b] - J.b_gcum[fb0]);
+  for (int64_t jj = jprev + 1; jj <= (int64_t)jb; jj++) st_le32(fbase + Ft + 4 * jj, val);
+}
+
+// Filter groups (at their first blocks): small filters one per thread, larger
+// ones one per warp (bits in the warp's shared memory, or in place).
 __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_filter[8][kFilterSmem / 4];  // blockDim 256: 8 warps
   const uint32_t lane = threadIdx.x & 31;
   if (J.bits_per_key <= 0 || J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t gb = J.b_gbytes[b];
+    if (gb != 0 && gb - 1 <= kFilterLocal) filter_group_thread(J, b, gb);
+  }
   const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride)
-    encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
+  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride) {
+    const uint32_t gb = J.b_gbytes[b];
+    if (gb != 0 && gb - 1 > kFilterLocal) encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
+  }
 }
 
 __device__ __forceinline__ void encode_index_entry(const JobDev& J, uint64_t b) {
@@ -1108,7 +1180,7 @@ void launch_emit_decoded(const Batch& bt, cudaStream_t st) {
                                   0, st>>>(bt.d);
 }
 void launch_encode_filters(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries * 32, 256, per_job(bt, 148 * 16)), bt.B),
+  note_launch(), k_encode_filters<<<dim3(grid_x(bt.max_entries, 256, per_job(bt, 148 * 8)), bt.B),
                                     256, 0, st>>>(bt.d);
 }
 void launch_encode_index(const Batch& bt, cudaStream_t st) {

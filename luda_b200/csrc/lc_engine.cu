@@ -576,6 +576,7 @@ void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer
     T.mark(kDrop);
   }
   launch_sizes(bt, st);
+  scan_batch(kScanKb, bt, bt.max_entries, st);
   launch_next(bt, st);
   launch_chain(bt, st);
   scan_batch(kScanBstart, bt, bt.max_entries, st);
@@ -651,6 +652,8 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
   J.files = A.get<FileOut>(J.cap_files);
   J.b_fnext = A.get<uint32_t>(N);
   J.t_blocks = A.get<uint32_t>(J.cap_triggers);
+  J.t_kept = A.get<uint32_t>(J.cap_triggers);
+  J.k_pb = A.get<uint64_t>(N + 1);
   J.b_file = A.get<uint32_t>(N);
   J.b_off = A.get<uint64_t>(N);
   J.b_isize = A.get<uint32_t>(N);
@@ -1164,6 +1167,10 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       }
       r.J.reserve_keys = exact ? 0 : 1;
       r.J.max_key_len = kFastMaxKey;
+      // blocks of a few entries each (long values): decoded in groups without
+      // staging the values
+      r.J.sparse_blocks = !r.failed && hc[i].n_blocks_in > 0 &&
+                          hc[i].n_entries_in <= 6 * hc[i].n_blocks_in;
       r.j->entries_in = r.N;
       r.j->key_bytes_in = exact ? r.K : 0;
     }
@@ -1531,7 +1538,7 @@ void run_build(lc_job* j, lc_slot& slot) {
 // (the at-size workloads have 67-250 bytes per entry) and the worker trues
 // the charge up to the batch's real allocation once the counts are known.
 constexpr uint64_t kEstEntryBytes = 40;
-constexpr uint64_t kEntryArrayBytes = 224;  // per-entry arrays of alloc_tail, rounded up
+constexpr uint64_t kEntryArrayBytes = 232;  // per-entry arrays of alloc_tail, rounded up
 uint64_t estimate_bytes(const lc_job* j) {
   uint64_t in = 0;
   for (auto& t : j->tables) in += round16(t.size);

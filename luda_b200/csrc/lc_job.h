@@ -201,6 +201,7 @@ struct JobDev {
   uint32_t reserve_keys;     // 1: decode reserves key-arena space per block (single
                              // pass, restart counts only); 0: blk_key_base from counting
   uint32_t max_key_len;      // 1: longest key the single-pass layout allows
+  uint32_t sparse_blocks;    // the blocks average few entries: decode them in groups
 
   // output blocks
   uint32_t* b_first;         // first kept entry of block (cap_blocks_out + 1)
@@ -219,6 +220,8 @@ struct JobDev {
   uint32_t* b_gkeys;         // keys in the group (at group starts)
   uint32_t* b_fnext;         // first block of the next file if a file starts here
   uint32_t* t_blocks;        // output block starting at each grandparent cut
+  uint32_t* t_kept;          // survivor position of each grandparent cut (ascending)
+  uint64_t* k_pb;            // n_kept + 1: prefix sums of k_b (block size estimates)
   uint64_t cap_blocks_out;
 
   // files

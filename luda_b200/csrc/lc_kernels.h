@@ -69,6 +69,7 @@ enum ScanSel : int {
   kScanGcum,           // b_gbytes -> b_gcum
   kScanIcum,           // b_isize -> b_icum
   kScanDecKey,         // k_klen -> dec_kcum (jobs that keep their decoded form)
+  kScanKb,             // k_b -> k_pb (block size estimates)
 };
 void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st);
 uint64_t scan_scratch_elems(uint64_t n_cap);

@@ -376,6 +376,7 @@ __global__ void k_forced(const JobDev* __restrict__ jobs) {
   if (i < J.ctr->n_triggers) {
     const uint32_t kp = J.kept_pos[J.triggers[i]];
     if (kp < nk) J.k_forced[kp] = 1;
+    J.t_kept[i] = kp;
   }
 }
 

@@ -113,6 +113,16 @@ struct ScanOf<kScanDecKey> {
   static __device__ uint64_t* total(const JobDev&) { return nullptr; }
 };
 
+template <>
+struct ScanOf<kScanKb> {
+  using TI = uint32_t;
+  using TO = uint64_t;
+  static __device__ const TI* in(const JobDev& J) { return J.k_b; }
+  static __device__ TO* out(const JobDev& J) { return J.k_pb; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_kept; }
+  static __device__ uint64_t* total(const JobDev&) { return nullptr; }
+};
+
 // Tile-sum scratch of a scan (the scans of a job run one after another).
 template <int S>
 __device__ __forceinline__ uint64_t* scan_tiles_of(const JobDev& J) {
@@ -260,6 +270,7 @@ void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st) {
     case kScanGcum: scan_sel<kScanGcum>(bt, n_cap, st); break;
     case kScanIcum: scan_sel<kScanIcum>(bt, n_cap, st); break;
     case kScanDecKey: scan_sel<kScanDecKey>(bt, n_cap, st); break;
+    case kScanKb: scan_sel<kScanKb>(bt, n_cap, st); break;
   }
 }
 
