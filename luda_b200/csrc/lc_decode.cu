@@ -327,7 +327,7 @@ __device__ __forceinline__ void run_bounds(const BlockView& v, uint32_t r, uint6
 constexpr uint32_t kDecWarps = 4;
 constexpr uint32_t kDecStage = 8448;    // data block bytes + 16-byte phase
 constexpr uint32_t kDecMaxEnt = 512;    // entries of one staged block
-constexpr uint32_t kDecKeyBuf = 4096 + 32;
+constexpr uint32_t kDecKeyBuf = 32 * 132 + 32;  // 4 KiB of keys, or 32 lane slices of 132 bytes
 constexpr uint32_t kDecLastKey = 256;   // longest key the staged path rebuilds
 struct DecWarpSmem {
   uint8_t stage[kDecStage];
@@ -888,8 +888,40 @@ __device__ void decode_sparse_group(const JobDev& J, uint64_t g0, uint64_t nblk,
     kbase = J.blk_key_base[b];
   }
   __syncwarp();
-  // 3. per sparse block: keys rebuilt in entry order, descriptors
+  // 3. keys rebuilt in entry order and descriptors: one lane per block when
+  // every key of the group fits a lane's 128-byte slice of the key buffer
+  // (slices 132 bytes apart, so that the lanes' byte stores hit distinct
+  // banks), else one block at a time across the warp
   const unsigned done = __ballot_sync(0xffffffffu, ok);
+  uint32_t gmaxk = maxk;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) gmaxk = max(gmaxk, __shfl_xor_sync(0xffffffffu, gmaxk, o));
+  if (gmaxk <= 128) {
+    if (ok) {
+      const uint8_t* p = J.in + J.blk_off[b];
+      const uint32_t voff0 = (uint32_t)J.blk_off[b];
+      const uint64_t ebase = J.blk_ent_base[b];
+      uint8_t* slice = W.keybuf + lane * 132;
+      uint8_t* gdst = J.keys + kbase;
+      uint32_t kofs = 0;
+      for (uint32_t x = 0; x < nent; x++) {
+        const uint32_t i = lane * kSparseEnt + x;
+        const uint32_t esh = W.sh[i], ekl = W.kl[i], edp = W.dpos[i];
+        for (uint32_t t = esh; t < ekl; t += 32)
+          copy_small(slice + t, p + edp + (t - esh), min(32u, ekl - t));
+        for (uint32_t t = 0; t < ekl; t++) gdst[kofs + t] = slice[t];
+        const uint64_t e = ebase + x;
+        J.e_koff[e] = (uint32_t)(kbase + kofs);
+        J.e_klen[e] = ekl;
+        J.e_voff[e] = voff0 + edp + (ekl - esh);
+        J.e_vlen[e] = W.vl[i];
+        J.e_pfx[e] = user_prefix(slice, ekl);
+        J.e_tag[e] = ld_le64(slice + ekl - 8);
+        kofs += ekl;
+      }
+    }
+    __syncwarp();
+  } else
   for (unsigned m = done; m; m &= m - 1) {
     const uint32_t L = __ffs(m) - 1;
     const uint64_t bb = g0 + L;

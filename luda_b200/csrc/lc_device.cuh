@@ -239,6 +239,26 @@ __device__ __forceinline__ uint32_t warp_block_crc(const JobDev& J, const uint32
   return ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
 }
 
+// Up to 32 bytes from src (any alignment) to dst: every word that holds a
+// needed byte is loaded before any byte is stored (no load waits on the
+// previous store), then the words are realigned by funnel shifts.
+__device__ __forceinline__ void copy_small(uint8_t* dst, const uint8_t* src, uint32_t len) {
+  if (!len) return;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = 8 * (uint32_t)(a & 3);
+  const uint32_t nw = ((uint32_t)(a & 3) + len + 3) >> 2;  // words holding the bytes
+  uint32_t w[9];
+#pragma unroll
+  for (uint32_t i = 0; i < 9; i++) w[i] = i < nw ? __ldg(base + i) : 0u;
+  uint32_t r[8];
+#pragma unroll
+  for (uint32_t i = 0; i < 8; i++) r[i] = __funnelshift_r(w[i], w[i + 1], sh);
+#pragma unroll
+  for (uint32_t i = 0; i < 32; i++)
+    if (i < len) dst[i] = (uint8_t)(r[i >> 2] >> (8 * (i & 3)));
+}
+
 // Error reporting: the first error code wins.
 __device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t detail) {
   if (atomicCAS(&c->error, 0u, code) == 0u) c->error_detail = detail;
@@ -309,11 +329,14 @@ __device__ __forceinline__ uint32_t warp_block_crc_smem(const JobDev& J, const u
   const uint32_t seg = 4 * m;
   const uint32_t b0 = lane * seg;
   const uint32_t e0 = min(total, b0 + seg);
-  const uint32_t c = b0 < e0 ? crc_raw4(tab4, 0, p + b0, e0 - b0) : 0;
+  // lane 0 starts from the CRC's initial value (all ones), which so reaches
+  // the result through lane 0's own shift; the others start from zero
+  const uint32_t init = lane == 0 ? 0xffffffffu : 0u;
+  const uint32_t c = b0 < e0 ? crc_raw4(tab4, init, p + b0, e0 - b0) : 0;
   uint32_t v = b0 < total ? crc_shift(J, c, total - e0) : 0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-  const uint32_t full = v ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
+  const uint32_t full = v ^ 0xffffffffu;
   return ((full >> 15) | (full << 17)) + 0xa282ead8u;
 }
 

@@ -596,8 +596,8 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
 // Blocks with more than kEncMaxEnt entries, or too large for the stage, take
 // the direct path.
 constexpr uint32_t kEncWarps = 8;
-constexpr uint32_t kEncMaxEnt = 128;
-constexpr uint32_t kEncStage = 8448;  // block + 5-byte trailer + 16-byte phase
+constexpr uint32_t kEncMaxEnt = 64;
+constexpr uint32_t kEncStage = 6144;  // block + 5-byte trailer + 16-byte phase
 constexpr uint32_t kEncLong = 32;     // stretches at least this long are copied in chunks
 constexpr uint32_t kEncChunks = 4;    // chunks in flight per lane
 struct EncWarp {
@@ -668,23 +668,22 @@ __device__ __forceinline__ uint32_t chunks_in(uint32_t a, uint32_t b, uint32_t* 
 }
 
 // Bytes [a, b) of the stage from src, except the full chunks of a long
-// stretch (step 3 writes those).
+// stretch (step 3 writes those): a short stretch (< kEncLong bytes) whole,
+// a long one's head and tail (< 16 bytes each).
 __device__ __forceinline__ void stretch_bytes(uint8_t* st, uint32_t a, uint32_t b,
                                               const uint8_t* src, bool chunked) {
-  uint32_t c0 = b, c1 = b;
-  if (chunked) {
-    uint32_t first;
-    const uint32_t nq = chunks_in(a, b, &first);
-    if (nq) {
-      c0 = first;
-      c1 = first + 16 * nq;
-    }
+  if (!chunked) {
+    copy_small(st + a, src, b - a);
+    return;
   }
-  for (uint32_t p = a; p < c0; p++) st[p] = __ldg(src + (p - a));
-  for (uint32_t p = c1; p < b; p++) st[p] = __ldg(src + (p - a));
+  uint32_t first;
+  const uint32_t nq = chunks_in(a, b, &first);  // >= 1: 32 bytes hold a whole chunk
+  const uint32_t c1 = first + 16 * nq;
+  copy_small(st + a, src, first - a);
+  copy_small(st + c1, src + (c1 - a), b - c1);
 }
 
-__global__ void __launch_bounds__(kEncWarps * 32, 2) k_encode_blocks(const JobDev* __restrict__ jobs) {
+__global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t enc_smem[];
   uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
@@ -932,9 +931,11 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
   }
 }
 
-// A filter group whose filter has at most kFilterLocal bytes, by one thread:
-// the bits in a thread-local array, then byte stores.
+// A filter group of at most kFilterThreadKeys keys whose filter has at most
+// kFilterLocal bytes, by one thread: the bits in a thread-local array, then
+// byte stores.  Groups of more keys are built by a warp.
 constexpr uint32_t kFilterLocal = 128;
+constexpr uint32_t kFilterThreadKeys = 8;
 __device__ __forceinline__ void filter_group_thread(const JobDev& J, uint64_t b, uint32_t gb) {
   const FileOut& F = J.files[J.b_file[b]];
   const uint32_t fb0 = F.first_block, fb1 = F.end_block;
@@ -968,8 +969,8 @@ __device__ __forceinline__ void filter_group_thread(const JobDev& J, uint64_t b,
   for (int64_t jj = jprev + 1; jj <= (int64_t)jb; jj++) st_le32(fbase + Ft + 4 * jj, val);
 }
 
-// Filter groups (at their first blocks): small filters one per thread, larger
-// ones one per warp (bits in the warp's shared memory, or in place).
+// Filter groups (at their first blocks): groups of a few keys one per thread,
+// larger ones one per warp (bits in the warp's shared memory, or in place).
 __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_filter[8][kFilterSmem / 4];  // blockDim 256: 8 warps
@@ -979,12 +980,14 @@ __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
        b += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t gb = J.b_gbytes[b];
-    if (gb != 0 && gb - 1 <= kFilterLocal) filter_group_thread(J, b, gb);
+    if (gb != 0 && J.b_gkeys[b] <= kFilterThreadKeys && gb - 1 <= kFilterLocal)
+      filter_group_thread(J, b, gb);
   }
   const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride) {
     const uint32_t gb = J.b_gbytes[b];
-    if (gb != 0 && gb - 1 > kFilterLocal) encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
+    if (gb != 0 && (J.b_gkeys[b] > kFilterThreadKeys || gb - 1 > kFilterLocal))
+      encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
   }
 }
 
@@ -1170,7 +1173,7 @@ void encode_kernel_attributes() {
 void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
   // grid-stride over the device-side block count: 5 CTAs per SM x 4 waves,
   // shared out among the jobs
-  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 2 * 4)),
+  note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 3 * 4)),
                                         bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);
 }
 void launch_emit_decoded(const Batch& bt, cudaStream_t st) {
