@@ -978,22 +978,31 @@ __device__ void decode_sparse_group(const JobDev& J, uint64_t g0, uint64_t nblk,
   for (unsigned m = rest; m; m &= m - 1) decode_one(J, g0 + (__ffs(m) - 1), lane, W);
 }
 
+// Jobs whose blocks are not sparse: one warp per block.
 __global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   extern __shared__ __align__(16) uint8_t dec_smem[];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
-  if (J.ctr->error) return;
+  if (J.ctr->error || J.sparse_blocks) return;
   const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  if (J.sparse_blocks) {
-    for (uint64_t g = (uint64_t)blockIdx.x * kDecWarps + warp; g * kSparseGroup < nblk;
-         g += (uint64_t)gridDim.x * kDecWarps)
-      decode_sparse_group(J, g * kSparseGroup, nblk, lane, W);
-    return;
-  }
   for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
        b += (uint64_t)gridDim.x * kDecWarps)
     decode_one(J, b, lane, W);
+}
+
+// Jobs whose blocks are sparse: one warp per group of kSparseGroup blocks
+// (a separate kernel, so that its registers do not weigh on the dense path).
+__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode_sparse(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  extern __shared__ __align__(16) uint8_t dec_smem[];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
+  if (J.ctr->error || !J.sparse_blocks) return;
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
+  for (uint64_t g = (uint64_t)blockIdx.x * kDecWarps + warp; g * kSparseGroup < nblk;
+       g += (uint64_t)gridDim.x * kDecWarps)
+    decode_sparse_group(J, g * kSparseGroup, nblk, lane, W);
 }
 
 __global__ void k_entries_from_offsets(const JobDev* __restrict__ jobs) {
@@ -1043,6 +1052,7 @@ static unsigned dec_ctas(const Batch& bt) {
 void decode_kernel_attributes() {
   dec_smem_attr((const void*)k_block_count);
   dec_smem_attr((const void*)k_block_decode);
+  dec_smem_attr((const void*)k_block_decode_sparse);
 }
 
 void launch_block_count(const Batch& bt, cudaStream_t st) {
@@ -1064,6 +1074,8 @@ void launch_run_bounds(const Batch& bt, cudaStream_t st) {
 void launch_block_decode(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
                                   kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
+  note_launch(), k_block_decode_sparse<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
+                                         kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
 }
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st) {
   note_launch(), k_entries_from_offsets<<<dim3(grid_x(bt.max_entries, 256, 148 * 8), bt.B), 256, 0,

@@ -110,6 +110,17 @@ __device__ __forceinline__ uint64_t user_prefix(const uint8_t* k, uint32_t klen)
   return v;
 }
 
+// The 8 user-key bytes after the first `skip`, big endian, zero padded: the
+// prefix of an entry when every key of the job shares its first `skip` bytes.
+__device__ __forceinline__ uint64_t user_prefix_after(const uint8_t* k, uint32_t klen,
+                                                      uint32_t skip) {
+  const uint32_t u = klen - 8;
+  uint64_t v = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < 8; i++) v = (v << 8) | (uint64_t)(skip + i < u ? k[skip + i] : 0);
+  return v;
+}
+
 // a before b in the merge (InternalKeyComparator order), given their user-key
 // prefixes: the prefixes decide unless equal.
 __device__ __forceinline__ bool entry_le(const JobDev& J, uint32_t a, uint64_t pa, uint32_t b,

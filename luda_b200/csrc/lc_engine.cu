@@ -566,6 +566,7 @@ struct Stage {
 void launch_tail(const Batch& bt, bool decode_merge, cudaStream_t st, PhaseTimer& T) {
   if (decode_merge) {
     launch_block_decode(bt, st);
+    launch_key_skip(bt, st);
     T.mark(kDecode);
     launch_merge(bt, st);
     T.mark(kMerge);
@@ -624,6 +625,8 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
     J.gp_idx = A.get<uint32_t>(J.n_gp ? N : 1);
     J.kept_pos = A.get<uint32_t>(N + 1);
     J.gp_first = A.get<uint32_t>(J.n_gp + 1);
+    J.gp_upfx = A.get<uint64_t>(J.n_gp + 1);
+    J.gp_mode = A.get<uint8_t>(J.n_gp + 1);
     J.k_forced = A.get<uint8_t>(N + 1);
   }
   J.k_koff = A.get<uint32_t>(N);
@@ -931,7 +934,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     std::vector<uint64_t> in_base(B, 0);
     std::vector<bool> zero_copy(B, false);
     struct Offs {
-      uint64_t td, dec, gpk, gpo, gpp, gpu, lb, bk, bso, blo, bsl, bll;
+      uint64_t td, dec, gpk, gpo, gpp, lb, bk, bso, blo, bsl, bll;
     };
     std::vector<Offs> offs(B);
     for (uint32_t i = 0; i < B; i++) {
@@ -991,19 +994,13 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       r.cap_blk = cap_blk;
       // grandparents: largest keys, offsets, size prefix
       J.n_gp = (uint32_t)j->gp_largest.size();
-      std::vector<uint64_t> gpo(J.n_gp + 1, 0), gpp(J.n_gp + 1, 0), gpu(J.n_gp + 1, 0);
+      std::vector<uint64_t> gpo(J.n_gp + 1, 0), gpp(J.n_gp + 1, 0);
       std::string gpk;
       for (uint32_t g = 0; g < J.n_gp; g++) {
         const std::string& k = j->gp_largest[g];
         gpk += k;
         gpo[g + 1] = gpk.size();
         gpp[g + 1] = gpp[g] + j->gp_size[g];
-        // first 8 user-key bytes, big endian, zero padded (as the decoded
-        // entries' prefixes)
-        uint64_t v = 0;
-        for (size_t b = 0; b < 8; b++)
-          v = (v << 8) | (b + 8 < k.size() ? (uint8_t)k[b] : 0u);
-        gpu[g] = v;
       }
       // base-level files, grouped by level
       const uint32_t nb = (uint32_t)j->base_level.size();
@@ -1034,7 +1031,6 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       o.gpk = S.put(gpk.data(), gpk.size());
       o.gpo = S.put(gpo.data(), gpo.size());
       o.gpp = S.put(gpp.data(), gpp.size());
-      o.gpu = S.put(gpu.data(), gpu.size());
       o.lb = S.put(lb.data(), lb.size());
       o.bk = S.put(bk.data(), bk.size());
       o.bso = S.put(so.data(), nb);
@@ -1078,7 +1074,6 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       J.gp_keys = d_stage + o.gpk;
       J.gp_key_off = (const uint64_t*)(d_stage + o.gpo);
       J.gp_prefix = (const uint64_t*)(d_stage + o.gpp);
-      J.gp_upfx = (const uint64_t*)(d_stage + o.gpu);
       J.base_level_begin = (const uint32_t*)(d_stage + o.lb);
       J.base_keys = d_stage + o.bk;
       J.base_small_off = (const uint64_t*)(d_stage + o.bso);

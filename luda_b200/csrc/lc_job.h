@@ -52,6 +52,8 @@ struct Counters {
   uint64_t kept_key_bytes;    // internal-key bytes of the survivors
   uint64_t kept_value_bytes;  // value bytes of the survivors
   uint64_t key_cursor;        // key bytes reserved by the single-pass decode
+  uint32_t key_skip;          // user-key bytes every input key shares (prefixes start after them)
+  uint32_t pad2;
 };
 
 struct TableDesc {
@@ -120,7 +122,10 @@ struct JobDev {
   const uint8_t* gp_keys;
   const uint64_t* gp_key_off;   // n_gp + 1
   const uint64_t* gp_prefix;    // n_gp + 1, prefix sums of file sizes
-  const uint64_t* gp_upfx;      // n_gp: first 8 user-key bytes of each largest key, big endian
+  uint64_t* gp_upfx;            // n_gp: 8 user-key bytes of each largest key after the
+                                // job's common prefix, big endian (k_key_skip)
+  uint8_t* gp_mode;             // n_gp: 0 compare by prefix then key; 1 every entry sorts
+                                // after the grandparent; 2 every entry sorts before it
   // base-level files: user-key ranges per level >= L+2
   uint32_t n_base_levels;
   const uint32_t* base_level_begin;  // n_base_levels + 1, into the file list
@@ -151,7 +156,7 @@ struct JobDev {
   uint32_t* e_klen;
   uint32_t* e_voff;
   uint32_t* e_vlen;
-  uint64_t* e_pfx;
+  uint64_t* e_pfx;           // 8 user-key bytes after the key_skip common bytes, big endian
   uint64_t* e_tag;           // the key's last 8 bytes: (sequence << 8) | type
   uint64_t cap_entries;
 

@@ -95,6 +95,8 @@ void launch_block_decode(const Batch& bt, cudaStream_t st);
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st);
 
 // lc_merge.cu -- merge, drop rule, grandparent cuts, survivors
+// the keys' common bytes, entry prefixes after them, grandparent prefixes
+void launch_key_skip(const Batch& bt, cudaStream_t st);
 void launch_merge(const Batch& bt, cudaStream_t st);
 void launch_drop(const Batch& bt, cudaStream_t st);
 void launch_triggers(const Batch& bt, cudaStream_t st);

@@ -33,6 +33,73 @@ namespace lc {
 
 namespace {
 
+// The user-key bytes every input key of the job shares: the common prefix
+// of the first and last keys of every merge child (each child is sorted, so
+// its keys share what its two ends share) with the first key of child 0.
+// Then, per grandparent, its prefix after those bytes, or where it sorts
+// against every entry when it does not share them.  One CTA per job.
+__global__ void k_key_skip(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_failed, s_skip;
+  if (threadIdx.x == 0) {
+    s_failed = J.ctr->error;
+    s_skip = 0xffffffffu;
+  }
+  __syncthreads();
+  if (s_failed) return;
+  const uint64_t n = J.ctr->n_entries_in;
+  uint32_t u0 = 0;
+  const uint8_t* k0 = nullptr;
+  if (n > 0) {
+    k0 = J.keys + J.e_koff[0];
+    u0 = J.e_klen[0] - 8;
+  }
+  // boundary keys: 2 per child
+  for (uint32_t x = threadIdx.x; x < 2 * J.n_runs && n > 0; x += blockDim.x) {
+    const uint32_t r = x >> 1;
+    const uint64_t a = J.run_entry_begin[r], z = J.run_entry_begin[r + 1];
+    if (a == z) continue;
+    const uint64_t e = (x & 1) ? z - 1 : a;
+    const uint8_t* k = J.keys + J.e_koff[e];
+    const uint32_t u = J.e_klen[e] - 8, m = min(u, u0);
+    uint32_t l = 0;
+    while (l < m && k[l] == k0[l]) l++;
+    atomicMin(&s_skip, l);
+  }
+  __syncthreads();
+  const uint32_t L = n > 0 ? min(s_skip, u0) : 0;
+  if (threadIdx.x == 0) J.ctr->key_skip = L;
+  for (uint32_t g = threadIdx.x; g < J.n_gp; g += blockDim.x) {
+    const uint64_t go = J.gp_key_off[g];
+    const uint8_t* gk = J.gp_keys + go;
+    const uint32_t gu = (uint32_t)(J.gp_key_off[g + 1] - go) - 8;
+    uint32_t i = 0;
+    const uint32_t m = min(gu, L);
+    while (i < m && gk[i] == k0[i]) i++;
+    uint8_t mode = 0;
+    if (i < L) {
+      // differs within the common bytes, or ends inside them: it sorts
+      // before every entry (1) or after every entry (2)
+      mode = (i == gu || gk[i] < k0[i]) ? 1 : 2;
+    }
+    J.gp_mode[g] = mode;
+    J.gp_upfx[g] = mode ? 0 : user_prefix_after(gk, gu + 8, L);
+  }
+}
+
+// e_pfx after the job's common bytes (only when there are some: the decode
+// wrote the prefixes from the keys' first byte).
+__global__ void k_prefix(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;
+  const uint32_t L = J.ctr->key_skip;
+  if (L == 0) return;
+  const uint64_t n = J.ctr->n_entries_in;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    J.e_pfx[e] = user_prefix_after(J.keys + J.e_koff[e], J.e_klen[e], L);
+}
+
 // A single merge child (no round): the merged order is the input order.
 __global__ void k_merge_single(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
@@ -252,8 +319,11 @@ __device__ __forceinline__ void drop_one(const JobDev& J, const uint32_t* __rest
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
       const uint64_t gp = J.gp_upfx[mid];
+      const uint32_t mode = J.gp_mode[mid];
       bool after;
-      if (gp != upfx) {
+      if (mode) {  // the grandparent lies outside the keys' common prefix
+        after = mode == 1;
+      } else if (gp != upfx) {
         after = upfx > gp;
       } else {
         const uint64_t go = J.gp_key_off[mid];
@@ -404,6 +474,11 @@ void merge_kernel_attributes() {
 uint64_t merge_tile_capacity(uint64_t entries, uint32_t runs) {
   // tiles of at least 64 positions, one partial tile per pair
   return entries / 64 + runs + 2;
+}
+
+void launch_key_skip(const Batch& bt, cudaStream_t st) {
+  note_launch(), k_key_skip<<<dim3(1, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_prefix<<<dim3(flat_ctas(bt, bt.max_entries, 256), bt.B), 256, 0, st>>>(bt.d);
 }
 
 void launch_merge(const Batch& bt, cudaStream_t st) {
