@@ -4,8 +4,9 @@
 // (util/coding.cc:9-192), the internal-key order (db/dbformat.cc:51-67), the
 // bloom hash (util/hash.cc:22-51) and CRC32C (util/crc32c.cc:276; reflected
 // Castagnoli polynomial 0x82F63B78 with pre/post inversion).  The CRC is
-// computed from a 256-entry table built from the polynomial at kernel start and
-// combined across lanes with multiplication by x^(8n) mod P in GF(2)[x].
+// computed from tables built from the polynomial (a 256-entry byte table, or
+// the 5-bit field tables of the block encoder's row CRC) and combined across
+// lanes with multiplication by x^(8n) mod P in GF(2)[x].
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -328,27 +329,99 @@ __device__ __forceinline__ uint32_t crc_raw4(const uint32_t* tab4, uint32_t c, c
   return c;
 }
 
-// Masked block trailer CRC of n bytes in shared memory plus the zero type
-// byte, which the caller has stored at p[n].  One warp; each lane takes a
-// contiguous stretch whose length in words is odd (distinct banks).
-__device__ __forceinline__ uint32_t warp_block_crc_smem(const JobDev& J, const uint32_t* tab4,
-                                                        const uint8_t* p, uint32_t n) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t total = n + 1;
-  uint32_t m = (total + 127) / 128;
-  m |= 1;
-  const uint32_t seg = 4 * m;
-  const uint32_t b0 = lane * seg;
-  const uint32_t e0 = min(total, b0 + seg);
-  // lane 0 starts from the CRC's initial value (all ones), which so reaches
-  // the result through lane 0's own shift; the others start from zero
-  const uint32_t init = lane == 0 ? 0xffffffffu : 0u;
-  const uint32_t c = b0 < e0 ? crc_raw4(tab4, init, p + b0, e0 - b0) : 0;
-  uint32_t v = b0 < total ? crc_shift(J, c, total - e0) : 0;
+// ---------------------------------------------------------------------------
+// Block CRC32C over 16-byte chunks, lane l of a warp taking chunks l, l + 32,
+// l + 64, ... (one 512-byte row of the block per step of all 32 lanes).
+//
+// The raw register after n bytes is linear in the bytes and in the register
+// it started from, and a register u before 16 bytes x equals register 0
+// before x with u xored into its first four bytes.  So a lane keeps
+//   u <- H(x ^ u),  H(x) = register after x and 496 zero bytes, from 0,
+// which accounts for the other lanes' bytes of the row as zeros; the block's
+// register is the xor over the lanes of their u, each moved back (x^-8n) by
+// the bytes it was carried past the block's end.  H is linear in the 128 bits
+// of x: the xor of 26 lookups, one per 5-bit field, in 32-entry tables.  A
+// warp's 32 lookups into one 32-entry table hit 32 distinct banks or share a
+// word, so each costs one shared-memory pass where a 256-entry byte table
+// costs about three.  The CRC's initial all-ones register is the same as ones
+// xored into the block's first four bytes.
+constexpr uint32_t kCrcH5Fields = 26;    // 5-bit fields of a 16-byte chunk
+constexpr uint32_t kCrcRowBytes = 512;   // 32 lanes x 16 bytes
+constexpr uint32_t kCrcH5Words = kCrcH5Fields * 32;
+constexpr uint32_t kCrcXinvN = 512;      // back shifts of 0..511 bytes
+
+// H(w0..w3) from the 26 tables (table i at h5[32 i], indexed by bits
+// [5i, 5i + 5) of the little-endian 128-bit chunk).
+__device__ __forceinline__ uint32_t crc_h5(const uint32_t* __restrict__ h5, uint32_t w0,
+                                           uint32_t w1, uint32_t w2, uint32_t w3) {
+  const uint32_t w[5] = {w0, w1, w2, w3, 0u};
+  uint32_t r = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < kCrcH5Fields; i++) {
+    const uint32_t s = 5 * i, q = s >> 5, o = s & 31;
+    const uint32_t f = o <= 27 ? (w[q] >> o) & 31 : __funnelshift_r(w[q], w[q + 1], o) & 31;
+    r ^= h5[32 * i + f];
+  }
+  return r;
+}
+
+// The bytes of word x of the chunk at grid position p that belong to the
+// message [m0, m1), zero elsewhere, with the message's first four bytes
+// inverted (the initial register).
+__device__ __forceinline__ uint32_t crc_edge_word(uint32_t x, uint32_t pos, uint32_t m0,
+                                                  uint32_t m1) {
+  const auto lo_mask = [](int32_t k) -> uint32_t {  // bytes [0, k) of a word, k clamped to 0..4
+    return k <= 0 ? 0u : (k >= 4 ? 0xffffffffu : (1u << (8 * k)) - 1u);
+  };
+  const int32_t a = (int32_t)m0 - (int32_t)pos, b = (int32_t)m1 - (int32_t)pos;
+  const uint32_t keep = lo_mask(b) & ~lo_mask(a);
+  const uint32_t inv = lo_mask(a + 4) & ~lo_mask(a);
+  return (x & keep) ^ inv;
+}
+
+// One lane's chunk at grid position p (16-aligned) into its CRC register u,
+// for the message [m0, m1) of the grid.
+__device__ __forceinline__ uint32_t crc_chunk_step(const uint32_t* __restrict__ h5, uint32_t u,
+                                                   uint32_t p, uint32_t m0, uint32_t m1,
+                                                   uint32_t w0, uint32_t w1, uint32_t w2,
+                                                   uint32_t w3) {
+  if (p < m0 + 4 || p + 16 > m1) {
+    w0 = crc_edge_word(w0, p, m0, m1);
+    w1 = crc_edge_word(w1, p + 4, m0, m1);
+    w2 = crc_edge_word(w2, p + 8, m0, m1);
+    w3 = crc_edge_word(w3, p + 12, m0, m1);
+  }
+  return crc_h5(h5, w0 ^ u, w1, w2, w3);
+}
+
+// The masked CRC from the lanes' registers: lane l's last chunk was at grid
+// position `last` (0xffffffff when it had none) and the message ends at m1.
+__device__ __forceinline__ uint32_t crc_rows_finish(const uint32_t* __restrict__ xinv, uint32_t u,
+                                                    uint32_t last, uint32_t m1) {
+  uint32_t v = 0;
+  if (last != 0xffffffffu) v = gf2_mulmod(xinv[last + kCrcRowBytes - m1], u);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
   const uint32_t full = v ^ 0xffffffffu;
-  return ((full >> 15) | (full << 17)) + 0xa282ead8u;
+  return ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
+}
+
+// Masked block trailer CRC of the block [p, p + n) plus the zero type byte at
+// p[n], read from memory in 16-byte chunks by one warp (p - (p & 15) is the
+// grid origin; bytes of the chunks outside the block are read and ignored).
+__device__ __forceinline__ uint32_t warp_block_crc_rows(const uint32_t* __restrict__ h5,
+                                                        const uint32_t* __restrict__ xinv,
+                                                        const uint8_t* p, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t m0 = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 15), m1 = m0 + n + 1;
+  const uint8_t* g = p - m0;
+  uint32_t u = 0, last = 0xffffffffu;
+  for (uint32_t q = 16 * lane; q < m1; q += kCrcRowBytes) {
+    const uint4 x = __ldcg(reinterpret_cast<const uint4*>(g + q));  // the warp's own stores, via L2
+    u = crc_chunk_step(h5, u, q, m0, m1, x.x, x.y, x.z, x.w);
+    last = q;
+  }
+  return crc_rows_finish(xinv, u, last, m1);
 }
 
 }  // namespace lc

@@ -578,43 +578,58 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
   }
 }
 
-// One warp per output data block, assembled in the warp's shared-memory stage
-// (which has the block's own 16-byte phase in global memory), in five steps:
-//  1. entry table, one lane per entry: output offsets, key/value sources and
-//     lengths, and the 16-byte chunks of the stage that lie wholly inside a
-//     long (>= kEncLong bytes) key delta or value;
-//  2. one lane per entry writes its header varints, its short stretches and
-//     the cut edges of its long ones byte by byte, and its restart word;
-//  3. the long stretches' chunks as one flat list over the warp: a chunk is
-//     five 4-byte read-only loads and four funnel shifts at any source
-//     alignment, then one 16-byte shared store; kEncChunks chunks per lane
-//     are loaded before any is stored;
-//  4. CRC32C of the block plus its type byte from the stage, lanes over
-//     contiguous stretches (slicing-by-4 tables), combined by x^(8n) shifts;
-//  5. the stage -- block, type byte and CRC -- to global memory with 16-byte
-//     stores (byte stores for the two partial chunks at the ends).
-// Blocks with more than kEncMaxEnt entries, or too large for the stage, take
-// the direct path.
+// One warp per output data block, assembled around the warp's shared-memory
+// stage, which has the block's own 16-byte phase in global memory: stage
+// position p is global byte dst - ph + p, ph = dst & 15.  Three steps:
+//  1. Entries in rounds of 32, one lane per entry: entry sizes and output
+//     offsets by a warp scan; the lane writes its entry header and restart
+//     word to the stage, and its key delta and value: a stretch shorter than
+//     kEncLong whole, a longer one only its unaligned head and tail, the
+//     16-byte chunks between joining the warp's list of long stretches (at
+//     most kEncMaxLong; a lane stages the chunks of a stretch past the list
+//     itself).
+//  2. The block's 16-byte chunks, lane l taking chunks l, l + 32, ..., two
+//     at a time: a chunk inside a listed stretch is read from global memory
+//     (five 4-byte loads and four funnel shifts at any source alignment),
+//     any other from the stage.  A chunk wholly inside the block and its
+//     type byte goes out with one 16-byte store, and every chunk feeds the
+//     lane's share of the block CRC (crc_chunk_step).
+//  3. The lanes' CRC shares combined, the trailer (type byte and CRC) into
+//     the stage, and the partial chunks at both ends from the stage with byte
+//     stores.
+// A block that does not fit the stage takes the direct path.
 constexpr uint32_t kEncWarps = 8;
-constexpr uint32_t kEncMaxEnt = 64;
-constexpr uint32_t kEncStage = 6144;  // block + 5-byte trailer + 16-byte phase
-constexpr uint32_t kEncLong = 32;     // stretches at least this long are copied in chunks
-constexpr uint32_t kEncChunks = 4;    // chunks in flight per lane
+constexpr uint32_t kEncStage = 6144;  // block + 5-byte trailer + 16-byte phase + read slack
+constexpr uint32_t kEncLong = 33;     // stretches at least this long are read by chunks
+constexpr uint32_t kEncMaxLong = 64;  // listed long stretches per block
+constexpr uint32_t kEncFromInput = 0x80000000u;
 struct EncWarp {
-  uint32_t off[kEncMaxEnt + 1];  // entry output offset in the block (+ end)
-  uint32_t kbeg[kEncMaxEnt];     // offset of the key delta (after the header)
-  uint32_t ksrc[kEncMaxEnt];     // key delta: offset in the key arena
-  uint32_t vsrc[kEncMaxEnt];     // value: offset in the input bytes
-  uint32_t kd[kEncMaxEnt];       // key delta length
-  uint32_t vl[kEncMaxEnt];       // value length
-  uint32_t sh[kEncMaxEnt];       // shared prefix length
-  uint32_t cc[kEncMaxEnt + 1];   // chunks of the long stretches before the entry
+  uint32_t ls_c0[kEncMaxLong];   // first whole chunk (stage grid) | kEncFromInput
+  uint32_t ls_n[kEncMaxLong];    // whole chunks
+  uint32_t ls_src[kEncMaxLong];  // source offset of the first chunk (key arena or input)
   __align__(16) uint8_t stage[kEncStage];
 };
-constexpr size_t kEncSmem = 4096 + (size_t)kEncWarps * sizeof(EncWarp);
+constexpr size_t kEncSmem = (size_t)kEncWarps * sizeof(EncWarp);
 
-__device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab, uint64_t b,
-                                           uint8_t* dst, uint32_t lane) {
+// 16 bytes from src at any alignment: the five words holding them (the fifth
+// only when src is not word aligned) and four funnel shifts.
+__device__ __forceinline__ void load16(const uint8_t* src, uint32_t (&w)[4]) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = 8 * (uint32_t)(a & 3);
+  uint32_t x[5];
+#pragma unroll
+  for (int i = 0; i < 4; i++) x[i] = __ldg(q + i);
+  x[4] = sh ? __ldg(q + 4) : 0u;
+#pragma unroll
+  for (int i = 0; i < 4; i++) w[i] = __funnelshift_r(x[i], x[i + 1], sh);
+}
+
+// The direct path: entries written straight to global memory, one lane per
+// entry, then the CRC read back from there.
+__device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* h5,
+                                           const uint32_t* xinv, uint64_t b, uint8_t* dst,
+                                           uint32_t lane) {
   const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
   const uint32_t R = J.restart_interval;
   const uint32_t bsz = J.b_size[b];
@@ -655,47 +670,81 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* tab,
     dst[bsz] = 0;
   }
   __syncwarp();
-  const uint32_t crc = warp_block_crc(J, tab, dst, bsz);
+  const uint32_t crc = warp_block_crc_rows(h5, xinv, dst, bsz);
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
-// Full 16-byte chunks of stage stretch [a, b) (stage offsets): first chunk
-// offset and count.
-__device__ __forceinline__ uint32_t chunks_in(uint32_t a, uint32_t b, uint32_t* first) {
-  const uint32_t a0 = (a + 15) & ~15u, b0 = b & ~15u;
-  *first = a0;
-  return b0 > a0 ? (b0 - a0) >> 4 : 0;
-}
-
-// Bytes [a, b) of the stage from src, except the full chunks of a long
-// stretch (step 3 writes those): a short stretch (< kEncLong bytes) whole,
-// a long one's head and tail (< 16 bytes each).
-__device__ __forceinline__ void stretch_bytes(uint8_t* st, uint32_t a, uint32_t b,
-                                              const uint8_t* src, bool chunked) {
-  if (!chunked) {
-    copy_small(st + a, src, b - a);
+// A key delta or value of `len` bytes for stage position pos, from base +
+// off: into the stage whole when shorter than kEncLong, else its unaligned
+// head and tail, with its whole chunks listed in slot li (or staged here when
+// the list is full); li advances past a long stretch.
+__device__ __forceinline__ void enc_stretch(EncWarp& W, uint8_t* st, uint32_t pos, uint32_t len,
+                                            const uint8_t* base, uint32_t off, uint32_t from,
+                                            uint32_t& li) {
+  const uint8_t* src = base + off;
+  if (len < kEncLong) {
+    copy_small(st + pos, src, len);
     return;
   }
-  uint32_t first;
-  const uint32_t nq = chunks_in(a, b, &first);  // >= 1: 32 bytes hold a whole chunk
-  const uint32_t c1 = first + 16 * nq;
-  copy_small(st + a, src, first - a);
-  copy_small(st + c1, src + (c1 - a), b - c1);
+  const uint32_t first = (pos + 15) & ~15u, last = (pos + len) & ~15u;
+  copy_small(st + pos, src, first - pos);
+  copy_small(st + last, src + (last - pos), pos + len - last);
+  const uint32_t nq = (last - first) >> 4;
+  if (li < kEncMaxLong) {
+    W.ls_c0[li] = (first >> 4) | from;
+    W.ls_n[li] = nq;
+    W.ls_src[li] = off + (first - pos);
+  } else {
+    for (uint32_t q = 0; q < nq; q++) {
+      uint32_t w[4];
+      load16(src + (first - pos) + 16 * q, w);
+      *reinterpret_cast<uint4*>(st + first + 16 * q) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+  li++;
+}
+
+// Chunk c of the stage grid: from its source when it lies in listed stretch
+// *k (k advances along the list), else from the stage.
+__device__ __forceinline__ void enc_fetch(const JobDev& J, const EncWarp& W, const uint8_t* st,
+                                          uint32_t nls, uint32_t c, uint32_t& k,
+                                          uint32_t (&w)[4]) {
+  while (k < nls && c >= (W.ls_c0[k] & ~kEncFromInput) + W.ls_n[k]) k++;
+  const uint32_t c0 = k < nls ? W.ls_c0[k] : 0xffffffffu;
+  if (c0 != 0xffffffffu && c >= (c0 & ~kEncFromInput)) {
+    const uint8_t* base = (c0 & kEncFromInput) ? J.in : J.keys;
+    load16(base + W.ls_src[k] + 16 * (c - (c0 & ~kEncFromInput)), w);
+  } else {
+    const uint4 v = *reinterpret_cast<const uint4*>(st + 16 * c);
+    w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
+  }
+}
+
+// Chunk at stage position p out to global memory when it lies wholly inside
+// the message [m0, m1) (block and type byte), and into the lane's CRC share.
+__device__ __forceinline__ void enc_chunk_out(const uint32_t* h5, uint8_t* gbase, uint32_t p,
+                                              uint32_t m0, uint32_t m1, const uint32_t (&w)[4],
+                                              uint32_t& u, uint32_t& last) {
+  if (p >= m0 && p + 16 <= m1)
+    *reinterpret_cast<uint4*>(gbase + p) = make_uint4(w[0], w[1], w[2], w[3]);
+  u = crc_chunk_step(h5, u, p, m0, m1, w[0], w[1], w[2], w[3]);
+  last = p;
 }
 
 __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_h5[kCrcH5Words];
+  __shared__ uint32_t s_xinv[kCrcXinvN];
   extern __shared__ __align__(16) uint8_t enc_smem[];
-  uint32_t* tab4 = reinterpret_cast<uint32_t*>(enc_smem);  // 4 x 256 words
-  crc_tables4_init(tab4);
+  for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = J.crc_h5[i];
+  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = J.crc_xinv[i];
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem + 4096)[warp];
+  EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem)[warp];
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t R = J.restart_interval;
-  const uint8_t* keys = J.keys;
-  const uint8_t* in = J.in;
+  uint8_t* st = W.stage;
   for (uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp; b < nb;
        b += (uint64_t)gridDim.x * kEncWarps) {
     const FileOut& F = J.files[J.b_file[b]];
@@ -704,139 +753,79 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     const uint64_t s = J.b_first[b];
     const uint32_t n = (uint32_t)(J.b_first[b + 1] - s);
     const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
-    if (n > kEncMaxEnt || ph + bsz + kTrailer + 16 > kEncStage) {
-      enc_direct(J, tab4, b, dst, lane);
+    if (ph + bsz + kTrailer + 16 > kEncStage) {
+      enc_direct(J, s_h5, s_xinv, b, dst, lane);
       continue;
     }
-    uint8_t* st = W.stage;
-    // 1. entry table
-    uint32_t carry = 0, ccarry = 0;
+    const uint32_t nrest = (n + R - 1) / R;
+    const uint32_t rbase = ph + bsz - 4 * nrest - 4;  // stage position of the restart array
+    // 1. entries: headers, restart words, short stretches, cut edges, list
+    uint32_t carry = 0, lcarry = 0;
     for (uint32_t j0 = 0; j0 < n; j0 += 32) {
       const uint32_t j = j0 + lane;
-      uint32_t size = 0, hl = 0, kd = 0, vl = 0;
+      uint32_t size = 0, hl = 0, kd = 0, vl = 0, sh = 0, koff = 0, voff = 0;
       if (j < n) {
         const uint64_t k = s + j;
         const uint32_t kl = J.k_klen[k];
-        const uint32_t sh = (j % R == 0) ? 0 : J.k_shared[k];
+        sh = (j % R == 0) ? 0 : J.k_shared[k];
         kd = kl - sh;
         vl = J.k_vlen[k];
+        koff = J.k_koff[k] + sh;
+        voff = J.k_voff[k];
         hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
         size = hl + kd + vl;
-        W.ksrc[j] = J.k_koff[k] + sh;
-        W.vsrc[j] = J.k_voff[k];
-        W.kd[j] = kd;
-        W.vl[j] = vl;
-        W.sh[j] = sh;
       }
-      uint32_t tot;
+      uint32_t tot, ltot;
       const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
-      uint32_t nq = 0;
+      const uint32_t nl = j < n ? (uint32_t)(kd >= kEncLong) + (uint32_t)(vl >= kEncLong) : 0u;
+      uint32_t li = warp_excl<uint32_t>(nl, &ltot) + lcarry;
+      carry += tot;
+      lcarry += ltot;
       if (j < n) {
-        W.off[j] = ex;
-        W.kbeg[j] = ex + hl;
-        uint32_t first;
-        if (kd >= kEncLong) nq += chunks_in(ph + ex + hl, ph + ex + hl + kd, &first);
-        if (vl >= kEncLong) nq += chunks_in(ph + ex + hl + kd, ph + ex + size, &first);
+        uint8_t* p = st + ph + ex;
+        p = put_varint(p, sh);
+        p = put_varint(p, kd);
+        put_varint(p, vl);
+        if (j % R == 0) {
+          const uint32_t rem = n - j;
+          st_le32(st + rbase + 4 * (j / R), (ex << 8) | (rem < R ? rem : R));
+        }
         if (J.dec_vpos)  // the value's place in its file, for the decoded form
           J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + kd);
-      }
-      uint32_t ctot;
-      const uint32_t cx = warp_excl<uint32_t>(nq, &ctot) + ccarry;
-      if (j < n) W.cc[j] = cx;
-      carry += tot;
-      ccarry += ctot;
-    }
-    if (lane == 0) {
-      W.off[n] = carry;
-      W.cc[n] = ccarry;
-    }
-    __syncwarp();
-    const uint32_t rbase = carry;  // restart array, then the restart count
-    const uint32_t nrest = (n + R - 1) / R;
-    // 2. headers, short stretches, edges, restart words
-    for (uint32_t j = lane; j < n; j += 32) {
-      const uint32_t o = W.off[j], kb = W.kbeg[j], kd = W.kd[j], vl = W.vl[j];
-      uint8_t* p = st + ph + o;
-      p = put_varint(p, W.sh[j]);
-      p = put_varint(p, kd);
-      put_varint(p, vl);
-      stretch_bytes(st, ph + kb, ph + kb + kd, keys + W.ksrc[j], kd >= kEncLong);
-      stretch_bytes(st, ph + kb + kd, ph + kb + kd + vl, in + W.vsrc[j], vl >= kEncLong);
-      if (j % R == 0) {
-        const uint32_t rem = n - j;
-        st_le32(st + ph + rbase + 4 * (j / R), (o << 8) | (rem < R ? rem : R));
+        const uint32_t kpos = ph + ex + hl;
+        enc_stretch(W, st, kpos, kd, J.keys, koff, 0u, li);
+        enc_stretch(W, st, kpos + kd, vl, J.in, voff, kEncFromInput, li);
       }
     }
     if (lane == 0) {
       st_le32(st + ph + bsz - 4, nrest);
       st[ph + bsz] = 0;  // kNoCompression
     }
-    // 3. the long stretches' chunks
-    const uint32_t nchunks = W.cc[n];
-    for (uint32_t c0 = lane; c0 < nchunks; c0 += 32 * kEncChunks) {
-      uint32_t w[kEncChunks][5];
-      uint32_t sh8[kEncChunks], at[kEncChunks];
-#pragma unroll
-      for (uint32_t u = 0; u < kEncChunks; u++) {
-        const uint32_t c = c0 + 32 * u;
-        at[u] = 0xffffffffu;
-        if (c < nchunks) {
-          // the entry holding chunk c: last j with cc[j] <= c
-          uint32_t lo = 0, hi = n;
-          while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (W.cc[mid] <= c) lo = mid;
-            else hi = mid;
-          }
-          const uint32_t j = lo, kb = W.kbeg[j], kd = W.kd[j];
-          uint32_t q = c - W.cc[j], first, nq = 0;
-          if (kd >= kEncLong) nq = chunks_in(ph + kb, ph + kb + kd, &first);
-          const uint8_t* src;
-          if (q < nq) {
-            src = keys + W.ksrc[j] + (first + 16 * q - (ph + kb));
-          } else {
-            q -= nq;
-            chunks_in(ph + kb + kd, ph + kb + kd + W.vl[j], &first);
-            src = in + W.vsrc[j] + (first + 16 * q - (ph + kb + kd));
-          }
-          at[u] = first + 16 * q;
-          const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-          const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-          sh8[u] = 8 * (uint32_t)(a & 3);
-#pragma unroll
-          for (int i = 0; i < 4; i++) w[u][i] = __ldg(base + i);
-          // the fifth word holds needed bytes only when the source is not
-          // word aligned (never read past the stretch)
-          w[u][4] = sh8[u] ? __ldg(base + 4) : 0u;
-        }
-      }
-#pragma unroll
-      for (uint32_t u = 0; u < kEncChunks; u++) {
-        if (at[u] == 0xffffffffu) continue;
-        uint4 v;
-        v.x = __funnelshift_r(w[u][0], w[u][1], sh8[u]);
-        v.y = __funnelshift_r(w[u][1], w[u][2], sh8[u]);
-        v.z = __funnelshift_r(w[u][2], w[u][3], sh8[u]);
-        v.w = __funnelshift_r(w[u][3], w[u][4], sh8[u]);
-        *reinterpret_cast<uint4*>(st + at[u]) = v;
-      }
-    }
     __syncwarp();
-    // 4. CRC32C of the block and its type byte
-    const uint32_t crc = warp_block_crc_smem(J, tab4, st + ph, bsz);
-    if (lane == 0) st_le32(st + ph + bsz + 1, crc);
-    __syncwarp();
-    // 5. block and trailer out
-    const uint32_t end = ph + bsz + kTrailer;
+    // 2. chunks: out to global memory and into the CRC, two per lane at a time
+    const uint32_t nls = min(lcarry, kEncMaxLong);
+    const uint32_t m0 = ph, m1 = ph + bsz + 1;
     uint8_t* gbase = dst - ph;
-    const uint32_t nch = (end + 15) >> 4;
-    for (uint32_t c = lane; c < nch; c += 32) {
-      const uint32_t a = 16 * c;
-      if (a >= ph && a + 16 <= end) {
-        *reinterpret_cast<uint4*>(gbase + a) = *reinterpret_cast<const uint4*>(st + a);
-      } else {
-        for (uint32_t x = max(a, ph); x < min(a + 16, end); x++) gbase[x] = st[x];
-      }
+    uint32_t u = 0, last = 0xffffffffu, k = 0;
+    for (uint32_t c = lane; 16 * c < m1; c += 64) {
+      uint32_t a[4], a2[4];
+      const bool two = 16 * (c + 32) < m1;
+      enc_fetch(J, W, st, nls, c, k, a);
+      if (two) enc_fetch(J, W, st, nls, c + 32, k, a2);
+      enc_chunk_out(s_h5, gbase, 16 * c, m0, m1, a, u, last);
+      if (two) enc_chunk_out(s_h5, gbase, 16 * (c + 32), m0, m1, a2, u, last);
+    }
+    // 3. CRC, trailer, partial chunks at both ends
+    const uint32_t crc = crc_rows_finish(s_xinv, u, last, m1);
+    if (lane == 0) st_le32(st + m1, crc);
+    __syncwarp();
+    const uint32_t cf0 = (m0 + 15) >> 4, cf1 = m1 >> 4;  // whole chunks [cf0, cf1) went out
+    uint32_t h1 = 16 * cf0, t0 = 16 * cf1;
+    if (cf1 < cf0) h1 = t0 = m0;  // the message lies inside one chunk
+    const uint32_t nh = h1 - m0, nt = m1 + 4 - t0;
+    for (uint32_t x = lane; x < nh + nt; x += 32) {
+      const uint32_t q = x < nh ? m0 + x : t0 + (x - nh);
+      gbase[q] = st[q];
     }
     __syncwarp();
   }
@@ -1171,7 +1160,7 @@ void encode_kernel_attributes() {
 }
 
 void launch_encode_blocks(const Batch& bt, cudaStream_t st) {
-  // grid-stride over the device-side block count: 5 CTAs per SM x 4 waves,
+  // grid-stride over the device-side block count: 3 CTAs per SM x 4 waves,
   // shared out among the jobs
   note_launch(), k_encode_blocks<<<dim3(grid_x(bt.max_entries, kEncWarps, per_job(bt, 148 * 3 * 4)),
                                         bt.B), kEncWarps * 32, kEncSmem, st>>>(bt.d);

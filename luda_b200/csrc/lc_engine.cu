@@ -478,6 +478,7 @@ const char* err_name(uint32_t code) {
     case kErrRetryExact: return "single-pass key arena too small";
     case kErrLimit: return "engine limit exceeded";
     case kErrChecksum: return "block checksum mismatch";
+    case kErrUnsorted: return "input entries out of internal-key order";
     default: return "unknown";
   }
 }
@@ -503,6 +504,8 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.max_gp_overlap = (int64_t)(10 * j->opt.max_file_size);  // db/version_set.cc:31-33
   J.crc_xpow = e->crc_xpow;
   J.crc_xpow_n = kCrcXpowN;
+  J.crc_h5 = e->crc_xpow + kCrcXpowN;
+  J.crc_xinv = J.crc_h5 + kCrcH5Words;
   J.chunk = kChunk;
   J.chain_smem_words = 11 * 1024;  // 44 KiB (static shared memory takes the rest of 48)
 }
@@ -1716,12 +1719,50 @@ void fill_out(lc_job* j, lc_job_out* o) {
   o->decoded_inputs = j->decoded_inputs;
 }
 
-void host_crc_xpow(std::vector<uint32_t>& t) {
-  t.resize(kCrcXpowN);
+// The engine's CRC tables, one device array: [x^(8n) | row fields | x^(-8n)].
+//  * x^(8n) mod P for n < kCrcXpowN (register shifts by n zero bytes);
+//  * for the row CRC of the block encoder: entry 32 i + v is the register
+//    after 16 bytes holding v at bits [5i, 5i + 5) and zero elsewhere, then
+//    kCrcRowBytes - 16 zero bytes, from register 0;
+//  * x^(-8n) mod P for n < kCrcXinvN: the shift that undoes n zero bytes.
+// Registers are reflected (bit 31 is x^0), as in util/crc32c.cc.
+uint32_t host_crc_byte(uint32_t c, uint8_t b) {
+  c ^= b;
+  for (int k = 0; k < 8; k++) c = (c & 1) ? (c >> 1) ^ kCrcPoly : (c >> 1);
+  return c;
+}
+
+void host_crc_tables(std::vector<uint32_t>& t) {
+  t.assign(kCrcXpowN + kCrcH5Words + kCrcXinvN, 0);
   uint32_t c = 0x80000000u;  // x^0
   for (uint32_t m = 0; m < kCrcXpowN; m++) {
     t[m] = c;
-    for (int b = 0; b < 8; b++) c = (c & 1) ? (c >> 1) ^ kCrcPoly : (c >> 1);
+    c = host_crc_byte(c, 0);
+  }
+  uint32_t* h5 = t.data() + kCrcXpowN;
+  for (uint32_t i = 0; i < kCrcH5Fields; i++)
+    for (uint32_t v = 0; v < 32; v++) {
+      uint8_t x[16] = {};
+      for (uint32_t bit = 0; bit < 5; bit++) {
+        const uint32_t at = 5 * i + bit;
+        if (((v >> bit) & 1) && at < 128) x[at >> 3] |= (uint8_t)(1u << (at & 7));
+      }
+      uint32_t r = 0;
+      for (uint32_t k = 0; k < 16; k++) r = host_crc_byte(r, x[k]);
+      for (uint32_t k = 16; k < kCrcRowBytes; k++) r = host_crc_byte(r, 0);
+      h5[32 * i + v] = r;
+    }
+  // one zero byte maps c to byte(c & 0xff) ^ (c >> 8), where byte(i) =
+  // host_crc_byte(0, i): its top byte names i (the table's top bytes are a
+  // permutation), which undoes the step
+  uint32_t by_top[256];
+  for (uint32_t i = 0; i < 256; i++) by_top[host_crc_byte(0, (uint8_t)i) >> 24] = i;
+  uint32_t* xinv = h5 + kCrcH5Words;
+  c = 0x80000000u;
+  for (uint32_t n = 0; n < kCrcXinvN; n++) {
+    xinv[n] = c;
+    const uint32_t i = by_top[c >> 24];
+    c = ((c ^ host_crc_byte(0, (uint8_t)i)) << 8) | i;
   }
 }
 
@@ -1788,7 +1829,7 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     merge_kernel_attributes();
     CK(cudaGetLastError());
     std::vector<uint32_t> t;
-    host_crc_xpow(t);
+    host_crc_tables(t);
     CK(cudaMalloc(&e->crc_xpow, t.size() * 4));
     CK(cudaMemcpy(e->crc_xpow, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
     for (int i = 0; i < e->max_inflight; i++) {

@@ -32,6 +32,7 @@ enum : uint32_t {
   kErrRetryExact = 8,     // the single-pass decode's bounded key arena (or key length
                           // bound) was too small: the host reruns the job with counting
   kErrChecksum = 9,       // a data block's stored CRC32C does not match its contents
+  kErrUnsorted = 10,      // a merge child's entries are not in internal-key order
 };
 
 struct Counters {
@@ -250,6 +251,8 @@ struct JobDev {
   // CRC32C shift table: x^(8m) mod P for m in [0, crc_tab_n)
   const uint32_t* crc_xpow;
   uint32_t crc_xpow_n;
+  const uint32_t* crc_h5;     // kCrcH5Words: the 5-bit field tables of the row CRC
+  const uint32_t* crc_xinv;   // kCrcXinvN: x^(-8n) mod P, back shifts by n bytes
 };
 
 }  // namespace lc

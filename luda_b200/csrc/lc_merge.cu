@@ -87,17 +87,56 @@ __global__ void k_key_skip(const JobDev* __restrict__ jobs) {
   }
 }
 
-// e_pfx after the job's common bytes (only when there are some: the decode
-// wrote the prefixes from the keys' first byte).
+// True when entry e is the first of its merge child.
+__device__ __forceinline__ bool run_first(const JobDev& J, uint64_t e) {
+  // the last child whose first entry is at or before e
+  uint32_t lo = 0, hi = J.n_runs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (J.run_entry_begin[mid] <= e) lo = mid;
+    else hi = mid;
+  }
+  return J.run_entry_begin[lo] == e;
+}
+
+// e_pfx after the job's common bytes (the decode wrote the prefixes from the
+// keys' first byte), and a check of the merge children's order: every key
+// starts with the common bytes and sorts at or after the entry before it in
+// its child.  table/merger.cc merges children it trusts to be sorted; a child
+// out of order fails the job here (kErrUnsorted) rather than reaching the
+// merge path, whose cuts assume sorted children.
 __global__ void k_prefix(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   if (J.ctr->error) return;
   const uint32_t L = J.ctr->key_skip;
-  if (L == 0) return;
   const uint64_t n = J.ctr->n_entries_in;
+  if (n == 0) return;
+  const uint8_t* k0 = J.keys + J.e_koff[0];
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (uint64_t)gridDim.x * blockDim.x)
-    J.e_pfx[e] = user_prefix_after(J.keys + J.e_koff[e], J.e_klen[e], L);
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint8_t* k = J.keys + J.e_koff[e];
+    const uint32_t kl = J.e_klen[e];  // >= 8: shorter keys failed the decode
+    bool bad = false;
+    uint64_t p;
+    if (L) {
+      if (kl - 8 < L) {
+        bad = true;
+      } else {
+        for (uint32_t i = 0; i < L; i++) bad |= k[i] != k0[i];
+      }
+      p = user_prefix_after(k, kl, L);
+      J.e_pfx[e] = p;  // neighbours recompute theirs from the key bytes
+    } else {
+      p = J.e_pfx[e];
+    }
+    if (!bad && e > 0 && !run_first(J, e)) {
+      const uint8_t* kp = J.keys + J.e_koff[e - 1];
+      const uint32_t klp = J.e_klen[e - 1];
+      const uint64_t pp = L ? (klp - 8 < L ? 0 : user_prefix_after(kp, klp, L)) : J.e_pfx[e - 1];
+      bad = pp > p || (pp == p && ikey_cmp(kp, klp, k, kl) > 0);
+    }
+    if (bad) set_error(J.ctr, kErrUnsorted, (uint32_t)e);
+  }
 }
 
 // A single merge child (no round): the merged order is the input order.
@@ -225,6 +264,12 @@ __global__ void __launch_bounds__(1024) k_merge_tile(const JobDev* __restrict__ 
     if (!merge_tile(J, r, g, tile, &t)) break;
     const uint64_t i0 = J.m_split[g];
     const uint64_t i1 = t.last ? t.na : J.m_split[g + 1];
+    if (i1 < i0 || i1 - i0 > t.d1 - t.d0) {
+      // cuts out of order: only children out of order give these, and the
+      // order check fails such a job first; the tile is skipped, never read
+      if (threadIdx.x == 0) set_error(J.ctr, kErrUnsorted, (uint32_t)g);
+      continue;
+    }
     const uint64_t j0 = t.d0 - i0, j1 = t.d1 - i1;
     const uint32_t na = (uint32_t)(i1 - i0), nb = (uint32_t)(j1 - j0), len = na + nb;
     __syncthreads();  // the previous tile's stores have read the buffers
