@@ -223,56 +223,6 @@ __device__ __forceinline__ const DecRun& pseudo_block(const JobDev& J, uint64_t 
   return R;
 }
 
-// Entry descriptors of a pseudo block (key lengths, value places and
-// lengths); its key bytes, one lane per entry.  Returns the key bytes and
-// the longest key; false if a key is shorter than 8 bytes or a value lies
-// outside its table.
-__device__ __forceinline__ bool pseudo_entries(const JobDev& J, uint64_t b, uint64_t ebase,
-                                               uint32_t lane, uint32_t lanes, uint64_t* kbytes,
-                                               uint32_t* maxk) {
-  uint32_t t;
-  uint64_t j0, j1;
-  const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
-  const TableDesc T = J.tables[t];
-  bool ok = true;
-  uint32_t mk = 0;
-  for (uint64_t j = j0 + lane; j < j1; j += lanes) {
-    const uint64_t e = ebase + (j - j0);
-    const uint32_t kl = (uint32_t)(R.kcum[j + 1] - R.kcum[j]);
-    const uint32_t vl = R.vlen[j], vp = R.vpos[j];
-    if (kl < 8 || (uint64_t)vp + vl > T.size || e >= J.cap_entries) {
-      ok = false;
-      continue;
-    }
-    J.e_klen[e] = kl;
-    J.e_vlen[e] = vl;
-    J.e_voff[e] = (uint32_t)(T.off + vp);
-    mk = max(mk, kl);
-  }
-  *kbytes = R.kcum[j1] - R.kcum[j0];
-  *maxk = mk;
-  return ok;
-}
-
-// Key bytes (one contiguous copy), key offsets, prefixes and tags of a
-// pseudo block, by one warp; its keys start at kbase in the arena.
-__device__ __forceinline__ void pseudo_keys(const JobDev& J, uint64_t b, uint64_t ebase,
-                                            uint64_t kbase, uint32_t lane) {
-  uint32_t t;
-  uint64_t j0, j1;
-  const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
-  const uint64_t k0 = R.kcum[j0], kn = R.kcum[j1] - k0;
-  const uint8_t* src = R.keys + k0;
-  uint8_t* dst = J.keys + kbase;
-  for (uint64_t x = lane; x < kn; x += 32) dst[x] = src[x];
-  for (uint64_t j = j0 + lane; j < j1; j += 32) {
-    const uint64_t e = ebase + (j - j0);
-    J.e_koff[e] = (uint32_t)(kbase + (R.kcum[j] - k0));
-    J.e_pfx[e] = R.pfx[j];
-    J.e_tag[e] = R.tag[j];
-  }
-}
-
 // Walks the entries of one restart run without writing them: counts key bytes
 // and validates every header against the run's bounds.
 __device__ __forceinline__ bool walk_run(const uint8_t* p, const uint8_t* lim, uint32_t cnt,
@@ -323,20 +273,14 @@ __device__ __forceinline__ void run_bounds(const BlockView& v, uint32_t r, uint6
   *end = (r + 1 < v.nr) ? (ld_le32(v.p + v.ra + 4ull * (r + 1)) >> 8) : v.ra;
 }
 
-// Per-warp shared memory of the staged decode kernels.
+// Per-warp shared memory of the counting walk (k_block_count), and the key
+// buffers of the decode.
 constexpr uint32_t kDecWarps = 4;
 constexpr uint32_t kDecStage = 8448;    // data block bytes + 16-byte phase
-constexpr uint32_t kDecMaxEnt = 512;    // entries of one staged block
-constexpr uint32_t kDecKeyBuf = 32 * 132 + 32;  // 4 KiB of keys, or 32 lane slices of 132 bytes
-constexpr uint32_t kDecLastKey = 256;   // longest key the staged path rebuilds
+constexpr uint32_t kDecKeyBuf = 4096 + 32;  // a round's keys + phase
+constexpr uint32_t kDecLastKey = 256;   // longest key the decode's buffers carry
 struct DecWarpSmem {
   uint8_t stage[kDecStage];
-  uint8_t keybuf[kDecKeyBuf];
-  uint16_t dpos[kDecMaxEnt];  // key delta position in the stage
-  uint16_t sh[kDecMaxEnt];    // shared prefix
-  uint16_t kl[kDecMaxEnt];    // key length
-  uint16_t vl[kDecMaxEnt];    // value length
-  uint8_t lastkey[kDecLastKey];  // last key of the previous group of 32 entries
 };
 
 // Copies data block b into this warp's stage at the block's own 16-byte phase
@@ -514,495 +458,290 @@ __global__ void k_run_bounds(const JobDev* __restrict__ jobs) {
   if (blockIdx.x == 0 && threadIdx.x == 0) J.run_entry_begin_w[J.n_runs] = J.ctr->n_entries_in;
 }
 
-// Decode of one block straight from global memory, one lane per restart run:
-// the path for blocks that do not fit the shared-memory stage.
-__device__ void decode_direct(const JobDev& J, uint64_t b, uint32_t lane) {
-  BlockView v = block_view(J, b, J.in + J.blk_off[b]);
-  uint64_t ent_carry = J.blk_ent_base[b];
-  uint64_t key_carry;
-  if (J.reserve_keys) {
-    // single pass: check every run and sum the block's key bytes first, then
-    // reserve them in the key arena
+// ---------------------------------------------------------------------------
+// Decode of the data blocks into the entry arrays, in two passes.
+//
+// Pass 1 (k_decode_walk): one warp per group of dec_group consecutive data
+// blocks (32, or 8 for blocks of many entries).  The group's restart runs,
+// one lane per run in rounds of 32, walk their entry headers straight from
+// global memory (the lines a run's headers lie in are read once, through L1)
+// with the checks of the counting walk, and write one 16-byte record per
+// entry -- where its key delta lies, its shared and key lengths, its value's
+// length and place -- and its key length.  A pseudo block (a decoded run,
+// from the decoded form of an earlier output) is cut into runs of
+// kDecRunSlice entries whose records come from that form.
+//
+// A scan of the key lengths gives every key its place in the arena (keys in
+// entry order).
+//
+// Pass 2 (k_decode_keys): one warp per unit of about kDecUnit entries, cut
+// at entries without a shared prefix (every restart has none), in rounds of
+// 32, one lane per entry: each lane copies its key delta into the warp's key
+// buffer at the key's place; the shared prefixes then follow in entry order
+// (a key's prefix is the head of the previous key, complete by then); the
+// round's keys go out to the arena with 16-byte stores and the entry arrays
+// with coalesced stores.  The round's last key carries into the next round;
+// a round whose keys do not fit the buffer is built in the arena directly.
+constexpr uint32_t kDecGroupMax = 32;   // data blocks per warp in pass 1
+constexpr uint32_t kDecRunSlice = 16;   // pseudo-block entries per lane
+constexpr uint32_t kDecUnit = 256;      // entries per warp in pass 2
+constexpr uint32_t kDecPseudo = 0xffffu;  // shared length of a pseudo entry's record
+
+// Record of entry e: x key delta offset in `in` (a pseudo entry: its block),
+// y shared length | key length << 16, z value length, w value offset in `in`.
+__device__ __forceinline__ uint4 dec_record(uint32_t src, uint32_t sh, uint32_t kl, uint32_t vl,
+                                            uint32_t voff) {
+  return make_uint4(src, sh | (kl << 16), vl, voff);
+}
+
+__global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  __shared__ uint32_t s_rb[8][kDecGroupMax + 1];  // per warp: first run of each block of its group
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (J.ctr->error) return;
+  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
+  const uint32_t G = J.dec_group;
+  const uint64_t ngrp = (nblk + G - 1) / G;
+  for (uint64_t g = (uint64_t)blockIdx.x * 8 + warp; g < ngrp; g += (uint64_t)gridDim.x * 8) {
+    const uint64_t g0 = g * G;
+    // runs of the lane's block (a pseudo block: slices of its entries)
+    uint32_t nr = 0;
+    if (lane < G && g0 + lane < nblk) {
+      const uint64_t b = g0 + lane;
+      const uint32_t size = J.blk_size[b];
+      if (size == kPseudoBlock) {
+        nr = (J.blk_nent[b] + kDecRunSlice - 1) / kDecRunSlice;
+      } else {
+        nr = ld_le32(J.in + J.blk_off[b] + size - 4);  // checked by k_block_restarts
+      }
+    }
+    uint32_t nrt;
+    s_rb[warp][lane] = warp_excl<uint32_t>(nr, &nrt);
+    if (lane == 0) s_rb[warp][kDecGroupMax] = nrt;
+    __syncwarp();
     uint64_t kb = 0;
     uint32_t maxk = 0;
-    bool ok = v.ok, sk = false;
-    for (uint32_t r = lane; ok && r < v.nr; r += 32) {
-      uint64_t s, e, rk = 0;
-      uint32_t cnt;
-      run_bounds(v, r, &s, &e, &cnt);
-      if (s > e || e > v.ra || !walk_run(v.p + s, v.p + e, cnt, &rk, &maxk, &sk)) ok = false;
-      kb += rk;
-    }
-    const bool all_ok = __all_sync(0xffffffffu, ok);
-    const bool any_short = __any_sync(0xffffffffu, sk);
-    kb = warp_sum(kb);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
-    uint64_t base = 0;
-    int fail = 0;
-    if (lane == 0) {
-      fail = 1;
-      if (!all_ok) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
-      else if (any_short) set_error(J.ctr, kErrShortKey, (uint32_t)b);
-      else if (maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-      else {
-        base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
-        if (base + kb > J.cap_key_bytes) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-        else fail = 0;
+    bool bad = false, short_key = false, long_key = false;
+    for (uint32_t q0 = 0; q0 < nrt; q0 += 32) {
+      const uint32_t q = q0 + lane;
+      if (q >= nrt) continue;
+      // the block of run q: the last with its first run at or before q
+      uint32_t lo = 0, hi = G;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_rb[warp][mid] <= q) lo = mid;
+        else hi = mid;
       }
-      atomicMax(&J.ctr->max_klen, maxk);
-    }
-    if (__shfl_sync(0xffffffffu, fail, 0)) return;
-    key_carry = __shfl_sync(0xffffffffu, base, 0);
-  } else {
-    key_carry = J.blk_key_base[b];
-  }
-  for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
-    const uint32_t r = r0 + lane;
-    uint64_t s = 0, e = 0, rk = 0;
-    uint32_t cnt = 0, maxk = 0;
-    bool sk = false;
-    if (r < v.nr) {
-      run_bounds(v, r, &s, &e, &cnt);
-      walk_run(v.p + s, v.p + e, cnt, &rk, &maxk, &sk);
-    }
-    uint64_t cnt_tot, kb_tot;
-    uint64_t ent = warp_excl<uint64_t>(cnt, &cnt_tot) + ent_carry;
-    uint64_t kpos = warp_excl<uint64_t>(rk, &kb_tot) + key_carry;
-    ent_carry += cnt_tot;
-    key_carry += kb_tot;
-    if (r < v.nr) {
-      const uint8_t* p = v.p + s;
-      const uint8_t* lim = v.p + e;
-      uint64_t prev = kpos;
-      for (uint32_t k = 0; k < cnt; k++) {
-        uint32_t sh, ns, vl;
-        const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
-        if (!q) break;
-        const uint32_t kl = sh + ns;
-        if (kpos + kl > J.cap_key_bytes || ent >= J.cap_entries) {
-          set_error(J.ctr, kErrArenaOverflow, (uint32_t)b);
-          return;
+      const uint64_t b = g0 + lo;
+      const uint32_t r = q - s_rb[warp][lo];
+      const uint64_t ebase = J.blk_ent_base[b];
+      const uint32_t size = J.blk_size[b];
+      if (size == kPseudoBlock) {
+        uint32_t t;
+        uint64_t j0, j1;
+        const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
+        const TableDesc& T = J.tables[t];
+        const uint64_t ja = j0 + (uint64_t)r * kDecRunSlice, jz = min(j1, ja + kDecRunSlice);
+        for (uint64_t j = ja; j < jz; j++) {
+          const uint32_t kl = (uint32_t)(R.kcum[j + 1] - R.kcum[j]);
+          const uint32_t vl = R.vlen[j], vp = R.vpos[j];
+          if (kl < 8) short_key = true;
+          if (kl > 0xffff) long_key = true;
+          if ((uint64_t)vp + vl > T.size) bad = true;
+          const uint64_t e = ebase + (j - j0);
+          J.e_rec[e] = dec_record((uint32_t)b, kDecPseudo, kl, vl, (uint32_t)(T.off + vp));
+          J.e_klen[e] = kl;
+          kb += kl;
+          maxk = max(maxk, kl);
         }
-        uint8_t* dst = J.keys + kpos;
-        for (uint32_t i = 0; i < sh; i++) dst[i] = J.keys[prev + i];
-        for (uint32_t i = 0; i < ns; i++) dst[sh + i] = q[i];
-        J.e_koff[ent] = (uint32_t)kpos;
-        J.e_klen[ent] = kl;
-        J.e_voff[ent] = (uint32_t)((q + ns) - J.in);
-        J.e_vlen[ent] = vl;
-        J.e_pfx[ent] = user_prefix(dst, kl);
-        J.e_tag[ent] = ld_le64(dst + kl - 8);
-        prev = kpos;
-        kpos += kl;
-        ent++;
-        p = q + ns + vl;
+        continue;
       }
-    }
-  }
-}
-
-// Decode of one staged block.  Lanes first walk the restart runs (one lane
-// per run, headers only) and record every entry's key-delta position, shared
-// prefix and lengths; then, 32 entries at a time, the warp rebuilds the keys
-// in entry order in shared memory (lanes over bytes: the shared prefix is the
-// front of the previous key, already rebuilt), writes them out with 16-byte
-// stores, and writes the descriptors one lane per entry.
-__device__ bool decode_staged(const JobDev& J, uint64_t b, uint32_t lane, const uint8_t* st,
-                              DecWarpSmem& W) {
-  BlockView v = block_view(J, b, st);
-  const uint32_t nent = J.blk_nent[b];
-  if (nent > kDecMaxEnt) return false;
-  // pass 1: headers of every entry, one lane per restart run; the checks of
-  // the counting walk (bounds, no shared prefix at a restart, shared prefix
-  // within the previous key, runs parsed exactly to their end, keys of at
-  // least 8 bytes) are made here too
-  uint32_t carry = 0;
-  bool long_key = false, bad = !v.ok, short_key = false;
-  uint64_t rk = 0;
-  uint32_t maxk = 0;
-  for (uint32_t r0 = 0; r0 < v.nr; r0 += 32) {
-    const uint32_t r = r0 + lane;
-    uint64_t s = 0, e = 0;
-    uint32_t cnt = 0;
-    if (r < v.nr) run_bounds(v, r, &s, &e, &cnt);
-    uint32_t tot;
-    const uint32_t e0 = warp_excl<uint32_t>(cnt, &tot) + carry;
-    carry += tot;
-    if (r < v.nr) {
-      if (s > e || e > v.ra) bad = true;
-      const uint8_t* p = st + s;
-      const uint8_t* lim = st + (e > v.ra ? v.ra : e);
-      uint32_t prev = 0;
-      for (uint32_t k = 0; k < cnt && !bad; k++) {
-        uint32_t sh, ns, vl;
-        const uint8_t* q = entry_header(p, lim, &sh, &ns, &vl);
-        if (!q || (k == 0 && sh != 0) || sh > prev) {
-          bad = true;
-          break;
-        }
-        const uint32_t kl = sh + ns;
-        const uint32_t idx = e0 + k;
-        if (idx < kDecMaxEnt) {
-          W.dpos[idx] = (uint16_t)(q - st);
-          W.sh[idx] = (uint16_t)sh;
-          W.kl[idx] = (uint16_t)kl;
-          W.vl[idx] = (uint16_t)vl;
-        }
-        if (kl > 0xffff) long_key = true;
-        if (kl < 8) short_key = true;
-        rk += kl;
-        maxk = max(maxk, kl);
-        prev = kl;
-        p = q + ns + vl;
-      }
-      if (!bad && p != lim) bad = true;
-    }
-  }
-  if (J.reserve_keys) {
-    if (__any_sync(0xffffffffu, bad)) {
-      if (lane == 0) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
-      return true;
-    }
-    if (__any_sync(0xffffffffu, short_key)) {
-      if (lane == 0) set_error(J.ctr, kErrShortKey, (uint32_t)b);
-      return true;
-    }
-  }
-  if (__any_sync(0xffffffffu, long_key)) return false;
-  __syncwarp();
-  // pass 2: keys and descriptors, 32 entries at a time
-  const uint64_t ebase = J.blk_ent_base[b];
-  uint64_t kbase;
-  if (J.reserve_keys) {
-    // reserve this block's key bytes in the arena
-    rk = warp_sum(rk);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
-    uint64_t base = 0;
-    bool retry = false;
-    if (lane == 0) {
-      atomicMax(&J.ctr->max_klen, maxk);
-      if (maxk > J.max_key_len) {
-        retry = true;
-      } else {
-        base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)rk);
-        retry = base + rk > J.cap_key_bytes;
-      }
-      if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-    }
-    if (__shfl_sync(0xffffffffu, (int)retry, 0)) return true;
-    kbase = __shfl_sync(0xffffffffu, base, 0);
-  } else {
-    kbase = J.blk_key_base[b];
-  }
-  const uint32_t voff0 = (uint32_t)J.blk_off[b];  // block offset in `in`
-  for (uint32_t g0 = 0; g0 < nent; g0 += 32) {
-    const uint32_t i = g0 + lane;
-    const bool valid = i < nent;
-    const uint32_t kl = valid ? W.kl[i] : 0;
-    uint32_t gk;
-    const uint32_t kofs = warp_excl<uint32_t>(kl, &gk);
-    uint8_t* gdst = J.keys + kbase;
-    const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
-    // the rest of the block goes through the direct path (which rewrites
-    // the whole block) when a group's keys overflow the buffers
-    if (__any_sync(0xffffffffu, kl > kDecLastKey) || gk + kph + 16 > kDecKeyBuf) {
-      // a single-pass block has reserved its key bytes already: a retry of
-      // the whole job with counting keeps the layout simple
-      if (J.reserve_keys) {
-        if (lane == 0) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-        return true;
-      }
-      return false;
-    }
-    uint8_t* kb = W.keybuf + kph;
-    const uint32_t cnt = min(32u, nent - g0);
-    for (uint32_t e = 0; e < cnt; e++) {
-      const uint32_t ie = g0 + e;
-      const uint32_t esh = W.sh[ie], ekl = W.kl[ie], edp = W.dpos[ie];
-      const uint32_t eofs = __shfl_sync(0xffffffffu, kofs, e);
-      const uint32_t pofs = __shfl_sync(0xffffffffu, kofs, (e + 31) & 31);
-      const uint8_t* prev = e == 0 ? W.lastkey : kb + pofs;
-      uint8_t* d = kb + eofs;
-      for (uint32_t t = lane; t < ekl; t += 32) d[t] = t < esh ? prev[t] : st[edp + t - esh];
-      __syncwarp();
-    }
-    {
-      // the group's last key is the next group's first prefix
-      const uint32_t lofs = __shfl_sync(0xffffffffu, kofs, cnt - 1);
-      const uint32_t lkl = W.kl[g0 + cnt - 1];
-      for (uint32_t t = lane; t < lkl; t += 32) W.lastkey[t] = kb[lofs + t];
-    }
-    __syncwarp();
-    // keys out: head bytes, 16-byte body, tail
-    const uint32_t head = (16 - kph) & 15;
-    const uint32_t h = head < gk ? head : gk;
-    if (lane < h) gdst[lane] = kb[lane];
-    const uint32_t body = (gk - h) & ~15u;
-    const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
-    uint4* dv = reinterpret_cast<uint4*>(gdst + h);
-    for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
-    const uint32_t t0 = h + body;
-    if (t0 + lane < gk) gdst[t0 + lane] = kb[t0 + lane];
-    if (valid) {
-      const uint64_t e = ebase + i;
-      const uint32_t ko = (uint32_t)(kbase + kofs);
-      J.e_koff[e] = ko;
-      J.e_klen[e] = kl;
-      J.e_voff[e] = voff0 + W.dpos[i] + (kl - W.sh[i]);
-      J.e_vlen[e] = W.vl[i];
-      J.e_pfx[e] = user_prefix(kb + kofs, kl);
-      J.e_tag[e] = ld_le64(kb + kofs + kl - 8);
-    }
-    kbase += gk;
-    __syncwarp();
-  }
-  return true;
-}
-
-// One block (warp per block): a decoded-run pseudo block, or a staged block,
-// or, when it does not fit the stage, the direct path.
-__device__ __forceinline__ void decode_one(const JobDev& J, uint64_t b, uint32_t lane,
-                                           DecWarpSmem& W) {
-  if (J.blk_size[b] == kPseudoBlock) {
-    uint64_t kb;
-    uint32_t mk;
-    if (!__all_sync(0xffffffffu, pseudo_entries(J, b, J.blk_ent_base[b], lane, 32, &kb, &mk))) {
-      if (lane == 0) set_error(J.ctr, kErrBadEntry, (uint32_t)b);
-      return;
-    }
-    uint64_t kbase = 0;
-    if (J.reserve_keys) {
-      // single pass: reserve the block's key bytes in the arena
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
-      int retry = 0;
-      if (lane == 0) {
-        atomicMax(&J.ctr->max_klen, mk);
-        if (mk > J.max_key_len) {
-          retry = 1;
-        } else {
-          kbase = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)kb);
-          retry = kbase + kb > J.cap_key_bytes;
-        }
-        if (retry) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-      }
-      if (__shfl_sync(0xffffffffu, retry, 0)) return;
-      kbase = __shfl_sync(0xffffffffu, kbase, 0);
-    } else {
-      kbase = J.blk_key_base[b];
-    }
-    pseudo_keys(J, b, J.blk_ent_base[b], kbase, lane);
-    return;
-  }
-  const uint8_t* st = stage_block(J, b, W.stage, lane);
-  if (!st || !decode_staged(J, b, lane, st, W)) decode_direct(J, b, lane);
-  __syncwarp();
-}
-
-// Sparse blocks: few entries with long values (the job's blocks average at
-// most kSparseEnt entries, the block at most 64 KiB).  Staging them would
-// move every value byte for a few header and key bytes, so a warp takes
-// kSparseGroup consecutive blocks: each lane walks its block's restart runs
-// straight from global memory (headers only), recording every entry in the
-// warp's arrays; one atomic reserves all their key spans; then the warp
-// rebuilds each block's keys (shared prefix from the previous key, delta
-// from global memory) and writes keys and descriptors.  Blocks that are not
-// sparse in such a group go through decode_one.
-constexpr uint32_t kSparseEnt = 8;
-constexpr uint32_t kSparseGroup = 32;
-
-__device__ __forceinline__ bool sparse_block(const JobDev& J, uint64_t b) {
-  const uint32_t size = J.blk_size[b], nent = J.blk_nent[b];
-  return size != kPseudoBlock && size <= 0xffff && nent > 0 && nent <= kSparseEnt &&
-         size >= 128u * nent;
-}
-
-__device__ void decode_sparse_group(const JobDev& J, uint64_t g0, uint64_t nblk, uint32_t lane,
-                                    DecWarpSmem& W) {
-  const uint64_t b = g0 + lane;
-  const bool mine = b < nblk && sparse_block(J, b);
-  const unsigned mask = __ballot_sync(0xffffffffu, mine);
-  // 1. one lane per sparse block: headers from global memory
-  bool bad = false, short_key = false;
-  uint32_t kb = 0, maxk = 0, nent = 0;
-  if (mine) {
-    const uint8_t* p = J.in + J.blk_off[b];
-    const uint32_t size = J.blk_size[b];
-    const uint32_t nr = ld_le32(p + size - 4);  // checked by k_block_restarts
-    const uint32_t ra = size - 4 - 4 * nr;
-    nent = J.blk_nent[b];
-    uint32_t e = 0;
-    for (uint32_t r = 0; r < nr && !bad; r++) {
+      const uint8_t* p = J.in + J.blk_off[b];
+      const uint32_t nrb = ld_le32(p + size - 4);
+      const uint32_t ra = size - 4 - 4 * nrb;
       const uint32_t w = ld_le32(p + ra + 4 * r);
       const uint32_t cnt = w & 0xff;
-      const uint8_t* q = p + (w >> 8);
-      const uint8_t* lim = p + ((r + 1 < nr) ? (ld_le32(p + ra + 4 * (r + 1)) >> 8) : ra);
+      const uint32_t s = w >> 8, e = (r + 1 < nrb) ? (ld_le32(p + ra + 4 * (r + 1)) >> 8) : ra;
+      uint32_t before = 0;  // entries of the block's earlier runs
+      for (uint32_t x = 0; x < r; x++) before += ld_le32(p + ra + 4 * x) & 0xff;
+      const uint8_t* qp = p + s;
+      const uint8_t* lim = p + e;  // run ranges checked by k_block_restarts
+      const uint32_t boff = (uint32_t)J.blk_off[b];
       uint32_t prev = 0;
       for (uint32_t k = 0; k < cnt; k++) {
         uint32_t sh, ns, vl;
-        const uint8_t* d = entry_header(q, lim, &sh, &ns, &vl);
-        if (!d || (k == 0 && sh != 0) || sh > prev || e >= nent) {
+        const uint8_t* d = entry_header(qp, lim, &sh, &ns, &vl);
+        if (!d || (k == 0 && sh != 0) || sh > prev) {
           bad = true;
           break;
         }
         const uint32_t kl = sh + ns;
         if (kl < 8) short_key = true;
-        const uint32_t x = lane * kSparseEnt + e;
-        W.dpos[x] = (uint16_t)(d - p);
-        W.sh[x] = (uint16_t)sh;
-        W.kl[x] = (uint16_t)kl;
-        W.vl[x] = (uint16_t)vl;
+        if (kl > 0xffff || sh >= kDecPseudo) long_key = true;
+        const uint32_t doff = boff + (uint32_t)(d - p);
+        J.e_rec[ebase + before + k] = dec_record(doff, sh, kl, vl, doff + ns);
+        J.e_klen[ebase + before + k] = kl;
         kb += kl;
         maxk = max(maxk, kl);
         prev = kl;
-        q = d + ns + vl;
-        e++;
+        qp = d + ns + vl;
       }
-      if (!bad && q != lim) bad = true;
+      if (!bad && qp != lim) bad = true;
     }
-    if (!bad && e != nent) bad = true;
-    if (bad) set_error(J.ctr, kErrBadBlock, (uint32_t)b);
-    else if (short_key) set_error(J.ctr, kErrShortKey, (uint32_t)b);
-    else if (J.reserve_keys && maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)b);
-    atomicMax(&J.ctr->max_klen, maxk);
-  }
-  // 2. key spans: one reservation for the group (single pass), else the scan's
-  const bool ok = mine && !bad && !short_key && (!J.reserve_keys || maxk <= J.max_key_len);
-  const uint32_t need = ok ? kb : 0;
-  uint64_t kbase = 0;
-  if (J.reserve_keys) {
-    uint32_t tot;
-    const uint32_t ex = warp_excl<uint32_t>(need, &tot);
-    uint64_t base = 0;
-    if (lane == 0 && tot)
-      base = atomicAdd((unsigned long long*)&J.ctr->key_cursor, (unsigned long long)tot);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (tot && base + tot > J.cap_key_bytes) {
-      if (lane == 0) set_error(J.ctr, kErrRetryExact, (uint32_t)g0);
-      return;
-    }
-    kbase = base + ex;
-  } else if (mine) {
-    kbase = J.blk_key_base[b];
-  }
-  __syncwarp();
-  // 3. keys rebuilt in entry order and descriptors: one lane per block when
-  // every key of the group fits a lane's 128-byte slice of the key buffer
-  // (slices 132 bytes apart, so that the lanes' byte stores hit distinct
-  // banks), else one block at a time across the warp
-  const unsigned done = __ballot_sync(0xffffffffu, ok);
-  uint32_t gmaxk = maxk;
+    const bool any_bad = __any_sync(0xffffffffu, bad);
+    const bool any_short = __any_sync(0xffffffffu, short_key);
+    const bool any_long = __any_sync(0xffffffffu, long_key);
+    kb = warp_sum(kb);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) gmaxk = max(gmaxk, __shfl_xor_sync(0xffffffffu, gmaxk, o));
-  if (gmaxk <= 128) {
-    if (ok) {
-      const uint8_t* p = J.in + J.blk_off[b];
-      const uint32_t voff0 = (uint32_t)J.blk_off[b];
-      const uint64_t ebase = J.blk_ent_base[b];
-      uint8_t* slice = W.keybuf + lane * 132;
-      uint8_t* gdst = J.keys + kbase;
-      uint32_t kofs = 0;
-      for (uint32_t x = 0; x < nent; x++) {
-        const uint32_t i = lane * kSparseEnt + x;
-        const uint32_t esh = W.sh[i], ekl = W.kl[i], edp = W.dpos[i];
-        for (uint32_t t = esh; t < ekl; t += 32)
-          copy_small(slice + t, p + edp + (t - esh), min(32u, ekl - t));
-        for (uint32_t t = 0; t < ekl; t++) gdst[kofs + t] = slice[t];
-        const uint64_t e = ebase + x;
-        J.e_koff[e] = (uint32_t)(kbase + kofs);
-        J.e_klen[e] = ekl;
-        J.e_voff[e] = voff0 + edp + (ekl - esh);
-        J.e_vlen[e] = W.vl[i];
-        J.e_pfx[e] = user_prefix(slice, ekl);
-        J.e_tag[e] = ld_le64(slice + ekl - 8);
-        kofs += ekl;
-      }
+    for (int o = 16; o > 0; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+    if (lane == 0) {
+      atomicMax(&J.ctr->max_klen, maxk);
+      atomicAdd((unsigned long long*)&J.ctr->key_total, (unsigned long long)kb);
+      if (any_bad) set_error(J.ctr, kErrBadBlock, (uint32_t)g0);
+      else if (any_short) set_error(J.ctr, kErrShortKey, (uint32_t)g0);
+      else if (any_long) set_error(J.ctr, kErrLimit, 4);
+      else if (J.reserve_keys && maxk > J.max_key_len) set_error(J.ctr, kErrRetryExact, (uint32_t)g0);
     }
     __syncwarp();
-  } else
-  for (unsigned m = done; m; m &= m - 1) {
-    const uint32_t L = __ffs(m) - 1;
-    const uint64_t bb = g0 + L;
-    const uint32_t n = __shfl_sync(0xffffffffu, nent, L);
-    const uint64_t kb0 = __shfl_sync(0xffffffffu, kbase, L);
-    const uint8_t* p = J.in + J.blk_off[bb];
-    const uint32_t voff0 = (uint32_t)J.blk_off[bb];
-    const uint64_t ebase = J.blk_ent_base[bb];
-    uint8_t* kbuf = W.keybuf;  // at most kSparseEnt keys of at most 256 bytes (single pass)
-    uint32_t kofs = 0, pofs = 0;
-    const bool fits = __shfl_sync(0xffffffffu, kb, L) <= kDecKeyBuf;
-    uint8_t* gdst = J.keys + kb0;
-    for (uint32_t x = 0; x < n; x++) {
-      const uint32_t i = L * kSparseEnt + x;
-      const uint32_t esh = W.sh[i], ekl = W.kl[i], edp = W.dpos[i];
-      if (fits) {
-        uint8_t* d = kbuf + kofs;
-        for (uint32_t t = lane; t < ekl; t += 32)
-          d[t] = t < esh ? kbuf[pofs + t] : __ldg(p + edp + t - esh);
+  }
+}
+
+// The arena holds every key (k_decode_keys checks it before writing any).
+__global__ void k_decode_fit(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (threadIdx.x == 0 && !J.ctr->error && J.ctr->key_total > J.cap_key_bytes)
+    set_error(J.ctr, J.reserve_keys ? kErrRetryExact : kErrArenaOverflow, 5);
+}
+
+struct DecKeysSmem {
+  uint8_t buf[kDecKeyBuf];    // the round's keys, at the arena's 16-byte phase
+  uint8_t last[kDecLastKey];  // the previous round's last key
+};
+
+// The key bytes a record points at: the key delta in `in`, or a pseudo
+// entry's whole key in its decoded run.
+__device__ __forceinline__ const uint8_t* dec_delta(const JobDev& J, uint64_t e, uint4 rec) {
+  if ((rec.y & 0xffff) == kDecPseudo) {
+    uint32_t t;
+    uint64_t j0, j1;
+    const uint64_t b = rec.x;
+    const DecRun& R = pseudo_block(J, b, &t, &j0, &j1);
+    return R.keys + R.kcum[j0 + (e - J.blk_ent_base[b])];
+  }
+  return J.in + rec.x;
+}
+
+// First entry at or after e (below n) without a shared prefix, else n.
+__device__ __forceinline__ uint64_t dec_unit_start(const JobDev& J, uint64_t e, uint64_t n,
+                                                   uint32_t lane) {
+  for (; e < n; e += 32) {
+    const uint64_t x = e + lane;
+    const uint32_t sh = x < n ? (J.e_rec[x].y & 0xffff) : 1u;
+    const unsigned m = __ballot_sync(0xffffffffu, x < n && (sh == 0 || sh == kDecPseudo));
+    if (m) return e + (__ffs(m) - 1);
+  }
+  return n;
+}
+
+__global__ void __launch_bounds__(256) k_decode_keys(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  __shared__ __align__(16) DecKeysSmem s_w[8];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DecKeysSmem& W = s_w[warp];
+  if (J.ctr->error) return;
+  const uint64_t n = J.ctr->n_entries_in;
+  const uint64_t nunits = (n + kDecUnit - 1) / kDecUnit;
+  for (uint64_t u = (uint64_t)blockIdx.x * 8 + warp; u < nunits; u += (uint64_t)gridDim.x * 8) {
+    const uint64_t e0 = u == 0 ? 0 : dec_unit_start(J, u * kDecUnit, n, lane);
+    const uint64_t e1 = dec_unit_start(J, (u + 1) * kDecUnit, n, lane);
+    bool last_staged = true;  // the previous key is in W.last (not needed at a unit start)
+    uint64_t last_at = 0;     // else its arena offset
+    for (uint64_t r0 = e0; r0 < e1; r0 += 32) {
+      const uint64_t e = r0 + lane;
+      const bool valid = e < e1;
+      const uint32_t cnt = (uint32_t)min(32ull, (unsigned long long)(e1 - r0));
+      const uint4 rec = valid ? J.e_rec[e] : make_uint4(0, 0, 0, 0);
+      const uint32_t kl = rec.y >> 16;
+      const uint32_t sh = (rec.y & 0xffff) == kDecPseudo ? 0 : (rec.y & 0xffff);
+      const uint8_t* src = valid ? dec_delta(J, e, rec) : nullptr;
+      const uint64_t kpos = J.e_koff[r0];  // arena offset of the round's first key
+      uint32_t tot;
+      const uint32_t ko = warp_excl<uint32_t>(kl, &tot);  // offset within the round
+      uint32_t mk = kl;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mk = max(mk, __shfl_xor_sync(0xffffffffu, mk, o));
+      uint8_t* gdst = J.keys + kpos;
+      const uint32_t kph = (uint32_t)(reinterpret_cast<uintptr_t>(gdst) & 15);
+      const uint32_t sh0 = __shfl_sync(0xffffffffu, sh, 0);
+      const uint32_t lkl = __shfl_sync(0xffffffffu, kl, cnt - 1);
+      const uint32_t lko = __shfl_sync(0xffffffffu, ko, cnt - 1);
+      if (tot + kph + 16 <= kDecKeyBuf && mk <= kDecLastKey && (sh0 == 0 || last_staged)) {
+        uint8_t* kb = W.buf + kph;
+        // deltas, every lane at once
+        if (valid) {
+          const uint32_t dl = kl - sh;
+          for (uint32_t t = 0; t < dl; t += 32) copy_small(kb + ko + sh + t, src + t, min(32u, dl - t));
+        }
+        __syncwarp();
+        // shared prefixes in entry order
+        for (uint32_t i = 0; i < cnt; i++) {
+          const uint32_t shi = __shfl_sync(0xffffffffu, sh, i);
+          const uint32_t koi = __shfl_sync(0xffffffffu, ko, i);
+          const uint32_t kpi = __shfl_sync(0xffffffffu, ko, (i + 31) & 31);
+          if (shi) {
+            const uint8_t* prev = i ? kb + kpi : W.last;
+            for (uint32_t t = lane; t < shi; t += 32) kb[koi + t] = prev[t];
+            __syncwarp();
+          }
+        }
+        // the round's last key for the next round; keys out: head bytes,
+        // 16-byte body, tail bytes
+        for (uint32_t t = lane; t < lkl; t += 32) W.last[t] = kb[lko + t];
+        last_staged = true;
+        const uint32_t head = (16 - kph) & 15;
+        const uint32_t h = head < tot ? head : tot;
+        if (lane < h) gdst[lane] = kb[lane];
+        const uint32_t body = (tot - h) & ~15u;
+        const uint4* sv = reinterpret_cast<const uint4*>(kb + h);
+        uint4* dv = reinterpret_cast<uint4*>(gdst + h);
+        for (uint32_t c = lane; c < body / 16; c += 32) dv[c] = sv[c];
+        const uint32_t t0 = h + body;
+        if (t0 + lane < tot) gdst[t0 + lane] = kb[t0 + lane];
+        if (valid) {
+          J.e_voff[e] = rec.w;
+          J.e_vlen[e] = rec.z;
+          J.e_pfx[e] = user_prefix(kb + ko, kl);
+          J.e_tag[e] = ld_le64(kb + ko + kl - 8);
+        }
       } else {
-        // longer keys (exact reruns): built in place in the arena, one key at a time
-        uint8_t* d = gdst + kofs;
-        for (uint32_t t = lane; t < ekl; t += 32) d[t] = t < esh ? gdst[pofs + t] : p[edp + t - esh];
+        // long keys: built in the arena, one key at a time, the lanes over
+        // its bytes
+        for (uint32_t i = 0; i < cnt; i++) {
+          const uint32_t shi = __shfl_sync(0xffffffffu, sh, i);
+          const uint32_t kli = __shfl_sync(0xffffffffu, kl, i);
+          const uint32_t koi = __shfl_sync(0xffffffffu, ko, i);
+          const uint32_t kpi = __shfl_sync(0xffffffffu, ko, (i + 31) & 31);
+          const uint8_t* srci = reinterpret_cast<const uint8_t*>(__shfl_sync(
+              0xffffffffu, (unsigned long long)reinterpret_cast<uintptr_t>(src), i));
+          const uint8_t* prev = i ? gdst + kpi : (last_staged ? W.last : J.keys + last_at);
+          uint8_t* d = gdst + koi;
+          for (uint32_t t = lane; t < kli; t += 32) d[t] = t < shi ? prev[t] : srci[t - shi];
+          __syncwarp();
+        }
+        last_at = kpos + lko;
+        last_staged = lkl <= kDecLastKey;
+        if (last_staged)
+          for (uint32_t t = lane; t < lkl; t += 32) W.last[t] = gdst[lko + t];
+        if (valid) {
+          J.e_voff[e] = rec.w;
+          J.e_vlen[e] = rec.z;
+          J.e_pfx[e] = user_prefix(gdst + ko, kl);
+          J.e_tag[e] = ld_le64(gdst + ko + kl - 8);
+        }
       }
       __syncwarp();
-      if (lane == 0) {
-        const uint64_t e = ebase + x;
-        J.e_koff[e] = (uint32_t)(kb0 + kofs);
-        J.e_klen[e] = ekl;
-        J.e_voff[e] = voff0 + edp + (ekl - esh);
-        J.e_vlen[e] = W.vl[i];
-      }
-      pofs = kofs;
-      kofs += ekl;
     }
-    __syncwarp();
-    if (fits) {
-      for (uint32_t t = lane; t < kofs; t += 32) gdst[t] = kbuf[t];
-    }
-    // prefixes and tags, one lane per entry
-    if (lane < n) {
-      const uint32_t i = L * kSparseEnt + lane;
-      uint32_t o = 0;
-      for (uint32_t x = 0; x < lane; x++) o += W.kl[L * kSparseEnt + x];
-      const uint8_t* k = fits ? kbuf + o : gdst + o;
-      const uint32_t kl = W.kl[i];
-      J.e_pfx[ebase + lane] = user_prefix(k, kl);
-      J.e_tag[ebase + lane] = ld_le64(k + kl - 8);
-    }
-    __syncwarp();
   }
-  // 4. the group's other blocks
-  const unsigned rest = __ballot_sync(0xffffffffu, b < nblk && !mine);
-  for (unsigned m = rest; m; m &= m - 1) decode_one(J, g0 + (__ffs(m) - 1), lane, W);
-}
-
-// Jobs whose blocks are not sparse: one warp per block.
-__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  extern __shared__ __align__(16) uint8_t dec_smem[];
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
-  if (J.ctr->error || J.sparse_blocks) return;
-  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  for (uint64_t b = (uint64_t)blockIdx.x * kDecWarps + warp; b < nblk;
-       b += (uint64_t)gridDim.x * kDecWarps)
-    decode_one(J, b, lane, W);
-}
-
-// Jobs whose blocks are sparse: one warp per group of kSparseGroup blocks
-// (a separate kernel, so that its registers do not weigh on the dense path).
-__global__ void __launch_bounds__(kDecWarps * 32) k_block_decode_sparse(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
-  extern __shared__ __align__(16) uint8_t dec_smem[];
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  DecWarpSmem& W = reinterpret_cast<DecWarpSmem*>(dec_smem)[warp];
-  if (J.ctr->error || !J.sparse_blocks) return;
-  const uint64_t nblk = min(J.ctr->n_blocks_in, J.cap_blocks_in);
-  for (uint64_t g = (uint64_t)blockIdx.x * kDecWarps + warp; g * kSparseGroup < nblk;
-       g += (uint64_t)gridDim.x * kDecWarps)
-    decode_sparse_group(J, g * kSparseGroup, nblk, lane, W);
 }
 
 __global__ void k_entries_from_offsets(const JobDev* __restrict__ jobs) {
@@ -1049,11 +788,7 @@ static unsigned dec_ctas(const Batch& bt) {
   return grid_x(bt.max_blocks_in, kDecWarps, cap);
 }
 
-void decode_kernel_attributes() {
-  dec_smem_attr((const void*)k_block_count);
-  dec_smem_attr((const void*)k_block_decode);
-  dec_smem_attr((const void*)k_block_decode_sparse);
-}
+void decode_kernel_attributes() { dec_smem_attr((const void*)k_block_count); }
 
 void launch_block_count(const Batch& bt, cudaStream_t st) {
   note_launch(), k_block_count<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
@@ -1072,10 +807,16 @@ void launch_run_bounds(const Batch& bt, cudaStream_t st) {
   note_launch(), k_run_bounds<<<dim3((bt.max_tables + 127) / 128 + 1, bt.B), 128, 0, st>>>(bt.d);
 }
 void launch_block_decode(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_block_decode<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
-                                  kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
-  note_launch(), k_block_decode_sparse<<<dim3(dec_ctas(bt), bt.B), kDecWarps * 32,
-                                         kDecWarps * sizeof(DecWarpSmem), st>>>(bt.d);
+  // pass 1: one warp per group of 8 or 32 blocks; pass 2: one warp per unit
+  // of kDecUnit entries; 8 warps per CTA, at most 8 CTAs per SM over the batch
+  const uint64_t cap = std::max<uint64_t>(1, bt.ctas_per_job ? bt.ctas_per_job : 148 * 8 / bt.B);
+  const uint64_t walk = (bt.max_blocks_in + 63) / 64, keys = (bt.max_entries + 8 * kDecUnit - 1) / (8 * kDecUnit);
+  note_launch(), k_decode_walk<<<dim3((unsigned)std::max<uint64_t>(1, std::min(walk, cap)), bt.B), 256, 0,
+                                 st>>>(bt.d);
+  scan_batch(kScanDecKlen, bt, bt.max_entries, st);
+  note_launch(), k_decode_fit<<<dim3(1, bt.B), 32, 0, st>>>(bt.d);
+  note_launch(), k_decode_keys<<<dim3((unsigned)std::max<uint64_t>(1, std::min(keys, cap)), bt.B), 256, 0,
+                                 st>>>(bt.d);
 }
 void launch_entries_from_offsets(const Batch& bt, cudaStream_t st) {
   note_launch(), k_entries_from_offsets<<<dim3(grid_x(bt.max_entries, 256, 148 * 8), bt.B), 256, 0,

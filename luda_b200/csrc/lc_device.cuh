@@ -5,8 +5,8 @@
 // bloom hash (util/hash.cc:22-51) and CRC32C (util/crc32c.cc:276; reflected
 // Castagnoli polynomial 0x82F63B78 with pre/post inversion).  The CRC is
 // computed from tables built from the polynomial (a 256-entry byte table, or
-// the 5-bit field tables of the block encoder's row CRC) and combined across
-// lanes with multiplication by x^(8n) mod P in GF(2)[x].
+// the field tables of the row CRC) and combined across lanes with
+// multiplication by x^(8n) mod P in GF(2)[x].
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -191,6 +191,29 @@ __device__ __forceinline__ uint32_t crc_raw(const uint32_t* tab, uint32_t c, con
   return c;
 }
 
+// a * b mod P with the byte table tab (tab[i] = register after byte i from
+// 0, that is i * x^32 mod P): a's four bytes by Horner, the byte groups of
+// b x^j (j < 8) by their bits, and each step of x^8 as one zero byte fed to
+// the register.
+__device__ __forceinline__ uint32_t gf2_mulmod_tab(const uint32_t* __restrict__ tab, uint32_t a,
+                                                   uint32_t b) {
+  uint32_t bx[8];
+  bx[0] = b;
+#pragma unroll
+  for (int j = 1; j < 8; j++) bx[j] = (bx[j - 1] >> 1) ^ ((bx[j - 1] & 1) ? kCrcPoly : 0u);
+  // reflected: bits 31..24 of a are x^0..x^7, bits 7..0 are x^24..x^31
+  uint32_t r = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (k) r = tab[r & 0xff] ^ (r >> 8);  // r x^8
+    const uint32_t byte = (a >> (8 * k)) & 0xff;  // degrees 8(3-k) .. 8(3-k)+7
+#pragma unroll
+    for (int d = 0; d < 8; d++)
+      if (byte & (0x80u >> d)) r ^= bx[d];  // bit 7 - d of the byte: x^d of its group
+  }
+  return r;
+}
+
 // a * b mod P in the reflected representation (bit 31 = x^0).
 __host__ __device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
   uint32_t p = 0;
@@ -340,69 +363,89 @@ __device__ __forceinline__ uint32_t crc_raw4(const uint32_t* tab4, uint32_t c, c
 // which accounts for the other lanes' bytes of the row as zeros; the block's
 // register is the xor over the lanes of their u, each moved back (x^-8n) by
 // the bytes it was carried past the block's end.  H is linear in the 128 bits
-// of x: the xor of 26 lookups, one per 5-bit field, in 32-entry tables.  A
-// warp's 32 lookups into one 32-entry table hit 32 distinct banks or share a
-// word, so each costs one shared-memory pass where a 256-entry byte table
-// costs about three.  The CRC's initial all-ones register is the same as ones
-// xored into the block's first four bytes.
-constexpr uint32_t kCrcH5Fields = 26;    // 5-bit fields of a 16-byte chunk
+// of x: the xor of one lookup per kCrcFieldBits-bit field, each in its own
+// table.  The CRC's initial all-ones register is the same as ones xored into
+// the block's first four bytes.
+constexpr uint32_t kCrcFieldBits = 5;
+constexpr uint32_t kCrcFields = (128 + kCrcFieldBits - 1) / kCrcFieldBits;
+constexpr uint32_t kCrcFieldEntries = 1u << kCrcFieldBits;
+constexpr uint32_t kCrcH5Words = kCrcFields * kCrcFieldEntries;  // the row tables
 constexpr uint32_t kCrcRowBytes = 512;   // 32 lanes x 16 bytes
-constexpr uint32_t kCrcH5Words = kCrcH5Fields * 32;
 constexpr uint32_t kCrcXinvN = 512;      // back shifts of 0..511 bytes
 
-// H(w0..w3) from the 26 tables (table i at h5[32 i], indexed by bits
-// [5i, 5i + 5) of the little-endian 128-bit chunk).
+// H(w0..w3) from the row tables (table i at h5[kCrcFieldEntries i], indexed
+// by bits [W i, W i + W) of the little-endian 128-bit chunk); the field's
+// byte offset into its table comes from one shift and one mask.
 __device__ __forceinline__ uint32_t crc_h5(const uint32_t* __restrict__ h5, uint32_t w0,
                                            uint32_t w1, uint32_t w2, uint32_t w3) {
   const uint32_t w[5] = {w0, w1, w2, w3, 0u};
+  constexpr uint32_t mask = (kCrcFieldEntries - 1) << 2;
+  const uint8_t* t = reinterpret_cast<const uint8_t*>(h5);
   uint32_t r = 0;
 #pragma unroll
-  for (uint32_t i = 0; i < kCrcH5Fields; i++) {
-    const uint32_t s = 5 * i, q = s >> 5, o = s & 31;
-    const uint32_t f = o <= 27 ? (w[q] >> o) & 31 : __funnelshift_r(w[q], w[q + 1], o) & 31;
-    r ^= h5[32 * i + f];
+  for (uint32_t i = 0; i < kCrcFields; i++) {
+    const uint32_t s = kCrcFieldBits * i, q = s >> 5, o = s & 31;
+    uint32_t f4;
+    if (o + kCrcFieldBits <= 32)
+      f4 = (o >= 2 ? (w[q] >> (o - 2)) : (w[q] << (2 - o))) & mask;
+    else
+      f4 = __funnelshift_r(w[q], w[q + 1], o - 2) & mask;
+    r ^= *reinterpret_cast<const uint32_t*>(t + 4 * kCrcFieldEntries * i + f4);
   }
   return r;
 }
 
-// The bytes of word x of the chunk at grid position p that belong to the
-// message [m0, m1), zero elsewhere, with the message's first four bytes
-// inverted (the initial register).
+// The bytes of word x at grid position pos that belong to the message
+// [m0, m1), zero elsewhere, with the grid bytes [i0, i0 + 4) inverted (the
+// message's first four when it starts the CRC: the initial register).
 __device__ __forceinline__ uint32_t crc_edge_word(uint32_t x, uint32_t pos, uint32_t m0,
-                                                  uint32_t m1) {
+                                                  uint32_t m1, uint32_t i0) {
   const auto lo_mask = [](int32_t k) -> uint32_t {  // bytes [0, k) of a word, k clamped to 0..4
     return k <= 0 ? 0u : (k >= 4 ? 0xffffffffu : (1u << (8 * k)) - 1u);
   };
   const int32_t a = (int32_t)m0 - (int32_t)pos, b = (int32_t)m1 - (int32_t)pos;
+  const int32_t c = (int32_t)i0 - (int32_t)pos;
   const uint32_t keep = lo_mask(b) & ~lo_mask(a);
-  const uint32_t inv = lo_mask(a + 4) & ~lo_mask(a);
+  const uint32_t inv = lo_mask(c + 4) & ~lo_mask(c);
   return (x & keep) ^ inv;
 }
 
 // One lane's chunk at grid position p (16-aligned) into its CRC register u,
-// for the message [m0, m1) of the grid.
+// for the message [m0, m1) of the grid (init: the message starts the CRC, so
+// its first four bytes are inverted).
 __device__ __forceinline__ uint32_t crc_chunk_step(const uint32_t* __restrict__ h5, uint32_t u,
                                                    uint32_t p, uint32_t m0, uint32_t m1,
                                                    uint32_t w0, uint32_t w1, uint32_t w2,
-                                                   uint32_t w3) {
+                                                   uint32_t w3, bool init = true) {
   if (p < m0 + 4 || p + 16 > m1) {
-    w0 = crc_edge_word(w0, p, m0, m1);
-    w1 = crc_edge_word(w1, p + 4, m0, m1);
-    w2 = crc_edge_word(w2, p + 8, m0, m1);
-    w3 = crc_edge_word(w3, p + 12, m0, m1);
+    const uint32_t i0 = init ? m0 : 0x40000000u;  // far past any chunk: nothing inverted
+    w0 = crc_edge_word(w0, p, m0, m1, i0);
+    w1 = crc_edge_word(w1, p + 4, m0, m1, i0);
+    w2 = crc_edge_word(w2, p + 8, m0, m1, i0);
+    w3 = crc_edge_word(w3, p + 12, m0, m1, i0);
   }
   return crc_h5(h5, w0 ^ u, w1, w2, w3);
 }
 
-// The masked CRC from the lanes' registers: lane l's last chunk was at grid
-// position `last` (0xffffffff when it had none) and the message ends at m1.
-__device__ __forceinline__ uint32_t crc_rows_finish(const uint32_t* __restrict__ xinv, uint32_t u,
-                                                    uint32_t last, uint32_t m1) {
+// The raw register at the message's end from the lanes' registers (lane l's
+// last chunk at grid position `last`, 0xffffffff when it had none), the same
+// in every lane.
+__device__ __forceinline__ uint32_t crc_rows_raw(const uint32_t* __restrict__ xinv,
+                                                 const uint32_t* __restrict__ tab8, uint32_t u,
+                                                 uint32_t last, uint32_t m1) {
   uint32_t v = 0;
-  if (last != 0xffffffffu) v = gf2_mulmod(xinv[last + kCrcRowBytes - m1], u);
+  if (last != 0xffffffffu) v = gf2_mulmod_tab(tab8, u, xinv[last + kCrcRowBytes - m1]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-  const uint32_t full = v ^ 0xffffffffu;
+  return v;
+}
+
+// The masked CRC from the lanes' registers: lane l's last chunk was at grid
+// position `last` (0xffffffff when it had none) and the message ends at m1.
+__device__ __forceinline__ uint32_t crc_rows_finish(const uint32_t* __restrict__ xinv,
+                                                    const uint32_t* __restrict__ tab8, uint32_t u,
+                                                    uint32_t last, uint32_t m1) {
+  const uint32_t full = crc_rows_raw(xinv, tab8, u, last, m1) ^ 0xffffffffu;
   return ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
 }
 
@@ -411,6 +454,7 @@ __device__ __forceinline__ uint32_t crc_rows_finish(const uint32_t* __restrict__
 // grid origin; bytes of the chunks outside the block are read and ignored).
 __device__ __forceinline__ uint32_t warp_block_crc_rows(const uint32_t* __restrict__ h5,
                                                         const uint32_t* __restrict__ xinv,
+                                                        const uint32_t* __restrict__ tab8,
                                                         const uint8_t* p, uint32_t n) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t m0 = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 15), m1 = m0 + n + 1;
@@ -421,7 +465,7 @@ __device__ __forceinline__ uint32_t warp_block_crc_rows(const uint32_t* __restri
     u = crc_chunk_step(h5, u, q, m0, m1, x.x, x.y, x.z, x.w);
     last = q;
   }
-  return crc_rows_finish(xinv, u, last, m1);
+  return crc_rows_finish(xinv, tab8, u, last, m1);
 }
 
 }  // namespace lc

@@ -560,6 +560,7 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
       F.meta_size = 8;
     }
     F.meta_off = meta_off;
+    F.crc_acc[0] = F.crc_acc[1] = F.crc_acc[2] = 0;
     F.index_off = meta_off + F.meta_size + kTrailer;
     F.index_size = (J.b_icum[fb1] - J.b_icum[fb0]) + 4ull * (fb1 - fb0) + 4;
     F.size = F.index_off + F.index_size + kTrailer + kFooter;
@@ -628,8 +629,8 @@ __device__ __forceinline__ void load16(const uint8_t* src, uint32_t (&w)[4]) {
 // The direct path: entries written straight to global memory, one lane per
 // entry, then the CRC read back from there.
 __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* h5,
-                                           const uint32_t* xinv, uint64_t b, uint8_t* dst,
-                                           uint32_t lane) {
+                                           const uint32_t* xinv, const uint32_t* tab8, uint64_t b,
+                                           uint8_t* dst, uint32_t lane) {
   const uint64_t s = J.b_first[b], n = J.b_first[b + 1] - s;
   const uint32_t R = J.restart_interval;
   const uint32_t bsz = J.b_size[b];
@@ -670,7 +671,7 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* h5,
     dst[bsz] = 0;
   }
   __syncwarp();
-  const uint32_t crc = warp_block_crc_rows(h5, xinv, dst, bsz);
+  const uint32_t crc = warp_block_crc_rows(h5, xinv, tab8, dst, bsz);
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
@@ -731,103 +732,166 @@ __device__ __forceinline__ void enc_chunk_out(const uint32_t* h5, uint8_t* gbase
   last = p;
 }
 
+// A block's place and entry range, and lane j's entry of its first 32: loaded
+// one block ahead (two rounds of dependent loads) so that the next block's
+// first steps do not wait on them.
+struct EncAhead {
+  uint8_t* dst;
+  uint32_t bsz, n;
+  uint64_t s;
+  uint32_t kl, sh, vl, koff, voff;  // lane's entry (j = lane < n)
+};
+
+__device__ __forceinline__ void enc_ahead_entries(const JobDev& J, EncAhead& A, uint32_t lane) {
+  if (lane < A.n) {
+    const uint64_t k = A.s + lane;
+    A.kl = J.k_klen[k];
+    A.sh = J.k_shared[k];
+    A.vl = J.k_vlen[k];
+    A.koff = J.k_koff[k];
+    A.voff = J.k_voff[k];
+  }
+}
+
 __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_h5[kCrcH5Words];
   __shared__ uint32_t s_xinv[kCrcXinvN];
+  __shared__ uint32_t s_tab8[256];
   extern __shared__ __align__(16) uint8_t enc_smem[];
   for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = J.crc_h5[i];
   for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = J.crc_xinv[i];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = J.crc_byte[i];
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem)[warp];
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t R = J.restart_interval;
+  const uint64_t stride = (uint64_t)gridDim.x * kEncWarps;
   uint8_t* st = W.stage;
-  for (uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp; b < nb;
-       b += (uint64_t)gridDim.x * kEncWarps) {
-    const FileOut& F = J.files[J.b_file[b]];
-    uint8_t* dst = J.out + F.out_off + J.b_off[b];
-    const uint32_t bsz = J.b_size[b];
-    const uint64_t s = J.b_first[b];
-    const uint32_t n = (uint32_t)(J.b_first[b + 1] - s);
+  uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp;
+  EncAhead cur{};
+  if (b < nb) {
+    cur.dst = J.out + J.files[J.b_file[b]].out_off + J.b_off[b];
+    cur.bsz = J.b_size[b];
+    cur.s = J.b_first[b];
+    cur.n = (uint32_t)(J.b_first[b + 1] - cur.s);
+    enc_ahead_entries(J, cur, lane);
+  }
+  for (; b < nb; b += stride) {
+    // the next block's place and range (its entries follow after step 2)
+    const uint64_t bn = b + stride;
+    EncAhead nxt{};
+    uint32_t n_file = 0;
+    uint64_t n_off = 0;
+    if (bn < nb) {
+      n_file = J.b_file[bn];
+      n_off = J.b_off[bn];
+      nxt.bsz = J.b_size[bn];
+      nxt.s = J.b_first[bn];
+      nxt.n = (uint32_t)(J.b_first[bn + 1] - nxt.s);
+    }
+    uint8_t* dst = cur.dst;
+    const uint32_t bsz = cur.bsz, n = cur.n;
+    const uint64_t s = cur.s;
     const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
     if (ph + bsz + kTrailer + 16 > kEncStage) {
-      enc_direct(J, s_h5, s_xinv, b, dst, lane);
-      continue;
-    }
-    const uint32_t nrest = (n + R - 1) / R;
-    const uint32_t rbase = ph + bsz - 4 * nrest - 4;  // stage position of the restart array
-    // 1. entries: headers, restart words, short stretches, cut edges, list
-    uint32_t carry = 0, lcarry = 0;
-    for (uint32_t j0 = 0; j0 < n; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      uint32_t size = 0, hl = 0, kd = 0, vl = 0, sh = 0, koff = 0, voff = 0;
-      if (j < n) {
-        const uint64_t k = s + j;
-        const uint32_t kl = J.k_klen[k];
-        sh = (j % R == 0) ? 0 : J.k_shared[k];
-        kd = kl - sh;
-        vl = J.k_vlen[k];
-        koff = J.k_koff[k] + sh;
-        voff = J.k_voff[k];
-        hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
-        size = hl + kd + vl;
-      }
-      uint32_t tot, ltot;
-      const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
-      const uint32_t nl = j < n ? (uint32_t)(kd >= kEncLong) + (uint32_t)(vl >= kEncLong) : 0u;
-      uint32_t li = warp_excl<uint32_t>(nl, &ltot) + lcarry;
-      carry += tot;
-      lcarry += ltot;
-      if (j < n) {
-        uint8_t* p = st + ph + ex;
-        p = put_varint(p, sh);
-        p = put_varint(p, kd);
-        put_varint(p, vl);
-        if (j % R == 0) {
-          const uint32_t rem = n - j;
-          st_le32(st + rbase + 4 * (j / R), (ex << 8) | (rem < R ? rem : R));
+      enc_direct(J, s_h5, s_xinv, s_tab8, b, dst, lane);
+    } else {
+      const uint32_t nrest = (n + R - 1) / R;
+      const uint32_t rbase = ph + bsz - 4 * nrest - 4;  // stage position of the restart array
+      // 1. entries: headers, restart words, short stretches, cut edges, list
+      uint32_t carry = 0, lcarry = 0;
+      for (uint32_t j0 = 0; j0 < n; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t size = 0, hl = 0, kd = 0, vl = 0, sh = 0, koff = 0, voff = 0;
+        if (j < n) {
+          uint32_t kl;
+          if (j0 == 0) {
+            kl = cur.kl, sh = cur.sh, vl = cur.vl, koff = cur.koff, voff = cur.voff;
+          } else {
+            const uint64_t k = s + j;
+            kl = J.k_klen[k], sh = J.k_shared[k], vl = J.k_vlen[k];
+            koff = J.k_koff[k], voff = J.k_voff[k];
+          }
+          if (j % R == 0) sh = 0;
+          kd = kl - sh;
+          koff += sh;
+          hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
+          size = hl + kd + vl;
         }
-        if (J.dec_vpos)  // the value's place in its file, for the decoded form
-          J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + kd);
-        const uint32_t kpos = ph + ex + hl;
-        enc_stretch(W, st, kpos, kd, J.keys, koff, 0u, li);
-        enc_stretch(W, st, kpos + kd, vl, J.in, voff, kEncFromInput, li);
+        uint32_t tot, ltot;
+        const uint32_t ex = warp_excl<uint32_t>(size, &tot) + carry;
+        const uint32_t nl = j < n ? (uint32_t)(kd >= kEncLong) + (uint32_t)(vl >= kEncLong) : 0u;
+        uint32_t li = warp_excl<uint32_t>(nl, &ltot) + lcarry;
+        carry += tot;
+        lcarry += ltot;
+        if (j < n) {
+          uint8_t* p = st + ph + ex;
+          p = put_varint(p, sh);
+          p = put_varint(p, kd);
+          put_varint(p, vl);
+          if (j % R == 0) {
+            const uint32_t rem = n - j;
+            st_le32(st + rbase + 4 * (j / R), (ex << 8) | (rem < R ? rem : R));
+          }
+          if (J.dec_vpos)  // the value's place in its file, for the decoded form
+            J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + kd);
+          const uint32_t kpos = ph + ex + hl;
+          enc_stretch(W, st, kpos, kd, J.keys, koff, 0u, li);
+          enc_stretch(W, st, kpos + kd, vl, J.in, voff, kEncFromInput, li);
+        }
       }
+      if (lane == 0) {
+        st_le32(st + ph + bsz - 4, nrest);
+        st[ph + bsz] = 0;  // kNoCompression
+      }
+      __syncwarp();
+      // 2. chunks: out to global memory and into the CRC; each chunk's loads
+      // are issued two chunks ahead of its use (three rotating slots)
+      const uint32_t nls = min(lcarry, kEncMaxLong);
+      const uint32_t m0 = ph, m1 = ph + bsz + 1;
+      uint8_t* gbase = dst - ph;
+      uint32_t u = 0, last = 0xffffffffu, k = 0;
+      uint32_t sa[4], sb[4], sc[4];
+      bool vb = 16 * (lane + 32) < m1;
+      if (16 * lane < m1) enc_fetch(J, W, st, nls, lane, k, sa);
+      if (vb) enc_fetch(J, W, st, nls, lane + 32, k, sb);
+      if (bn < nb) {  // the next block's place and entries, in flight meanwhile
+        nxt.dst = J.out + J.files[n_file].out_off + n_off;
+        enc_ahead_entries(J, nxt, lane);
+      }
+      for (uint32_t c = lane; 16 * c < m1; c += 96) {
+        const bool vc = 16 * (c + 64) < m1;
+        if (vc) enc_fetch(J, W, st, nls, c + 64, k, sc);
+        enc_chunk_out(s_h5, gbase, 16 * c, m0, m1, sa, u, last);
+        if (16 * (c + 96) < m1) enc_fetch(J, W, st, nls, c + 96, k, sa);
+        if (vb) enc_chunk_out(s_h5, gbase, 16 * (c + 32), m0, m1, sb, u, last);
+        const bool ve = 16 * (c + 128) < m1;
+        if (ve) enc_fetch(J, W, st, nls, c + 128, k, sb);
+        if (vc) enc_chunk_out(s_h5, gbase, 16 * (c + 64), m0, m1, sc, u, last);
+        vb = ve;
+      }
+      // 3. CRC, trailer, partial chunks at both ends
+      const uint32_t crc = crc_rows_finish(s_xinv, s_tab8, u, last, m1);
+      if (lane == 0) st_le32(st + m1, crc);
+      __syncwarp();
+      const uint32_t cf0 = (m0 + 15) >> 4, cf1 = m1 >> 4;  // whole chunks [cf0, cf1) went out
+      uint32_t h1 = 16 * cf0, t0 = 16 * cf1;
+      if (cf1 < cf0) h1 = t0 = m0;  // the message lies inside one chunk
+      const uint32_t nh = h1 - m0, nt = m1 + 4 - t0;
+      for (uint32_t x = lane; x < nh + nt; x += 32) {
+        const uint32_t q = x < nh ? m0 + x : t0 + (x - nh);
+        gbase[q] = st[q];
+      }
+      __syncwarp();
     }
-    if (lane == 0) {
-      st_le32(st + ph + bsz - 4, nrest);
-      st[ph + bsz] = 0;  // kNoCompression
+    if (bn < nb && nxt.dst == nullptr) {  // the direct path
+      nxt.dst = J.out + J.files[n_file].out_off + n_off;
+      enc_ahead_entries(J, nxt, lane);
     }
-    __syncwarp();
-    // 2. chunks: out to global memory and into the CRC, two per lane at a time
-    const uint32_t nls = min(lcarry, kEncMaxLong);
-    const uint32_t m0 = ph, m1 = ph + bsz + 1;
-    uint8_t* gbase = dst - ph;
-    uint32_t u = 0, last = 0xffffffffu, k = 0;
-    for (uint32_t c = lane; 16 * c < m1; c += 64) {
-      uint32_t a[4], a2[4];
-      const bool two = 16 * (c + 32) < m1;
-      enc_fetch(J, W, st, nls, c, k, a);
-      if (two) enc_fetch(J, W, st, nls, c + 32, k, a2);
-      enc_chunk_out(s_h5, gbase, 16 * c, m0, m1, a, u, last);
-      if (two) enc_chunk_out(s_h5, gbase, 16 * (c + 32), m0, m1, a2, u, last);
-    }
-    // 3. CRC, trailer, partial chunks at both ends
-    const uint32_t crc = crc_rows_finish(s_xinv, u, last, m1);
-    if (lane == 0) st_le32(st + m1, crc);
-    __syncwarp();
-    const uint32_t cf0 = (m0 + 15) >> 4, cf1 = m1 >> 4;  // whole chunks [cf0, cf1) went out
-    uint32_t h1 = 16 * cf0, t0 = 16 * cf1;
-    if (cf1 < cf0) h1 = t0 = m0;  // the message lies inside one chunk
-    const uint32_t nh = h1 - m0, nt = m1 + 4 - t0;
-    for (uint32_t x = lane; x < nh + nt; x += 32) {
-      const uint32_t q = x < nh ? m0 + x : t0 + (x - nh);
-      gbase[q] = st[q];
-    }
-    __syncwarp();
+    cur = nxt;
   }
 }
 
@@ -875,7 +939,7 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
   if (gb != 0) {
     uint8_t* fdst = fbase + (J.b_gcum[b] - J.b_gcum[fb0]);
     const uint32_t nbytes = gb - 1;
-    const uint64_t bits = (uint64_t)nbytes * 8;
+    const uint32_t bits = nbytes * 8;  // a group's filter is far below 2^29 bytes
     const bool in_smem = nbytes <= kFilterSmem;
     if (in_smem) {
       for (uint32_t i = lane; i < (nbytes + 3) / 4; i += 32) sbuf[i] = 0;
@@ -1022,13 +1086,10 @@ __global__ void k_encode_index(const JobDev* __restrict__ jobs) {
 // Metaindex, footer and the tail of the filter block's offset array (thread
 // 0), then the trailers of the filter, metaindex and index blocks, each a
 // CRC32C over the whole CTA: one CTA per output file.
-__global__ void __launch_bounds__(1024) k_encode_meta(const JobDev* __restrict__ jobs) {
+__global__ void __launch_bounds__(256) k_encode_meta(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
-  __shared__ uint32_t tab4[4 * 256];
-  __shared__ uint32_t s_x[32];
   __shared__ uint32_t s_skip;
   if (threadIdx.x == 0) s_skip = J.ctr->error || blockIdx.x >= J.ctr->n_files;
-  crc_tables4_init(tab4);
   __syncthreads();
   if (s_skip) return;
   const uint32_t f = blockIdx.x;
@@ -1080,36 +1141,90 @@ __global__ void __launch_bounds__(1024) k_encode_meta(const JobDev* __restrict__
     for (uint32_t t = threadIdx.x; t < l; t += blockDim.x) d[t] = k[t];
     if (threadIdx.x == 0) J.fkoff[2 * f + which] = l;
   }
-  for (uint32_t which = 0; which < 3; which++) {
-    if (which == 0 && J.bits_per_key <= 0) continue;
-    const uint64_t off = which == 0 ? F.filter_off : (which == 1 ? F.meta_off : F.index_off);
-    const uint64_t len = which == 0 ? F.filter_size : (which == 1 ? F.meta_size : F.index_size);
-    uint8_t* p = J.out + F.out_off + off;
-    const uint64_t total = len + 1;
-    // contiguous stretches of whole words per thread (the last thread also
-    // takes the type byte, which is 0 for these blocks)
-    const uint64_t seg = ((total + blockDim.x - 1) / blockDim.x + 3) & ~uint64_t(3);
-    const uint64_t b = (uint64_t)threadIdx.x * seg;
-    const uint64_t e = min(total, b + seg);
-    uint32_t c = 0;
-    if (b < e) {
-      const uint64_t e_data = min(e, len);
-      if (e_data > b) c = crc_raw4(tab4, 0, p + b, (uint32_t)(e_data - b));
-      if (e > len) c = tab4[c & 0xff] ^ (c >> 8);  // the type byte
+}
+
+// The filter, metaindex and index blocks' trailers: each region is cut into
+// kMetaPiece-byte pieces, one warp per piece (the row CRC, lanes over the
+// piece's 16-byte chunks); a piece's raw register, moved to the region's end
+// past its type byte, is xored into the file's accumulator (the xor of every
+// byte's share is the register of the whole), and k_meta_trailers writes the
+// finished CRCs.  kMetaCtas CTAs per file.
+constexpr uint32_t kMetaPiece = 4096;
+constexpr uint32_t kMetaCtas = 8;
+
+__device__ __forceinline__ void meta_region(const FileOut& F, uint32_t r, uint64_t* off,
+                                            uint64_t* len) {
+  if (r == 0) {
+    *off = F.filter_off;
+    *len = F.filter_size;
+  } else if (r == 1) {
+    *off = F.meta_off;
+    *len = F.meta_size;
+  } else {
+    *off = F.index_off;
+    *len = F.index_size;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_meta_crc(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.z];
+  __shared__ uint32_t s_h5[kCrcH5Words];
+  __shared__ uint32_t s_xinv[kCrcXinvN];
+  __shared__ uint32_t s_tab8[256];
+  __shared__ uint32_t s_skip;
+  if (threadIdx.x == 0) s_skip = J.ctr->error || blockIdx.y >= J.ctr->n_files;
+  for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = J.crc_h5[i];
+  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = J.crc_xinv[i];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = J.crc_byte[i];
+  __syncthreads();
+  if (s_skip) return;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t nf = J.ctr->n_files;
+  for (uint32_t f = blockIdx.y; f < nf; f += gridDim.y) {
+    const FileOut& F = J.files[f];
+    uint64_t off[3], len[3], np[3];
+    for (uint32_t r = 0; r < 3; r++) {
+      meta_region(F, r, &off[r], &len[r]);
+      np[r] = (r == 0 && J.bits_per_key <= 0) ? 0 : (len[r] + kMetaPiece - 1) / kMetaPiece;
     }
-    uint32_t v = b < total ? crc_shift(J, c, total - e) : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) s_x[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t x = 0;
-      for (uint32_t w = 0; w < blockDim.x / 32; w++) x ^= s_x[w];
-      const uint32_t full = x ^ crc_shift(J, 0xffffffffu, total) ^ 0xffffffffu;
-      p[len] = 0;
-      st_le32(p + len + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);
+    const uint8_t* fbase = J.out + F.out_off;
+    const uint64_t total = np[0] + np[1] + np[2];
+    for (uint64_t p = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp; p < total;
+         p += (uint64_t)gridDim.x * (blockDim.x / 32)) {
+      uint32_t r = 0;
+      uint64_t q = p;
+      while (q >= np[r]) q -= np[r++];
+      const uint64_t a = q * kMetaPiece, e = min(len[r], a + kMetaPiece);
+      const uint8_t* pa = fbase + off[r] + a;
+      const uint32_t m0 = (uint32_t)(reinterpret_cast<uintptr_t>(pa) & 15);
+      const uint32_t m1 = m0 + (uint32_t)(e - a);
+      const uint8_t* g = pa - m0;
+      uint32_t u = 0, last = 0xffffffffu;
+      for (uint32_t x = 16 * lane; x < m1; x += kCrcRowBytes) {
+        const uint4 v = *reinterpret_cast<const uint4*>(g + x);
+        u = crc_chunk_step(s_h5, u, x, m0, m1, v.x, v.y, v.z, v.w, a == 0);
+        last = x;
+      }
+      const uint32_t raw = crc_rows_raw(s_xinv, s_tab8, u, last, m1);
+      if (lane == 0) atomicXor(&J.files[f].crc_acc[r], crc_shift(J, raw, len[r] + 1 - e));
     }
-    __syncthreads();
+  }
+}
+
+__global__ void k_meta_trailers(const JobDev* __restrict__ jobs) {
+  const JobDev& J = jobs[blockIdx.y];
+  if (J.ctr->error) return;
+  const uint32_t nf = J.ctr->n_files;
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < 3 * nf; x += gridDim.x * blockDim.x) {
+    const uint32_t f = x / 3, r = x % 3;
+    if (r == 0 && J.bits_per_key <= 0) continue;
+    const FileOut& F = J.files[f];
+    uint64_t off, len;
+    meta_region(F, r, &off, &len);
+    uint8_t* p = J.out + F.out_off + off + len;
+    const uint32_t full = F.crc_acc[r] ^ 0xffffffffu;
+    p[0] = 0;  // kNoCompression
+    st_le32(p + 1, ((full >> 15) | (full << 17)) + 0xa282ead8u);  // crc32c::Mask
   }
 }
 
@@ -1180,7 +1295,10 @@ void launch_encode_index(const Batch& bt, cudaStream_t st) {
                                   0, st>>>(bt.d);
 }
 void launch_encode_meta(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 1024, 0, st>>>(bt.d);
+  note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 256, 0, st>>>(bt.d);
+  note_launch(), k_meta_crc<<<dim3(kMetaCtas, std::min<uint32_t>(bt.max_cap_files, 65535), bt.B),
+                              256, 0, st>>>(bt.d);
+  note_launch(), k_meta_trailers<<<dim3((3 * bt.max_cap_files + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
 }
 
 }  // namespace lc

@@ -506,6 +506,7 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.crc_xpow_n = kCrcXpowN;
   J.crc_h5 = e->crc_xpow + kCrcXpowN;
   J.crc_xinv = J.crc_h5 + kCrcH5Words;
+  J.crc_byte = J.crc_xinv + kCrcXinvN;
   J.chunk = kChunk;
   J.chain_smem_words = 11 * 1024;  // 44 KiB (static shared memory takes the rest of 48)
 }
@@ -610,7 +611,8 @@ void alloc_tail(JobRun& r, DevAlloc& A, bool with_merge) {
     J.keys = A.get<uint8_t>(r.K + 16);
     J.cap_key_bytes = r.K;
     J.cap_entries = N;
-    J.e_koff = A.get<uint32_t>(N);
+    J.e_rec = A.get<uint4>(N);
+    J.e_koff = A.get<uint32_t>(N + 1);  // + the total (the scan of the key lengths)
     J.e_klen = A.get<uint32_t>(N);
     J.e_voff = A.get<uint32_t>(N);
     J.e_vlen = A.get<uint32_t>(N);
@@ -1165,10 +1167,9 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       }
       r.J.reserve_keys = exact ? 0 : 1;
       r.J.max_key_len = kFastMaxKey;
-      // blocks of a few entries each (long values): decoded in groups without
-      // staging the values
-      r.J.sparse_blocks = !r.failed && hc[i].n_blocks_in > 0 &&
-                          hc[i].n_entries_in <= 6 * hc[i].n_blocks_in;
+      // blocks of many entries are walked 8 to a warp (four restart runs of
+      // 16 entries each fill its lanes), blocks of few 32
+      r.J.dec_group = (!r.failed && hc[i].n_entries_in > 16 * hc[i].n_blocks_in) ? 8 : 32;
       r.j->entries_in = r.N;
       r.j->key_bytes_in = exact ? r.K : 0;
     }
@@ -1536,7 +1537,7 @@ void run_build(lc_job* j, lc_slot& slot) {
 // (the at-size workloads have 67-250 bytes per entry) and the worker trues
 // the charge up to the batch's real allocation once the counts are known.
 constexpr uint64_t kEstEntryBytes = 40;
-constexpr uint64_t kEntryArrayBytes = 232;  // per-entry arrays of alloc_tail, rounded up
+constexpr uint64_t kEntryArrayBytes = 248;  // per-entry arrays of alloc_tail, rounded up
 uint64_t estimate_bytes(const lc_job* j) {
   uint64_t in = 0;
   for (auto& t : j->tables) in += round16(t.size);
@@ -1719,12 +1720,14 @@ void fill_out(lc_job* j, lc_job_out* o) {
   o->decoded_inputs = j->decoded_inputs;
 }
 
-// The engine's CRC tables, one device array: [x^(8n) | row fields | x^(-8n)].
+// The engine's CRC tables, one device array: [x^(8n) | row fields | x^(-8n) |
+// byte table].
 //  * x^(8n) mod P for n < kCrcXpowN (register shifts by n zero bytes);
-//  * for the row CRC of the block encoder: entry 32 i + v is the register
-//    after 16 bytes holding v at bits [5i, 5i + 5) and zero elsewhere, then
-//    kCrcRowBytes - 16 zero bytes, from register 0;
-//  * x^(-8n) mod P for n < kCrcXinvN: the shift that undoes n zero bytes.
+//  * for the row CRC: entry kCrcFieldEntries i + v is the register after 16
+//    bytes holding v at bits [W i, W i + W) (W = kCrcFieldBits) and zero
+//    elsewhere, then kCrcRowBytes - 16 zero bytes, from register 0;
+//  * x^(-8n) mod P for n < kCrcXinvN: the shift that undoes n zero bytes;
+//  * the byte table: the register after byte i, from 0.
 // Registers are reflected (bit 31 is x^0), as in util/crc32c.cc.
 uint32_t host_crc_byte(uint32_t c, uint8_t b) {
   c ^= b;
@@ -1733,24 +1736,24 @@ uint32_t host_crc_byte(uint32_t c, uint8_t b) {
 }
 
 void host_crc_tables(std::vector<uint32_t>& t) {
-  t.assign(kCrcXpowN + kCrcH5Words + kCrcXinvN, 0);
+  t.assign(kCrcXpowN + kCrcH5Words + kCrcXinvN + 256, 0);
   uint32_t c = 0x80000000u;  // x^0
   for (uint32_t m = 0; m < kCrcXpowN; m++) {
     t[m] = c;
     c = host_crc_byte(c, 0);
   }
   uint32_t* h5 = t.data() + kCrcXpowN;
-  for (uint32_t i = 0; i < kCrcH5Fields; i++)
-    for (uint32_t v = 0; v < 32; v++) {
+  for (uint32_t i = 0; i < kCrcFields; i++)
+    for (uint32_t v = 0; v < kCrcFieldEntries; v++) {
       uint8_t x[16] = {};
-      for (uint32_t bit = 0; bit < 5; bit++) {
-        const uint32_t at = 5 * i + bit;
+      for (uint32_t bit = 0; bit < kCrcFieldBits; bit++) {
+        const uint32_t at = kCrcFieldBits * i + bit;
         if (((v >> bit) & 1) && at < 128) x[at >> 3] |= (uint8_t)(1u << (at & 7));
       }
       uint32_t r = 0;
       for (uint32_t k = 0; k < 16; k++) r = host_crc_byte(r, x[k]);
       for (uint32_t k = 16; k < kCrcRowBytes; k++) r = host_crc_byte(r, 0);
-      h5[32 * i + v] = r;
+      h5[kCrcFieldEntries * i + v] = r;
     }
   // one zero byte maps c to byte(c & 0xff) ^ (c >> 8), where byte(i) =
   // host_crc_byte(0, i): its top byte names i (the table's top bytes are a
@@ -1764,6 +1767,8 @@ void host_crc_tables(std::vector<uint32_t>& t) {
     const uint32_t i = by_top[c >> 24];
     c = ((c ^ host_crc_byte(0, (uint8_t)i)) << 8) | i;
   }
+  uint32_t* byte = xinv + kCrcXinvN;
+  for (uint32_t i = 0; i < 256; i++) byte[i] = host_crc_byte(0, (uint8_t)i);
 }
 
 }  // namespace

@@ -52,9 +52,10 @@ struct Counters {
   uint32_t pad;
   uint64_t kept_key_bytes;    // internal-key bytes of the survivors
   uint64_t kept_value_bytes;  // value bytes of the survivors
-  uint64_t key_cursor;        // key bytes reserved by the single-pass decode
+  uint64_t key_cursor;        // key bytes of the decoded entries (the scan of their lengths)
   uint32_t key_skip;          // user-key bytes every input key shares (prefixes start after them)
   uint32_t pad2;
+  uint64_t key_total;         // decoded key bytes, summed by the decode's first pass
 };
 
 struct TableDesc {
@@ -92,7 +93,8 @@ struct FileOut {       // per output file
   uint64_t first_kept, end_kept;      // kept entries [first, end)
   uint32_t first_block, end_block;    // output blocks [first, end)
   uint32_t n_filters;                 // filter offsets in the filter block
-  uint32_t pad;
+  uint32_t crc_acc[3];                // raw CRC32C registers of the filter, metaindex and
+                                      // index blocks, xored together from pieces
 };
 
 struct JobDev {
@@ -153,6 +155,8 @@ struct JobDev {
   // entries (input order)
   uint8_t* keys;             // key arena
   uint64_t cap_key_bytes;
+  uint4* e_rec;              // per entry: decode record (pass 1 -> pass 2)
+  uint32_t dec_group;        // data blocks per warp in the decode's first pass
   uint32_t* e_koff;
   uint32_t* e_klen;
   uint32_t* e_voff;
@@ -207,7 +211,6 @@ struct JobDev {
   uint32_t reserve_keys;     // 1: decode reserves key-arena space per block (single
                              // pass, restart counts only); 0: blk_key_base from counting
   uint32_t max_key_len;      // 1: longest key the single-pass layout allows
-  uint32_t sparse_blocks;    // the blocks average few entries: decode them in groups
 
   // output blocks
   uint32_t* b_first;         // first kept entry of block (cap_blocks_out + 1)
@@ -251,8 +254,9 @@ struct JobDev {
   // CRC32C shift table: x^(8m) mod P for m in [0, crc_tab_n)
   const uint32_t* crc_xpow;
   uint32_t crc_xpow_n;
-  const uint32_t* crc_h5;     // kCrcH5Words: the 5-bit field tables of the row CRC
+  const uint32_t* crc_h5;     // kCrcH5Words: the field tables of the row CRC
   const uint32_t* crc_xinv;   // kCrcXinvN: x^(-8n) mod P, back shifts by n bytes
+  const uint32_t* crc_byte;   // 256: the byte table (register after byte i, from 0)
 };
 
 }  // namespace lc

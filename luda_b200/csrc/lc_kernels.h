@@ -70,6 +70,7 @@ enum ScanSel : int {
   kScanIcum,           // b_isize -> b_icum
   kScanDecKey,         // k_klen -> dec_kcum (jobs that keep their decoded form)
   kScanKb,             // k_b -> k_pb (block size estimates)
+  kScanDecKlen,        // e_klen -> e_koff (decode: key places)  (total: key_cursor)
 };
 void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st);
 uint64_t scan_scratch_elems(uint64_t n_cap);

@@ -123,6 +123,16 @@ struct ScanOf<kScanKb> {
   static __device__ uint64_t* total(const JobDev&) { return nullptr; }
 };
 
+template <>
+struct ScanOf<kScanDecKlen> {
+  using TI = uint32_t;
+  using TO = uint32_t;
+  static __device__ const TI* in(const JobDev& J) { return J.e_klen; }
+  static __device__ TO* out(const JobDev& J) { return J.e_koff; }
+  static __device__ uint64_t n(const JobDev& J) { return J.ctr->n_entries_in; }
+  static __device__ uint64_t* total(const JobDev& J) { return &J.ctr->key_cursor; }
+};
+
 // Tile-sum scratch of a scan (the scans of a job run one after another).
 template <int S>
 __device__ __forceinline__ uint64_t* scan_tiles_of(const JobDev& J) {
@@ -271,6 +281,7 @@ void scan_batch(ScanSel sel, const Batch& bt, uint64_t n_cap, cudaStream_t st) {
     case kScanIcum: scan_sel<kScanIcum>(bt, n_cap, st); break;
     case kScanDecKey: scan_sel<kScanDecKey>(bt, n_cap, st); break;
     case kScanKb: scan_sel<kScanKb>(bt, n_cap, st); break;
+    case kScanDecKlen: scan_sel<kScanDecKlen>(bt, n_cap, st); break;
   }
 }
 
