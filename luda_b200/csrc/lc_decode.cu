@@ -567,8 +567,13 @@ __global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ 
       const uint8_t* qp = p + s;
       const uint8_t* lim = p + e;  // run ranges checked by k_block_restarts
       const uint32_t boff = (uint32_t)J.blk_off[b];
+      // the run's first lines into L1 ahead of the walk, and one line further
+      // at every entry (a run of short entries is read as a stream)
+      for (uint32_t x = 0; x < 3; x++)
+        if (qp + 128 * x < lim) prefetch_l1(qp + 128 * x);
       uint32_t prev = 0;
       for (uint32_t k = 0; k < cnt; k++) {
+        if (qp + 384 < lim) prefetch_l1(qp + 384);
         uint32_t sh, ns, vl;
         const uint8_t* d = entry_header(qp, lim, &sh, &ns, &vl);
         if (!d || (k == 0 && sh != 0) || sh > prev) {
@@ -680,20 +685,35 @@ __global__ void __launch_bounds__(256) k_decode_keys(const JobDev* __restrict__ 
         // deltas, every lane at once
         if (valid) {
           const uint32_t dl = kl - sh;
-          for (uint32_t t = 0; t < dl; t += 32) copy_small(kb + ko + sh + t, src + t, min(32u, dl - t));
+          for (uint32_t t = 0; t < dl; t += 32) copy_small_w(kb + ko + sh + t, src + t, min(32u, dl - t));
         }
         __syncwarp();
-        // shared prefixes in entry order
-        for (uint32_t i = 0; i < cnt; i++) {
-          const uint32_t shi = __shfl_sync(0xffffffffu, sh, i);
-          const uint32_t koi = __shfl_sync(0xffffffffu, ko, i);
-          const uint32_t kpi = __shfl_sync(0xffffffffu, ko, (i + 31) & 31);
-          if (shi) {
-            const uint8_t* prev = i ? kb + kpi : W.last;
-            for (uint32_t t = lane; t < shi; t += 32) kb[koi + t] = prev[t];
-            __syncwarp();
+        // shared prefixes: a key's bytes below the least shared length of
+        // the round's entries up to it are the previous round's last key's;
+        // each other prefix byte is the own (delta) byte of the nearest
+        // earlier entry whose shared length lies below it -- the entries in
+        // between share it -- found by walking back (every walk ends at the
+        // entry with that least shared length)
+        uint32_t m = valid ? sh : 0;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, m, o);
+          if (lane >= o) m = min(m, y);
+        }
+        if (valid)
+          for (uint32_t t = 0; t < m; t++) kb[ko + t] = W.last[t];
+        uint32_t lim = valid ? sh : 0;
+        for (uint32_t d = 1; d < 32 && __any_sync(0xffffffffu, lim > m); d++) {
+          const uint32_t j = lane >= d ? lane - d : lane;
+          const uint32_t shj = __shfl_sync(0xffffffffu, sh, j);
+          const uint32_t koj = __shfl_sync(0xffffffffu, ko, j);
+          if (lim > m && lane >= d && shj < lim) {
+            const uint32_t a = max(shj, m);
+            for (uint32_t t = a; t < lim; t++) kb[ko + t] = kb[koj + t];
+            lim = a;
           }
         }
+        __syncwarp();
         // the round's last key for the next round; keys out: head bytes,
         // 16-byte body, tail bytes
         for (uint32_t t = lane; t < lkl; t += 32) W.last[t] = kb[lko + t];

@@ -294,6 +294,42 @@ __device__ __forceinline__ void copy_small(uint8_t* dst, const uint8_t* src, uin
     if (i < len) dst[i] = (uint8_t)(r[i >> 2] >> (8 * (i & 3)));
 }
 
+// Up to 32 bytes from src (global memory, any alignment) to dst (shared
+// memory, any alignment): the destination's whole words with word stores,
+// its partial words at both ends byte by byte (their other bytes belong to
+// other writers).  Only source words that hold a needed byte are loaded.
+__device__ __forceinline__ void copy_small_w(uint8_t* dst, const uint8_t* src, uint32_t len) {
+  if (!len) return;
+  const uintptr_t d = reinterpret_cast<uintptr_t>(dst), s = reinterpret_cast<uintptr_t>(src);
+  const uint32_t da = (uint32_t)(d & 3);
+  // destination word q covers source bytes from s - da + 4q
+  const uintptr_t s0 = s - da;
+  const uint32_t* base = reinterpret_cast<const uint32_t*>(s0 & ~uintptr_t(3));
+  const uint32_t sh = 8 * (uint32_t)(s0 & 3);
+  const uintptr_t b0 = reinterpret_cast<uintptr_t>(base);
+  uint32_t w[11];
+#pragma unroll
+  for (uint32_t i = 0; i < 11; i++) {
+    const uintptr_t wa = b0 + 4 * i;  // word [wa, wa + 4) holds a needed byte?
+    w[i] = (wa + 4 > s && wa < s + len) ? __ldg(base + i) : 0u;
+  }
+  uint32_t* dw = reinterpret_cast<uint32_t*>(d - da);
+  const uint32_t end = da + len;  // destination bytes [da, end) of the words from dw
+#pragma unroll
+  for (uint32_t q = 0; q < 9; q++) {
+    if (4 * q >= end) break;
+    const uint32_t v = __funnelshift_r(w[q], w[q + 1], sh);
+    if (4 * q >= da && 4 * q + 4 <= end) {
+      dw[q] = v;
+    } else {
+      uint8_t* db = reinterpret_cast<uint8_t*>(dw + q);
+#pragma unroll
+      for (uint32_t i = 0; i < 4; i++)
+        if (4 * q + i >= da && 4 * q + i < end) db[i] = (uint8_t)(v >> (8 * i));
+    }
+  }
+}
+
 // Error reporting: the first error code wins.
 __device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t detail) {
   if (atomicCAS(&c->error, 0u, code) == 0u) c->error_detail = detail;
@@ -310,6 +346,9 @@ namespace lc {
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p));
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");

@@ -215,6 +215,18 @@ struct lc_engine {
   bool use_graphs = true;
   std::mutex tun_mu;
   Tunables tun;
+  // Host<->device copies of jobs from host buffers run one job at a time per
+  // direction, in the order they are issued: each batch's uploads wait on an
+  // event after the previous batch's uploads (downloads likewise), so that one
+  // job's download overlaps the next one's upload at each direction's full
+  // rate instead of several jobs sharing a direction and then idling it
+  // together.
+  struct CopyLane {
+    std::mutex mu;
+    cudaEvent_t done = nullptr;
+    bool any = false;
+  };
+  CopyLane up_lane, down_lane;
   // one slot per worker thread, then slots for synchronous calls (grown on
   // demand, one per concurrent caller)
   std::vector<std::unique_ptr<lc_slot>> slots;
@@ -1060,6 +1072,14 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     bt.ctas_per_job = tun.ctas_per_job;
     bt.merge_items = tun.merge_items;
     bt.merge_threads = tun.merge_threads;
+    bool host_up = false;
+    for (uint32_t i = 0; i < B; i++)
+      host_up = host_up || (!zero_copy[i] && !jobs[i]->inputs_on_device && !runs[i].failed);
+    std::unique_lock<std::mutex> up_lk(e->up_lane.mu, std::defer_lock);
+    if (host_up) {
+      up_lk.lock();
+      if (e->up_lane.any) CK(cudaStreamWaitEvent(st, e->up_lane.done, 0));
+    }
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       JobDev& J = r.J;
@@ -1108,6 +1128,11 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       bt.any_verify = bt.any_verify || (J.verify_checksums && !r.failed);
       bt.any_keep_decoded = bt.any_keep_decoded || (j->keep_decoded && !r.failed);
       bt.max_blocks_in = std::max(bt.max_blocks_in, cap_blk);
+    }
+    if (host_up) {
+      CK(cudaEventRecord(e->up_lane.done, st));
+      e->up_lane.any = true;
+      up_lk.unlock();
     }
     JobDev* hj = reinterpret_cast<JobDev*>(pin1 + o_hj);
     for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
@@ -1258,6 +1283,16 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       memcpy(r.j->key_bytes.data(), q, std::min<uint64_t>(kb, r.j->key_bytes.size()));
     }
     std::vector<lc_job*> retry;  // single-pass jobs whose key arena was too small
+    // downloads of this batch after the previous batch's (CopyLane)
+    std::unique_lock<std::mutex> down_lk(e->down_lane.mu, std::defer_lock);
+    bool host_down = false;
+    for (uint32_t i = 0; i < B; i++)
+      host_down = host_down || (!runs[i].failed && runs[i].j->outputs_on_device != 1 &&
+                                hc[i].bytes_out && !hc[i].error);
+    if (host_down) {
+      down_lk.lock();
+      if (e->down_lane.any) CK(cudaStreamWaitEvent(st, e->down_lane.done, 0));
+    }
     for (uint32_t i = 0; i < B; i++) {
       JobRun& r = runs[i];
       if (r.failed) continue;
@@ -1326,6 +1361,11 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
           j->out_dec_ptrs[f] = &x;
         }
       }
+    }
+    if (host_down) {
+      CK(cudaEventRecord(e->down_lane.done, st));
+      e->down_lane.any = true;
+      down_lk.unlock();
     }
     T.mark(kDownload);
     CK(cudaEventRecord(ev1, st));
@@ -1837,6 +1877,8 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
     host_crc_tables(t);
     CK(cudaMalloc(&e->crc_xpow, t.size() * 4));
     CK(cudaMemcpy(e->crc_xpow, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaEventCreateWithFlags(&e->up_lane.done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->down_lane.done, cudaEventDisableTiming));
     for (int i = 0; i < e->max_inflight; i++) {
       std::unique_ptr<lc_slot> sl(new lc_slot());
       sl->init(e->device, e->max_batch);
@@ -1847,6 +1889,8 @@ lc_status lc_engine_create(const lc_config* cfg, lc_engine** out) {
   } catch (const CudaError& ce) {
     std::string m = std::string(ce.what) + ": " + cudaGetErrorString(ce.e);
     if (e->crc_xpow) cudaFree(e->crc_xpow);
+    if (e->up_lane.done) cudaEventDestroy(e->up_lane.done);
+    if (e->down_lane.done) cudaEventDestroy(e->down_lane.done);
     e->dev_out.clear();
     e->scratch.clear();
     e->pinned.clear();
@@ -1872,6 +1916,8 @@ void lc_engine_destroy(lc_engine* e) {
   e->dev_out.clear();
   e->scratch.clear();
   cudaFree(e->crc_xpow);
+  cudaEventDestroy(e->up_lane.done);
+  cudaEventDestroy(e->down_lane.done);
   delete e;  // destroys the slots
 }
 
