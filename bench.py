@@ -103,9 +103,11 @@ def parse_args():
 
 # DRAM bytes (read + write) per launch of each kernel, from one ncu capture
 # on each workload: (workload, kernel) -> bytes; None where none was taken.
+# large_A's capture ran at scale 0.25 (profiles/k_encode_blocks_large_A.md:
+# 276.8 + 222.3 MB); the kernel's traffic grows with the bytes it moves, so
+# the full-size figure is four times that.
 NCU_TRAFFIC = {
-    ("l1_l2_at_size", "encode_blocks"): 88.962560e6 + 32.451328e6,
-    ("l1_l2_at_size", "decode"): 68.024832e6 + 3.235840e6,
+    ("large_A", "encode_blocks"): 4 * (276.819968e6 + 222.344192e6),
 }
 
 
@@ -315,7 +317,11 @@ def alg_bytes(r, in_bytes):
     n_in, k_in = r.entries_in, r.key_bytes_in
     n_keep, k_keep, v_keep = r.entries_out, r.key_bytes_out, r.value_bytes_out
     return {
-        "decode": in_bytes + k_in + 16 * n_in,
+        # the decode reads the 32-byte sectors holding the entry headers and
+        # key deltas (values are not read; at most the whole input), writes
+        # the keys and 32 bytes of entry arrays, and passes a 16-byte record
+        # per entry from its header walk to its key pass
+        "decode": min(in_bytes, 32 * n_in + k_in) + k_in + 32 * n_in + 32 * n_in,
         "merge": k_in + 16 * n_in + 4 * n_in,
         # merged ids, key offsets and lengths, tags, prefixes; keep flags and
         # grandparent counts written
@@ -479,7 +485,7 @@ def job_leg(name, args, eng, eng_ph, flush, torch, steps, warmup, clocks=None, p
                 "bytes_h2d": int(src.numel()), "bytes_d2h": int(d2h),
                 "note": "copy test: one pinned-host<->device copy of the job's input and output "
                         "bytes, best of 3; engine: its upload and download phases for one job "
-                        "from host buffers (copies split in 2 MiB pieces)"}
+                        "from host buffers (copies in pieces of about a sixteenth of the job, 2-64 MiB)"}
         del src, dst, back
 
     cpu_res = None

@@ -86,14 +86,16 @@ __global__ void k_table_index_count(const JobDev* __restrict__ jobs) {
   if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
   if (T.cached) {  // read from its decoded form: pseudo blocks of kDecRunBlock entries
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
       J.tbl_nblocks[t] = (uint32_t)((J.dec_runs[t].n + kDecRunBlock - 1) / kDecRunBlock);
+      J.tbl_unit[t] = 0;
+    }
     return;
   }
   const uint8_t* base = J.in + T.off;
   __shared__ uint64_t s_ioff, s_isize;
   __shared__ uint32_t s_nr, s_ok;
-  __shared__ uint32_t s_part[32];
+  __shared__ uint32_t s_part[32], s_other[32];
   if (threadIdx.x == 0) {
     uint64_t io = 0, is = 0;
     bool ok = parse_footer(base, T.size, &io, &is);
@@ -110,27 +112,48 @@ __global__ void k_table_index_count(const JobDev* __restrict__ jobs) {
   }
   __syncthreads();
   if (!s_ok) {
-    if (threadIdx.x == 0) J.tbl_nblocks[t] = 0;
+    if (threadIdx.x == 0) {
+      J.tbl_nblocks[t] = 0;
+      J.tbl_unit[t] = 0;
+    }
     return;
   }
   const uint8_t* ra = base + s_ioff + s_isize - 4 - 4ull * s_nr;
-  uint32_t sum = 0;
-  for (uint32_t r = threadIdx.x; r < s_nr; r += blockDim.x) sum += ld_le32(ra + 4ull * r) & 0xff;
+  uint32_t sum = 0, other = 0;  // entries; restart runs of other than one entry
+  for (uint32_t r = threadIdx.x; r < s_nr; r += blockDim.x) {
+    const uint32_t c = ld_le32(ra + 4ull * r) & 0xff;
+    sum += c;
+    other += c != 1;
+  }
   sum = warp_sum(sum);
-  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = sum;
+  other = warp_sum(other);
+  if ((threadIdx.x & 31) == 0) {
+    s_part[threadIdx.x >> 5] = sum;
+    s_other[threadIdx.x >> 5] = other;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint32_t s = 0;
-    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) s += s_part[w];
+    uint32_t s = 0, o = 0;
+    for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) s += s_part[w], o += s_other[w];
     J.tbl_nblocks[t] = s;
+    J.tbl_unit[t] = o == 0;
   }
 }
 
+// Data block handles from the index blocks.  An index block whose restart
+// runs each hold one entry (the table builder writes index blocks with a
+// restart interval of 1) is cut into kIdxSplit parts, one CTA each, every
+// thread parsing its own entries; any other is parsed by one CTA, the
+// entries' places from a block-wide scan of the run counts.
+constexpr uint32_t kIdxSplit = 16;
+
 __global__ void k_table_index_entries(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
-  const uint32_t t = blockIdx.x;
+  const uint32_t t = blockIdx.x / kIdxSplit, part = blockIdx.x % kIdxSplit;
   if (t >= J.n_tables) return;
   const TableDesc T = J.tables[t];
+  const bool unit = J.tbl_unit[t] != 0;
+  if (part != 0 && (T.cached || !unit)) return;
   if (T.cached) {
     const uint64_t out_base = J.tbl_block_base[t], out_end = J.tbl_block_base[t + 1];
     for (uint64_t o = out_base + threadIdx.x; o < out_end && o < J.cap_blocks_in; o += blockDim.x) {
@@ -150,6 +173,37 @@ __global__ void k_table_index_entries(const JobDev* __restrict__ jobs) {
   const uint8_t* ra = idx + ra_off;
   const uint64_t out_base = J.tbl_block_base[t];
   const uint64_t out_end = J.tbl_block_base[t + 1];
+  if (unit) {
+    const uint32_t r0 = (uint32_t)((uint64_t)nr * part / kIdxSplit);
+    const uint32_t r1 = (uint32_t)((uint64_t)nr * (part + 1) / kIdxSplit);
+    for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const uint64_t start = ld_le32(ra + 4ull * r) >> 8;
+      const uint64_t end = (r + 1 < nr) ? (ld_le32(ra + 4ull * (r + 1)) >> 8) : ra_off;
+      bool ok = start <= end && end <= ra_off;
+      const uint8_t* p = idx + start;
+      const uint8_t* lim = idx + end;
+      uint32_t sh, ns, vl;
+      const uint8_t* q = ok ? entry_header(p, lim, &sh, &ns, &vl) : nullptr;
+      uint64_t b_off = 0, b_size = 0;
+      const uint8_t* h = nullptr;
+      if (q) {
+        q += ns;
+        h = get_varint64(q, q + vl, &b_off);
+        if (h) h = get_varint64(h, q + vl, &b_size);
+      }
+      const uint64_t o = out_base + r;
+      ok = h && b_off <= T.size && b_size + kTrailer <= T.size - b_off && o < out_end &&
+           o < J.cap_blocks_in && q + vl == lim;
+      if (ok) {
+        J.blk_off[o] = T.off + b_off;
+        J.blk_size[o] = (uint32_t)b_size;
+        J.blk_run[o] = T.run;
+      } else {
+        set_error(J.ctr, kErrBadIndex, t);
+      }
+    }
+    return;
+  }
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
   if (threadIdx.x == 0) s_carry = 0;
@@ -567,13 +621,8 @@ __global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ 
       const uint8_t* qp = p + s;
       const uint8_t* lim = p + e;  // run ranges checked by k_block_restarts
       const uint32_t boff = (uint32_t)J.blk_off[b];
-      // the run's first lines into L1 ahead of the walk, and one line further
-      // at every entry (a run of short entries is read as a stream)
-      for (uint32_t x = 0; x < 3; x++)
-        if (qp + 128 * x < lim) prefetch_l1(qp + 128 * x);
       uint32_t prev = 0;
       for (uint32_t k = 0; k < cnt; k++) {
-        if (qp + 384 < lim) prefetch_l1(qp + 384);
         uint32_t sh, ns, vl;
         const uint8_t* d = entry_header(qp, lim, &sh, &ns, &vl);
         if (!d || (k == 0 && sh != 0) || sh > prev) {
@@ -793,7 +842,7 @@ void launch_table_index_count(const Batch& bt, cudaStream_t st) {
   note_launch(), k_table_index_count<<<dim3(bt.max_tables, bt.B), 1024, 0, st>>>(bt.d);
 }
 void launch_table_index_entries(const Batch& bt, cudaStream_t st) {
-  note_launch(), k_table_index_entries<<<dim3(bt.max_tables, bt.B), 1024, 0, st>>>(bt.d);
+  note_launch(), k_table_index_entries<<<dim3(bt.max_tables * kIdxSplit, bt.B), 1024, 0, st>>>(bt.d);
 }
 
 static void dec_smem_attr(const void* fn) {

@@ -175,27 +175,63 @@ __global__ void k_next(const JobDev* __restrict__ jobs) {
 
 
 // Per chunk: exits of the chain for every entry point in the first `window`
-// survivors of the chunk.
+// survivors of the chunk.  The chunk's next() values are staged in shared
+// memory and cut into sub-chunks of kChainSub survivors: every (sub-chunk,
+// entry point) pair is walked in parallel to the sub-chunk's exit, and the
+// chunk's exits are composed from the sub-chunk exits (C / kChainSub steps
+// per entry point instead of a walk over the whole chunk).  Windows wider
+// than a sub-chunk walk the chunk directly.
+constexpr uint32_t kChainSub = 256;
+
+// Exit of sub-chunk s of a staged chunk [c0, c1) for entry point e (an
+// absolute survivor index inside the sub-chunk's first `W`).
+__device__ __forceinline__ uint64_t chain_sub_walk(const uint32_t* s_next, uint64_t c0, uint64_t c1,
+                                                   uint64_t e, uint64_t sub_end) {
+  const uint64_t end = min(c1, sub_end);
+  while (e < end) e = s_next[e - c0];
+  return e;
+}
+
 __global__ void k_chain_tables(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
   if (threadIdx.x == 0) s_failed = J.ctr->error;
   __syncthreads();
   if (s_failed) return;
-  extern __shared__ uint32_t s_next[];
+  extern __shared__ uint32_t s_next[];  // chunk next() values, then sub-chunk exits
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
   const uint32_t W = J.ctr->max_jump;
   if (W > C) return;  // resolved sequentially instead
+  const bool sub = W <= kChainSub;
+  uint32_t* s_sub = s_next + C;  // (C / kChainSub) x W sub-chunk exits
   for (uint64_t c = blockIdx.x; c * C < n; c += gridDim.x) {
     const uint64_t c0 = c * C;
     const uint64_t c1 = min(n, c0 + C);
     __syncthreads();
     for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
     __syncthreads();
+    if (!sub) {
+      for (uint32_t i = threadIdx.x; i < W; i += blockDim.x) {
+        uint64_t e = c0 + i;
+        while (e < c1) e = s_next[e - c0];
+        J.chunk_table[c * C + i] = (uint32_t)e;
+      }
+      continue;
+    }
+    const uint32_t nsub = (uint32_t)((c1 - c0 + kChainSub - 1) / kChainSub);
+    for (uint32_t x = threadIdx.x; x < nsub * W; x += blockDim.x) {
+      const uint32_t sb = x / W, i = x % W;
+      const uint64_t s0 = c0 + (uint64_t)sb * kChainSub;
+      s_sub[x] = (uint32_t)chain_sub_walk(s_next, c0, c1, s0 + i, s0 + kChainSub);
+    }
+    __syncthreads();
     for (uint32_t i = threadIdx.x; i < W; i += blockDim.x) {
       uint64_t e = c0 + i;
-      while (e < c1) e = s_next[e - c0];
+      for (uint32_t sb = 0; sb < nsub && e < c1; sb++) {
+        const uint64_t s0 = c0 + (uint64_t)sb * kChainSub;
+        e = s_sub[sb * W + (uint32_t)(e - s0)];  // e lies in the sub-chunk's first W survivors
+      }
       J.chunk_table[c * C + i] = (uint32_t)e;
     }
   }
@@ -294,6 +330,10 @@ __global__ void k_chain_resolve(const JobDev* __restrict__ jobs) {
   }
 }
 
+// Block starts: each chunk's chain from its resolved entry point.  With
+// sub-chunks, one thread finds the sub-chunks' entry points from their exits
+// (recomputed as k_chain_tables does) and every sub-chunk is walked by its
+// own thread.
 __global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_failed;  // read once per CTA: the CTA's barriers stay uniform
@@ -303,16 +343,47 @@ __global__ void k_chain_mark(const JobDev* __restrict__ jobs) {
   extern __shared__ uint32_t s_next[];
   const uint64_t n = J.ctr->n_kept;
   const uint32_t C = J.chunk;
-  if (J.ctr->max_jump > C) return;
+  const uint32_t W = J.ctr->max_jump;
+  if (W > C) return;
+  const bool sub = W <= kChainSub;
+  uint32_t* s_sub = s_next + C;
+  uint32_t* s_entry = s_sub + (C / kChainSub) * (sub ? W : 0);  // sub-chunk entry points
   for (uint64_t c = blockIdx.x; c * C < n; c += gridDim.x) {
     const uint64_t c0 = c * C;
     const uint64_t c1 = min(n, c0 + C);
     __syncthreads();
     for (uint64_t i = threadIdx.x; i < c1 - c0; i += blockDim.x) s_next[i] = J.k_next[c0 + i];
     __syncthreads();
+    if (!sub) {
+      if (threadIdx.x == 0) {
+        uint64_t e = J.chunk_entry[c];
+        while (e < c1) {
+          J.k_bstart[e] = 1;
+          e = s_next[e - c0];
+        }
+      }
+      continue;
+    }
+    const uint32_t nsub = (uint32_t)((c1 - c0 + kChainSub - 1) / kChainSub);
+    for (uint32_t x = threadIdx.x; x < nsub * W; x += blockDim.x) {
+      const uint32_t sb = x / W, i = x % W;
+      const uint64_t s0 = c0 + (uint64_t)sb * kChainSub;
+      s_sub[x] = (uint32_t)chain_sub_walk(s_next, c0, c1, s0 + i, s0 + kChainSub);
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
       uint64_t e = J.chunk_entry[c];
-      while (e < c1) {
+      for (uint32_t sb = 0; sb < nsub; sb++) {
+        s_entry[sb] = (uint32_t)e;
+        const uint64_t s0 = c0 + (uint64_t)sb * kChainSub;
+        if (e < c1) e = s_sub[sb * W + (uint32_t)(e - s0)];
+      }
+    }
+    __syncthreads();
+    for (uint32_t sb = threadIdx.x; sb < nsub; sb += blockDim.x) {
+      const uint64_t s0 = c0 + (uint64_t)sb * kChainSub, send = min(c1, s0 + kChainSub);
+      uint64_t e = s_entry[sb];
+      while (e < send) {
         J.k_bstart[e] = 1;
         e = s_next[e - c0];
       }
@@ -1036,11 +1107,19 @@ __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
     if (gb != 0 && J.b_gkeys[b] <= kFilterThreadKeys && gb - 1 <= kFilterLocal)
       filter_group_thread(J, b, gb);
   }
+  // the larger groups: each warp looks at 32 blocks at once and builds the
+  // ones that need it
   const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t b = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += stride) {
-    const uint32_t gb = J.b_gbytes[b];
-    if (gb != 0 && (J.b_gkeys[b] > kFilterThreadKeys || gb - 1 > kFilterLocal))
-      encode_filter_group(J, b, lane, s_filter[threadIdx.x >> 5]);
+  for (uint64_t b0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; b0 < nb;
+       b0 += stride * 32) {
+    const uint64_t b = b0 + lane;
+    bool big = false;
+    if (b < nb) {
+      const uint32_t gb = J.b_gbytes[b];
+      big = gb != 0 && (J.b_gkeys[b] > kFilterThreadKeys || gb - 1 > kFilterLocal);
+    }
+    for (unsigned m = __ballot_sync(0xffffffffu, big); m; m &= m - 1)
+      encode_filter_group(J, b0 + (__ffs(m) - 1), lane, s_filter[threadIdx.x >> 5]);
   }
 }
 
@@ -1150,7 +1229,7 @@ __global__ void __launch_bounds__(256) k_encode_meta(const JobDev* __restrict__ 
 // byte's share is the register of the whole), and k_meta_trailers writes the
 // finished CRCs.  kMetaCtas CTAs per file.
 constexpr uint32_t kMetaPiece = 4096;
-constexpr uint32_t kMetaCtas = 8;
+constexpr uint32_t kMetaCtas = 32;
 
 __device__ __forceinline__ void meta_region(const FileOut& F, uint32_t r, uint64_t* off,
                                             uint64_t* len) {
@@ -1244,7 +1323,8 @@ void launch_next(const Batch& bt, cudaStream_t st) {
 }
 void launch_chain(const Batch& bt, cudaStream_t st) {
   const uint64_t chunks = (bt.max_entries + bt.chunk - 1) / bt.chunk + 1;
-  const size_t smem = (size_t)bt.chunk * sizeof(uint32_t);
+  // next() values, sub-chunk exits (windows up to kChainSub) and entry points
+  const size_t smem = ((size_t)bt.chunk + (bt.chunk / kChainSub) * (kChainSub + 1)) * sizeof(uint32_t);
   const unsigned g = (unsigned)std::min<uint64_t>(chunks, per_job(bt, 148 * 4));
   note_launch(), k_chain_tables<<<dim3(g, bt.B), 256, smem, st>>>(bt.d);
   if (chunks > kChainGroup)

@@ -67,20 +67,27 @@ struct StatusError {
 
 uint64_t round16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
 
-// A host<->device copy as copies of at most 2 MiB.  With one job's upload and
-// another's download in flight at once (the pipelined case), one large copy
-// in one direction took most of the PCIe bandwidth from many smaller ones in
-// the other (measured on B200: 68 MB down at 50 GB/s while 33 table uploads
-// got 31 GB/s); pieces of similar size in both directions share the link
-// evenly (40 + 40 GB/s) and a pipelined job finishes ~20% sooner.
-void copy_pieces(void* dst, const void* src, uint64_t n, cudaMemcpyKind kind, cudaStream_t st) {
-  constexpr uint64_t kPiece = 2ull << 20;
+// A host<->device copy as pieces of `piece` bytes.  Jobs' host copies run one
+// job at a time per direction (CopyLane), so an upload shares the link only
+// with one download.  Measured on B200 with an upload and a download of 1 GiB
+// each in flight at once: pieces of 2 MiB moved 40 + 40 GB/s, of 16 MiB
+// 46 + 49, whole copies 50 + 51 (55 and 57 GB/s each alone).  A copy engine
+// takes one piece at a time, so the next job's copies in the same direction
+// wait up to one piece: piece_for() keeps a piece at about a sixteenth of
+// the job's bytes (64 MiB pieces had slowed pipelined 66 MiB jobs by half).
+void copy_pieces(void* dst, const void* src, uint64_t n, cudaMemcpyKind kind, cudaStream_t st,
+                 uint64_t piece) {
   if (kind == cudaMemcpyDeviceToDevice) {
     CK(cudaMemcpyAsync(dst, src, n, kind, st));
     return;
   }
-  for (uint64_t o = 0; o < n; o += kPiece)
-    CK(cudaMemcpyAsync((uint8_t*)dst + o, (const uint8_t*)src + o, std::min(kPiece, n - o), kind, st));
+  for (uint64_t o = 0; o < n; o += piece)
+    CK(cudaMemcpyAsync((uint8_t*)dst + o, (const uint8_t*)src + o, std::min(piece, n - o), kind, st));
+}
+uint64_t piece_for(uint64_t job_bytes) {
+  uint64_t p = 2ull << 20;
+  while (p < (64ull << 20) && p * 2 <= job_bytes / 16) p *= 2;
+  return p;
 }
 
 // Memory for job outputs and scratch, pinned host memory or device memory.  Taking
@@ -1061,7 +1068,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     uint8_t* pin1 = slot.pinned(o_hc + sizeof(Counters) * B);
     memcpy(pin1, S.h.data(), S.h.size());
     uint8_t* d_stage = A.get<uint8_t>(S.h.size());
-    CK(cudaMemcpyAsync(d_stage, pin1, S.h.size(), cudaMemcpyHostToDevice, st));
+    slot.to_device(d_stage, pin1, S.h.size());  // not behind other jobs' bulk copies
     uint8_t* d_in_all = in_total ? A.get<uint8_t>(in_total) : nullptr;
     Counters* d_ctr = A.get<Counters>(B);
     CK(cudaMemsetAsync(d_ctr, 0, sizeof(Counters) * B, st));
@@ -1090,7 +1097,8 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
         for (uint32_t t = 0; t < J.n_tables && !r.failed; t++) {
           if (!j->tables[t].size) continue;
           copy_pieces((uint8_t*)J.in + tds[i][t].off, j->tables[t].data, j->tables[t].size,
-                      j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+                      j->inputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st,
+                      piece_for(J.in_size));
         }
       }
       J.in_end = J.in + J.in_size + (zero_copy[i] ? 0 : 16);
@@ -1113,6 +1121,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
       const uint64_t cap_blk = r.cap_blk;
       J.cap_blocks_in = cap_blk;
       J.tbl_nblocks = A.get<uint32_t>(J.n_tables);
+      J.tbl_unit = A.get<uint32_t>(J.n_tables);
       J.tbl_block_base = A.get<uint64_t>(J.n_tables + 1);
       J.blk_off = A.get<uint64_t>(cap_blk);
       J.blk_size = A.get<uint32_t>(cap_blk);
@@ -1136,7 +1145,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
     }
     JobDev* hj = reinterpret_cast<JobDev*>(pin1 + o_hj);
     for (uint32_t i = 0; i < B; i++) hj[i] = runs[i].J;
-    CK(cudaMemcpyAsync(slot.d_jobs, hj, sizeof(JobDev) * B, cudaMemcpyHostToDevice, st));
+    slot.to_device(slot.d_jobs, (const uint8_t*)hj, sizeof(JobDev) * B);
     T.mark(kUpload);
     e->note_setup(t_setup0);
     // ---- parse: index blocks, then entry counts -- exact: a walk of every
@@ -1316,7 +1325,7 @@ void run_batch(std::vector<lc_job*>& jobs, lc_slot& slot, const Tunables& tun,
           job_fail(r, LC_ERR_NO_MEMORY, "pinned host buffer");
           continue;
         }
-        copy_pieces(j->h_out, r.J.out, nbytes, cudaMemcpyDeviceToHost, st);
+        copy_pieces(j->h_out, r.J.out, nbytes, cudaMemcpyDeviceToHost, st, piece_for(nbytes));
       }
       const uint32_t nf = hc[i].n_files;
       j->file_offset.resize(nf);
@@ -1467,8 +1476,8 @@ void run_build(lc_job* j, lc_slot& slot) {
     uint8_t* d_vals = A.get<uint8_t>(vb + 16);
     uint64_t* d_ko = A.get<uint64_t>(N + 1);
     uint64_t* d_vo = A.get<uint64_t>(N + 1);
-    if (kb) copy_pieces(J.keys, j->bkeys, kb, kind, st);
-    if (vb) copy_pieces(d_vals, j->bvals, vb, kind, st);
+    if (kb) copy_pieces(J.keys, j->bkeys, kb, kind, st, piece_for(kb + vb));
+    if (vb) copy_pieces(d_vals, j->bvals, vb, kind, st, piece_for(kb + vb));
     CK(cudaMemcpyAsync(d_ko, j->bkoffs, (N + 1) * 8, kind, st));
     CK(cudaMemcpyAsync(d_vo, j->bvoffs, (N + 1) * 8, kind, st));
     J.in = d_vals;
@@ -1525,7 +1534,7 @@ void run_build(lc_job* j, lc_slot& slot) {
     if (nbytes) {
       j->h_out = e->pinned.take(nbytes, &j->h_out_cap);
       if (!j->h_out) throw StatusError{LC_ERR_NO_MEMORY, "pinned host buffer"};
-      copy_pieces(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st);
+      copy_pieces(j->h_out, J.out, nbytes, cudaMemcpyDeviceToHost, st, piece_for(nbytes));
     }
     const uint32_t nf = hc.n_files;
     j->file_offset.resize(nf);

@@ -142,6 +142,7 @@ struct JobDev {
 
   // input blocks
   uint32_t* tbl_nblocks;     // n_tables
+  uint32_t* tbl_unit;        // n_tables: 1 when every index restart run holds one entry
   uint64_t* tbl_block_base;  // n_tables + 1
   uint64_t* blk_off;         // cap_blocks_in
   uint32_t* blk_size;
