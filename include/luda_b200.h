@@ -28,12 +28,14 @@ extern "C" {
 typedef enum {
   LC_OK = 0,
   LC_ERR_INVALID_ARG = 1, /* bad descriptor, option or handle */
-  LC_ERR_CORRUPT = 2,     /* an input table failed a format check */
+  LC_ERR_CORRUPT = 2,     /* an input table failed a format check, or a merge
+                           * child's entries are out of internal-key order */
   LC_ERR_CUDA = 3,        /* a CUDA runtime call failed */
   LC_ERR_NO_MEMORY = 4,   /* device or host allocation failed */
   LC_ERR_BUDGET = 5,      /* job larger than the engine's device budget */
   LC_ERR_TIMEOUT = 6,     /* lc_job_wait timed out, or a device wait gave up */
-  LC_ERR_UNSUPPORTED = 7, /* input beyond an engine limit (e.g. >= 4 GiB) */
+  LC_ERR_UNSUPPORTED = 7, /* input beyond an engine limit (a job of 4 GiB or more,
+                           * a key of 64 KiB or more) */
   LC_ERR_SHUTDOWN = 8     /* engine is being destroyed */
 } lc_status;
 

@@ -621,6 +621,10 @@ __global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ 
       const uint8_t* qp = p + s;
       const uint8_t* lim = p + e;  // run ranges checked by k_block_restarts
       const uint32_t boff = (uint32_t)J.blk_off[b];
+      // the record arrays in registers: the stores below cannot then make the
+      // compiler reload them from the job descriptor
+      uint4* const rec = J.e_rec + ebase + before;
+      uint32_t* const klen = J.e_klen + ebase + before;
       uint32_t prev = 0;
       for (uint32_t k = 0; k < cnt; k++) {
         uint32_t sh, ns, vl;
@@ -633,8 +637,8 @@ __global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ 
         if (kl < 8) short_key = true;
         if (kl > 0xffff || sh >= kDecPseudo) long_key = true;
         const uint32_t doff = boff + (uint32_t)(d - p);
-        J.e_rec[ebase + before + k] = dec_record(doff, sh, kl, vl, doff + ns);
-        J.e_klen[ebase + before + k] = kl;
+        rec[k] = dec_record(doff, sh, kl, vl, doff + ns);
+        klen[k] = kl;
         kb += kl;
         maxk = max(maxk, kl);
         prev = kl;
@@ -737,20 +741,36 @@ __global__ void __launch_bounds__(256) k_decode_keys(const JobDev* __restrict__ 
           for (uint32_t t = 0; t < dl; t += 32) copy_small_w(kb + ko + sh + t, src + t, min(32u, dl - t));
         }
         __syncwarp();
-        // shared prefixes: a key's bytes below the least shared length of
-        // the round's entries up to it are the previous round's last key's;
-        // each other prefix byte is the own (delta) byte of the nearest
-        // earlier entry whose shared length lies below it -- the entries in
-        // between share it -- found by walking back (every walk ends at the
-        // entry with that least shared length)
-        uint32_t m = valid ? sh : 0;
+        // shared prefixes.  Within the round, an entry z without a shared
+        // prefix holds its whole key as its delta; for the entries after it
+        // (up to the next such entry), the bytes below the least shared
+        // length since z are z's bytes -- every entry in between shares them.
+        // Before the round's first such entry the same holds with the
+        // previous round's last key.  Each other prefix byte is the own
+        // (delta) byte of the nearest earlier entry whose shared length lies
+        // below it (the entries in between share it), found by a walk back
+        // that ends at the entry with that least shared length.
+        const unsigned zmask = __ballot_sync(0xffffffffu, valid && sh == 0);
+        const unsigned zbelow = zmask & (0xffffffffu >> (31 - lane));
+        const int z = zbelow ? 31 - __clz(zbelow) : -1;
+        const uint32_t koz = __shfl_sync(0xffffffffu, ko, z < 0 ? 0 : z);
+        // segmented running minimum of the shared lengths since z (z excluded)
+        uint32_t m = (valid && sh != 0) ? sh : 0xffffffffu;
+        bool seg = valid && sh == 0;  // this lane's range reaches a segment head
 #pragma unroll
         for (uint32_t o = 1; o < 32; o <<= 1) {
           const uint32_t y = __shfl_up_sync(0xffffffffu, m, o);
-          if (lane >= o) m = min(m, y);
+          const bool ys = __shfl_up_sync(0xffffffffu, seg, o);
+          if (lane >= o && !seg) {
+            m = min(m, y);
+            seg = ys;
+          }
         }
-        if (valid)
-          for (uint32_t t = 0; t < m; t++) kb[ko + t] = W.last[t];
+        if (!valid || sh == 0) m = 0;
+        if (valid && m) {
+          const uint8_t* from = z >= 0 ? kb + koz : W.last;
+          for (uint32_t t = 0; t < m; t++) kb[ko + t] = from[t];
+        }
         uint32_t lim = valid ? sh : 0;
         for (uint32_t d = 1; d < 32 && __any_sync(0xffffffffu, lim > m); d++) {
           const uint32_t j = lane >= d ? lane - d : lane;

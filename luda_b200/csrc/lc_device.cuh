@@ -143,32 +143,46 @@ __device__ __forceinline__ bool same_user_key(const JobDev& J, uint32_t a, uint6
   return true;
 }
 
-// util/hash.cc:22-51.
-__device__ __forceinline__ uint32_t leveldb_hash(const uint8_t* data, uint32_t n, uint32_t seed) {
+// Hash of util/hash.cc:22-51 (the bloom filter's hash) over bytes that may
+// start at any alignment, four at a time from aligned word loads realigned by
+// funnel shifts.  Reads up to one word past the data: only for data in a
+// buffer with that much slack (the key arena keeps 16 bytes).
+__device__ __forceinline__ uint32_t leveldb_hash_words(const uint8_t* data, uint32_t n,
+                                                       uint32_t seed) {
   const uint32_t m = 0xc6a4a793u;
-  const uint8_t* limit = data + n;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(data);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = 8 * (uint32_t)(a & 3);
   uint32_t h = seed ^ (n * m);
-  while (data + 4 <= limit) {
-    h += ld_le32(data);
-    data += 4;
+  uint32_t lo = q[0], i = 0;
+  for (; i + 4 <= n; i += 4) {
+    const uint32_t hi = q[(i >> 2) + 1];
+    h += __funnelshift_r(lo, hi, sh);
+    lo = hi;
     h *= m;
     h ^= (h >> 16);
   }
-  switch (limit - data) {
-    case 3:
-      h += (uint32_t)data[2] << 16;
-      [[fallthrough]];
-    case 2:
-      h += (uint32_t)data[1] << 8;
-      [[fallthrough]];
-    case 1:
-      h += data[0];
-      h *= m;
-      h ^= (h >> 24);
-      break;
+  const uint32_t r = n - i;
+  if (r) {
+    const uint32_t w = __funnelshift_r(lo, q[(i >> 2) + 1], sh);  // bytes i.. of the data
+    h += w & ((1u << (8 * r)) - 1u);
+    h *= m;
+    h ^= (h >> 24);
   }
   return h;
 }
+
+// a % d for 32-bit a and a divisor d >= 1 fixed over many calls, from
+// M = floor((2^64 - 1) / d) + 1: (M a mod 2^64) d >> 64 (Lemire, Kaser and
+// Kurz, "Faster remainder by direct computation", 2019).
+struct FastMod {
+  uint64_t M;
+  uint32_t d;
+  __device__ __forceinline__ explicit FastMod(uint32_t div) : M(~0ull / div + 1), d(div) {}
+  __device__ __forceinline__ uint32_t operator()(uint32_t a) const {
+    return (uint32_t)__umul64hi(M * a, d);
+  }
+};
 
 // ---------------------------------------------------------------------------
 // CRC32C

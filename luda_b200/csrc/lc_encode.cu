@@ -1020,13 +1020,14 @@ __device__ __forceinline__ void encode_filter_group(const JobDev& J, uint64_t b,
     __syncwarp();
     const uint64_t k0 = J.b_first[b];
     const uint32_t nk = J.b_gkeys[b];
+    const FastMod mod(bits);
     for (uint32_t i = lane; i < nk; i += 32) {
       uint32_t kl;
       const uint8_t* key = kept_key(J, k0 + i, &kl);
-      uint32_t h = leveldb_hash(key, kl - 8, 0xbc9f1d34u);
+      uint32_t h = leveldb_hash_words(key, kl - 8, 0xbc9f1d34u);
       const uint32_t delta = (h >> 17) | (h << 15);
       for (uint32_t q = 0; q < J.bloom_k; q++) {
-        const uint32_t bitpos = (uint32_t)(h % bits);
+        const uint32_t bitpos = mod(h);
         if (in_smem) {
           // byte bitpos/8, bit bitpos%8 = bit (bitpos & 31) of little-endian word bitpos/32
           atomicOr(&sbuf[bitpos >> 5], 1u << (bitpos & 31));
@@ -1073,13 +1074,14 @@ __device__ __forceinline__ void filter_group_thread(const JobDev& J, uint64_t b,
   for (uint32_t i = 0; i < kFilterLocal / 4; i++) w[i] = 0;
   const uint64_t k0 = J.b_first[b];
   const uint32_t nk = J.b_gkeys[b];
+  const FastMod mod(bits);
   for (uint32_t i = 0; i < nk; i++) {
     uint32_t kl;
     const uint8_t* key = kept_key(J, k0 + i, &kl);
-    uint32_t h = leveldb_hash(key, kl - 8, 0xbc9f1d34u);
+    uint32_t h = leveldb_hash_words(key, kl - 8, 0xbc9f1d34u);
     const uint32_t delta = (h >> 17) | (h << 15);
     for (uint32_t q = 0; q < J.bloom_k; q++) {
-      const uint32_t bitpos = h % bits;
+      const uint32_t bitpos = mod(h);
       w[bitpos >> 5] |= 1u << (bitpos & 31);  // byte bitpos/8, bit bitpos%8
       h += delta;
     }
@@ -1107,19 +1109,20 @@ __global__ void k_encode_filters(const JobDev* __restrict__ jobs) {
     if (gb != 0 && J.b_gkeys[b] <= kFilterThreadKeys && gb - 1 <= kFilterLocal)
       filter_group_thread(J, b, gb);
   }
-  // the larger groups: each warp looks at 32 blocks at once and builds the
-  // ones that need it
-  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t b0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; b0 < nb;
-       b0 += stride * 32) {
-    const uint64_t b = b0 + lane;
+  // the larger groups: warp w takes blocks w, w + W, w + 2W, ... (W warps in
+  // all), looking at 32 of them with one load per lane and building the ones
+  // that need it
+  const uint64_t W = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (uint64_t b0 = w; b0 < nb; b0 += 32 * W) {
+    const uint64_t b = b0 + lane * W;
     bool big = false;
     if (b < nb) {
       const uint32_t gb = J.b_gbytes[b];
       big = gb != 0 && (J.b_gkeys[b] > kFilterThreadKeys || gb - 1 > kFilterLocal);
     }
     for (unsigned m = __ballot_sync(0xffffffffu, big); m; m &= m - 1)
-      encode_filter_group(J, b0 + (__ffs(m) - 1), lane, s_filter[threadIdx.x >> 5]);
+      encode_filter_group(J, b0 + (uint64_t)(__ffs(m) - 1) * W, lane, s_filter[threadIdx.x >> 5]);
   }
 }
 
@@ -1227,9 +1230,9 @@ __global__ void __launch_bounds__(256) k_encode_meta(const JobDev* __restrict__ 
 // piece's 16-byte chunks); a piece's raw register, moved to the region's end
 // past its type byte, is xored into the file's accumulator (the xor of every
 // byte's share is the register of the whole), and k_meta_trailers writes the
-// finished CRCs.  kMetaCtas CTAs per file.
+// finished CRCs.  CTAs per file: from the entries per file (the filter and
+// index blocks grow with them), 4 to 32.
 constexpr uint32_t kMetaPiece = 4096;
-constexpr uint32_t kMetaCtas = 32;
 
 __device__ __forceinline__ void meta_region(const FileOut& F, uint32_t r, uint64_t* off,
                                             uint64_t* len) {
@@ -1376,7 +1379,11 @@ void launch_encode_index(const Batch& bt, cudaStream_t st) {
 }
 void launch_encode_meta(const Batch& bt, cudaStream_t st) {
   note_launch(), k_encode_meta<<<dim3(bt.max_cap_files, bt.B), 256, 0, st>>>(bt.d);
-  note_launch(), k_meta_crc<<<dim3(kMetaCtas, std::min<uint32_t>(bt.max_cap_files, 65535), bt.B),
+  uint32_t per_file = 4;
+  while (per_file < 32 && (uint64_t)per_file * 8192 * std::max<uint32_t>(bt.max_cap_files, 1) <
+                              bt.max_entries)
+    per_file *= 2;
+  note_launch(), k_meta_crc<<<dim3(per_file, std::min<uint32_t>(bt.max_cap_files, 65535), bt.B),
                               256, 0, st>>>(bt.d);
   note_launch(), k_meta_trailers<<<dim3((3 * bt.max_cap_files + 255) / 256, bt.B), 256, 0, st>>>(bt.d);
 }
