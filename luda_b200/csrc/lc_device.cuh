@@ -71,6 +71,18 @@ __host__ __device__ __forceinline__ uint32_t varint_len(uint64_t v) {
   }
   return n;
 }
+// 32-bit forms of the two above (no 64-bit shifts or compares).
+__device__ __forceinline__ uint32_t varint_len32(uint32_t v) {
+  return 1u + (v >= (1u << 7)) + (v >= (1u << 14)) + (v >= (1u << 21)) + (v >= (1u << 28));
+}
+__device__ __forceinline__ uint8_t* put_varint32(uint8_t* p, uint32_t v) {
+  while (v >= 128) {
+    *p++ = (uint8_t)(v | 128);
+    v >>= 7;
+  }
+  *p++ = (uint8_t)v;
+  return p;
+}
 __device__ __forceinline__ uint8_t* put_varint(uint8_t* p, uint64_t v) {
   while (v >= 128) {
     *p++ = (uint8_t)(v | 128);
@@ -261,6 +273,19 @@ __device__ __forceinline__ uint32_t crc_shift(const JobDev& J, uint32_t c, uint6
   return gf2_mulmod(crc_xpow8(J, n), c);
 }
 
+// shift(c, n) with the byte table tab (in shared memory): x^(8n) as the
+// product of two table entries (n = hi N + lo, N = crc_xpow_n) for n < N^2,
+// then one more product with c.
+__device__ __forceinline__ uint32_t crc_shift_tab(const JobDev& J, const uint32_t* tab,
+                                                  uint32_t c, uint64_t n) {
+  const uint64_t N = J.crc_xpow_n;
+  if (n >= N * N) return crc_shift(J, c, n);
+  const uint32_t lo = (uint32_t)(n % N), hi = (uint32_t)(n / N);
+  uint32_t m = __ldg(J.crc_xpow + lo);
+  if (hi) m = gf2_mulmod_tab(tab, m, __ldg(J.crc_xpow_hi + hi));
+  return gf2_mulmod_tab(tab, c, m);
+}
+
 // Masked CRC32C of contents followed by the type byte: the block trailer of
 // table/table_builder.cc:186-189, computed cooperatively by one warp over `n`
 // bytes at `p` (the type byte, 0 for an uncompressed block, is appended
@@ -288,23 +313,26 @@ __device__ __forceinline__ uint32_t warp_block_crc(const JobDev& J, const uint32
   return ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
 }
 
-// Up to 32 bytes from src (any alignment) to dst: every word that holds a
-// needed byte is loaded before any byte is stored (no load waits on the
-// previous store), then the words are realigned by funnel shifts.
+// Up to kMax (a multiple of 4, at most 32) bytes from src (any alignment) to
+// dst: every word that holds a needed byte is loaded before any byte is
+// stored (no load waits on the previous store), then the words are realigned
+// by funnel shifts.
+template <uint32_t kMax = 32>
 __device__ __forceinline__ void copy_small(uint8_t* dst, const uint8_t* src, uint32_t len) {
   if (!len) return;
+  constexpr uint32_t kW = kMax / 4 + 1;
   const uintptr_t a = reinterpret_cast<uintptr_t>(src);
   const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
   const uint32_t sh = 8 * (uint32_t)(a & 3);
   const uint32_t nw = ((uint32_t)(a & 3) + len + 3) >> 2;  // words holding the bytes
-  uint32_t w[9];
+  uint32_t w[kW];
 #pragma unroll
-  for (uint32_t i = 0; i < 9; i++) w[i] = i < nw ? __ldg(base + i) : 0u;
-  uint32_t r[8];
+  for (uint32_t i = 0; i < kW; i++) w[i] = i < nw ? __ldg(base + i) : 0u;
+  uint32_t r[kW - 1];
 #pragma unroll
-  for (uint32_t i = 0; i < 8; i++) r[i] = __funnelshift_r(w[i], w[i + 1], sh);
+  for (uint32_t i = 0; i + 1 < kW; i++) r[i] = __funnelshift_r(w[i], w[i + 1], sh);
 #pragma unroll
-  for (uint32_t i = 0; i < 32; i++)
+  for (uint32_t i = 0; i < kMax; i++)
     if (i < len) dst[i] = (uint8_t)(r[i >> 2] >> (8 * (i & 3)));
 }
 
@@ -360,6 +388,13 @@ namespace lc {
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");

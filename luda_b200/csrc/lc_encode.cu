@@ -654,18 +654,24 @@ __global__ void k_file_layout(const JobDev* __restrict__ jobs) {
 // stage, which has the block's own 16-byte phase in global memory: stage
 // position p is global byte dst - ph + p, ph = dst & 15.  Three steps:
 //  1. Entries in rounds of 32, one lane per entry: entry sizes and output
-//     offsets by a warp scan; the lane writes its entry header and restart
-//     word to the stage, and its key delta and value: a stretch shorter than
-//     kEncLong whole, a longer one only its unaligned head and tail, the
-//     16-byte chunks between joining the warp's list of long stretches (at
-//     most kEncMaxLong; a lane stages the chunks of a stretch past the list
-//     itself).
-//  2. The block's 16-byte chunks, lane l taking chunks l, l + 32, ..., two
-//     at a time: a chunk inside a listed stretch is read from global memory
-//     (five 4-byte loads and four funnel shifts at any source alignment),
-//     any other from the stage.  A chunk wholly inside the block and its
-//     type byte goes out with one 16-byte store, and every chunk feeds the
-//     lane's share of the block CRC (crc_chunk_step).
+//     offsets by a warp scan.  A key delta or value of at least kEncLong
+//     bytes lists its whole 16-byte chunks in the warp's list of long
+//     stretches (at most kEncMaxLong; a lane stages the chunks of a stretch
+//     past the list itself).  Once the list is complete (the last round), the
+//     listed chunks of the first two chunk rows are loaded, and while they
+//     are in flight the lanes write entry headers, restart words, short
+//     stretches whole and the unaligned heads and tails of long ones to the
+//     stage.
+//  2. The block's 16-byte chunks, lane l taking chunks l, l + 32, ..., each
+//     loaded two chunks ahead of its use: a chunk inside a listed stretch is
+//     read from global memory (five 4-byte loads and four funnel shifts at
+//     any source alignment), any other from the stage.  A chunk wholly
+//     inside the block and its type byte goes out with one 16-byte store,
+//     and every chunk feeds the lane's share of the block CRC (crc_h5).  The
+//     stage's first and last chunks are cleared before step 1, so the grid
+//     bytes outside the message are zero and every chunk takes the same CRC
+//     step; the initial all-ones register enters at the end, as its register
+//     carried over the message's length (crc_ones).
 //  3. The lanes' CRC shares combined, the trailer (type byte and CRC) into
 //     the stage, and the partial chunks at both ends from the stage with byte
 //     stores.
@@ -679,6 +685,8 @@ struct EncWarp {
   uint32_t ls_c0[kEncMaxLong];   // first whole chunk (stage grid) | kEncFromInput
   uint32_t ls_n[kEncMaxLong];    // whole chunks
   uint32_t ls_src[kEncMaxLong];  // source offset of the first chunk (key arena or input)
+  uint32_t ahead[5][32];         // next block: lane j's entry (key length, shared, value
+                                 // length, key offset, value offset), copied ahead
   __align__(16) uint8_t stage[kEncStage];
 };
 constexpr size_t kEncSmem = (size_t)kEncWarps * sizeof(EncWarp);
@@ -746,83 +754,151 @@ __device__ __forceinline__ void enc_direct(const JobDev& J, const uint32_t* h5,
   if (lane == 0) st_le32(dst + bsz + 1, crc);
 }
 
-// A key delta or value of `len` bytes for stage position pos, from base +
-// off: into the stage whole when shorter than kEncLong, else its unaligned
-// head and tail, with its whole chunks listed in slot li (or staged here when
-// the list is full); li advances past a long stretch.
-__device__ __forceinline__ void enc_stretch(EncWarp& W, uint8_t* st, uint32_t pos, uint32_t len,
-                                            const uint8_t* base, uint32_t off, uint32_t from,
-                                            uint32_t& li) {
-  const uint8_t* src = base + off;
+// A key delta or value of `len` bytes at stage position pos, from base +
+// off.  A stretch shorter than kEncLong is staged whole; a longer one lists
+// its whole 16-byte chunks in slot li while the list has room, and stages only
+// its unaligned head and tail.  enc_list records the slot (li advances past
+// every long stretch); enc_stage writes the staged bytes, and the chunks of a
+// long stretch that found the list full.
+__device__ __forceinline__ void enc_list(EncWarp& W, uint32_t pos, uint32_t len, uint32_t off,
+                                         uint32_t from, uint32_t& li) {
+  if (len < kEncLong) return;
+  if (li < kEncMaxLong) {
+    const uint32_t first = (pos + 15) & ~15u, last = (pos + len) & ~15u;
+    W.ls_c0[li] = (first >> 4) | from;
+    W.ls_n[li] = (last - first) >> 4;
+    W.ls_src[li] = off + (first - pos);
+  }
+  li++;
+}
+
+__device__ __forceinline__ void enc_stage(uint8_t* st, uint32_t pos, uint32_t len,
+                                          const uint8_t* src, bool listed) {
   if (len < kEncLong) {
-    copy_small(st + pos, src, len);
+    // the 16-byte form when every lane here has at most 16 bytes (a lane
+    // that takes the 32-byte form is right for any length below kEncLong)
+    if (__all_sync(__activemask(), len <= 16))
+      copy_small<16>(st + pos, src, len);
+    else
+      copy_small<32>(st + pos, src, len);
     return;
   }
   const uint32_t first = (pos + 15) & ~15u, last = (pos + len) & ~15u;
-  copy_small(st + pos, src, first - pos);
-  copy_small(st + last, src + (last - pos), pos + len - last);
-  const uint32_t nq = (last - first) >> 4;
-  if (li < kEncMaxLong) {
-    W.ls_c0[li] = (first >> 4) | from;
-    W.ls_n[li] = nq;
-    W.ls_src[li] = off + (first - pos);
-  } else {
+  copy_small<16>(st + pos, src, first - pos);
+  copy_small<16>(st + last, src + (last - pos), pos + len - last);
+  if (!listed) {
+    const uint32_t nq = (last - first) >> 4;
     for (uint32_t q = 0; q < nq; q++) {
       uint32_t w[4];
       load16(src + (first - pos) + 16 * q, w);
       *reinterpret_cast<uint4*>(st + first + 16 * q) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
-  li++;
 }
 
-// Chunk c of the stage grid: from its source when it lies in listed stretch
-// *k (k advances along the list), else from the stage.
-__device__ __forceinline__ void enc_fetch(const JobDev& J, const EncWarp& W, const uint8_t* st,
-                                          uint32_t nls, uint32_t c, uint32_t& k,
-                                          uint32_t (&w)[4]) {
+// A chunk slot: the five words holding a chunk's 16 bytes as loaded, and
+// the right shift (bits) that aligns them.  Loads fill the slot; the shift is
+// applied only where the chunk is used, so a slot loaded ahead does not hold
+// up the warp until then.
+struct EncSlot {
+  uint32_t x[5];
+  uint32_t sh;
+};
+
+__device__ __forceinline__ void enc_slot_load(const uint8_t* src, EncSlot& s) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  s.sh = 8 * (uint32_t)(a & 3);
+#pragma unroll
+  for (int i = 0; i < 4; i++) s.x[i] = __ldg(q + i);
+  s.x[4] = s.sh ? __ldg(q + 4) : 0u;
+}
+
+// Chunk c of the stage grid from its source when it lies in listed stretch
+// *k (k advances along the list); false when it is a stage chunk.
+__device__ __forceinline__ bool enc_fetch_listed(const JobDev& J, const EncWarp& W, uint32_t nls,
+                                                 uint32_t c, uint32_t& k, EncSlot& s) {
   while (k < nls && c >= (W.ls_c0[k] & ~kEncFromInput) + W.ls_n[k]) k++;
   const uint32_t c0 = k < nls ? W.ls_c0[k] : 0xffffffffu;
   if (c0 != 0xffffffffu && c >= (c0 & ~kEncFromInput)) {
     const uint8_t* base = (c0 & kEncFromInput) ? J.in : J.keys;
-    load16(base + W.ls_src[k] + 16 * (c - (c0 & ~kEncFromInput)), w);
-  } else {
-    const uint4 v = *reinterpret_cast<const uint4*>(st + 16 * c);
-    w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
+    enc_slot_load(base + W.ls_src[k] + 16 * (c - (c0 & ~kEncFromInput)), s);
+    return true;
   }
+  return false;
+}
+
+__device__ __forceinline__ void enc_fetch_stage(const uint8_t* st, uint32_t c, EncSlot& s) {
+  const uint4 v = *reinterpret_cast<const uint4*>(st + 16 * c);
+  s.x[0] = v.x, s.x[1] = v.y, s.x[2] = v.z, s.x[3] = v.w, s.x[4] = 0u;
+  s.sh = 0u;
+}
+
+__device__ __forceinline__ void enc_fetch(const JobDev& J, const EncWarp& W, const uint8_t* st,
+                                          uint32_t nls, uint32_t c, uint32_t& k, EncSlot& s) {
+  if (!enc_fetch_listed(J, W, nls, c, k, s)) enc_fetch_stage(st, c, s);
 }
 
 // Chunk at stage position p out to global memory when it lies wholly inside
 // the message [m0, m1) (block and type byte), and into the lane's CRC share.
+// The grid bytes outside the message are zero in every chunk (the stage's
+// edges are cleared), so every chunk takes the same step; the CRC's initial
+// register is added at the end.
 __device__ __forceinline__ void enc_chunk_out(const uint32_t* h5, uint8_t* gbase, uint32_t p,
-                                              uint32_t m0, uint32_t m1, const uint32_t (&w)[4],
+                                              uint32_t m0, uint32_t m1, const EncSlot& s,
                                               uint32_t& u, uint32_t& last) {
+  uint32_t w[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) w[i] = __funnelshift_r(s.x[i], s.x[i + 1], s.sh);
   if (p >= m0 && p + 16 <= m1)
     *reinterpret_cast<uint4*>(gbase + p) = make_uint4(w[0], w[1], w[2], w[3]);
-  u = crc_chunk_step(h5, u, p, m0, m1, w[0], w[1], w[2], w[3]);
+  u = crc_h5(h5, w[0] ^ u, w[1], w[2], w[3]);
   last = p;
 }
 
-// A block's place and entry range, and lane j's entry of its first 32: loaded
-// one block ahead (two rounds of dependent loads) so that the next block's
-// first steps do not wait on them.
+// A block's place and entry range, loaded one block ahead; lane j's entry of
+// its first 32 is copied to the warp's `ahead` area (cp.async, no registers
+// held) while the current block is encoded, so that the next block's first
+// steps do not wait on two rounds of dependent loads.
 struct EncAhead {
   uint8_t* dst;
   uint32_t bsz, n;
   uint64_t s;
-  uint32_t kl, sh, vl, koff, voff;  // lane's entry (j = lane < n)
 };
 
-__device__ __forceinline__ void enc_ahead_entries(const JobDev& J, EncAhead& A, uint32_t lane) {
+__device__ __forceinline__ void enc_ahead_entries(const JobDev& J, EncWarp& W, const EncAhead& A,
+                                                  uint32_t lane) {
+  cp_async_wait_all();  // no copy into the area is still in flight
   if (lane < A.n) {
     const uint64_t k = A.s + lane;
-    A.kl = J.k_klen[k];
-    A.sh = J.k_shared[k];
-    A.vl = J.k_vlen[k];
-    A.koff = J.k_koff[k];
-    A.voff = J.k_voff[k];
+    cp_async4(&W.ahead[0][lane], J.k_klen + k);
+    cp_async4(&W.ahead[1][lane], J.k_shared + k);
+    cp_async4(&W.ahead[2][lane], J.k_vlen + k);
+    cp_async4(&W.ahead[3][lane], J.k_koff + k);
+    cp_async4(&W.ahead[4][lane], J.k_voff + k);
   }
 }
+
+// x / R for the restart interval R: a shift when R is a power of two (the
+// common 16), else a division.
+struct RestartDiv {
+  uint32_t R, sh;
+  bool pow2;
+  __device__ __forceinline__ explicit RestartDiv(uint32_t r) {
+    R = r;
+    pow2 = (r & (r - 1u)) == 0u;
+    sh = (uint32_t)__popc(r - 1u);  // log2 r when r is a power of two
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t x) const {
+    uint32_t q;
+    if (pow2)
+      q = x >> sh;
+    else
+      q = x / R;
+    return q;
+  }
+  __device__ __forceinline__ bool starts_run(uint32_t x) const { return x - div(x) * R == 0u; }
+};
 
 __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.y];
@@ -839,6 +915,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
   if (J.ctr->error) return;
   const uint64_t nb = J.ctr->n_blocks_out;
   const uint32_t R = J.restart_interval;
+  const RestartDiv rd(R);
   const uint64_t stride = (uint64_t)gridDim.x * kEncWarps;
   uint8_t* st = W.stage;
   uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp;
@@ -848,7 +925,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     cur.bsz = J.b_size[b];
     cur.s = J.b_first[b];
     cur.n = (uint32_t)(J.b_first[b + 1] - cur.s);
-    enc_ahead_entries(J, cur, lane);
+    enc_ahead_entries(J, W, cur, lane);
   }
   for (; b < nb; b += stride) {
     // the next block's place and range (its entries follow after step 2)
@@ -870,26 +947,40 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     if (ph + bsz + kTrailer + 16 > kEncStage) {
       enc_direct(J, s_h5, s_xinv, s_tab8, b, dst, lane);
     } else {
-      const uint32_t nrest = (n + R - 1) / R;
+      const uint32_t nrest = rd.div(n + R - 1);
       const uint32_t rbase = ph + bsz - 4 * nrest - 4;  // stage position of the restart array
-      // 1. entries: headers, restart words, short stretches, cut edges, list
-      uint32_t carry = 0, lcarry = 0;
+      const uint32_t m0 = ph, m1 = ph + bsz + 1;        // the message: block and type byte
+      // the initial register's share of the CRC, and zeros in the stage's
+      // first and last chunks (grid bytes outside the message)
+      const uint32_t ones = __ldg(J.crc_ones + (m1 - m0));
+      if (lane == 0) *reinterpret_cast<uint4*>(st) = make_uint4(0u, 0u, 0u, 0u);
+      if (lane == 1) *reinterpret_cast<uint4*>(st + ((m1 - 1) & ~15u)) = make_uint4(0u, 0u, 0u, 0u);
+      __syncwarp();
+      // 1. entries: the long stretches listed first; once the list is
+      // complete (last round) the first two chunk rows' listed chunks are
+      // loaded while the lanes write headers, restart words, short stretches
+      // and cut edges to the stage
+      uint32_t carry = 0, lcarry = 0, nls = 0, k = 0;
+      EncSlot sa{}, sb{};
+      bool ga = false, gb = false;  // sa / sb came from a listed stretch
       for (uint32_t j0 = 0; j0 < n; j0 += 32) {
         const uint32_t j = j0 + lane;
         uint32_t size = 0, hl = 0, kd = 0, vl = 0, sh = 0, koff = 0, voff = 0;
         if (j < n) {
           uint32_t kl;
           if (j0 == 0) {
-            kl = cur.kl, sh = cur.sh, vl = cur.vl, koff = cur.koff, voff = cur.voff;
+            cp_async_wait_all();  // this lane's own copies
+            kl = W.ahead[0][lane], sh = W.ahead[1][lane], vl = W.ahead[2][lane];
+            koff = W.ahead[3][lane], voff = W.ahead[4][lane];
           } else {
-            const uint64_t k = s + j;
-            kl = J.k_klen[k], sh = J.k_shared[k], vl = J.k_vlen[k];
-            koff = J.k_koff[k], voff = J.k_voff[k];
+            const uint64_t e = s + j;
+            kl = J.k_klen[e], sh = J.k_shared[e], vl = J.k_vlen[e];
+            koff = J.k_koff[e], voff = J.k_voff[e];
           }
-          if (j % R == 0) sh = 0;
+          if (rd.starts_run(j)) sh = 0;
           kd = kl - sh;
           koff += sh;
-          hl = varint_len(sh) + varint_len(kd) + varint_len(vl);
+          hl = varint_len32(sh) + varint_len32(kd) + varint_len32(vl);
           size = hl + kd + vl;
         }
         uint32_t tot, ltot;
@@ -898,20 +989,31 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
         uint32_t li = warp_excl<uint32_t>(nl, &ltot) + lcarry;
         carry += tot;
         lcarry += ltot;
+        const uint32_t kpos = ph + ex + hl;
+        const uint32_t lik = li;
+        if (j < n) enc_list(W, kpos, kd, koff, 0u, li);
+        const uint32_t liv = li;
+        if (j < n) enc_list(W, kpos + kd, vl, voff, kEncFromInput, li);
+        if (j0 + 32 >= n) {
+          __syncwarp();
+          nls = min(lcarry, kEncMaxLong);
+          if (16 * lane < m1) ga = enc_fetch_listed(J, W, nls, lane, k, sa);
+          if (16 * (lane + 32) < m1) gb = enc_fetch_listed(J, W, nls, lane + 32, k, sb);
+        }
         if (j < n) {
           uint8_t* p = st + ph + ex;
-          p = put_varint(p, sh);
-          p = put_varint(p, kd);
-          put_varint(p, vl);
-          if (j % R == 0) {
+          p = put_varint32(p, sh);
+          p = put_varint32(p, kd);
+          put_varint32(p, vl);
+          const uint32_t run = rd.div(j);
+          if (j == run * R) {
             const uint32_t rem = n - j;
-            st_le32(st + rbase + 4 * (j / R), (ex << 8) | (rem < R ? rem : R));
+            st_le32(st + rbase + 4 * run, (ex << 8) | (rem < R ? rem : R));
           }
           if (J.dec_vpos)  // the value's place in its file, for the decoded form
             J.dec_vpos[s + j] = (uint32_t)(J.b_off[b] + ex + hl + kd);
-          const uint32_t kpos = ph + ex + hl;
-          enc_stretch(W, st, kpos, kd, J.keys, koff, 0u, li);
-          enc_stretch(W, st, kpos + kd, vl, J.in, voff, kEncFromInput, li);
+          enc_stage(st, kpos, kd, J.keys + koff, lik < kEncMaxLong);
+          enc_stage(st, kpos + kd, vl, J.in + voff, liv < kEncMaxLong);
         }
       }
       if (lane == 0) {
@@ -921,17 +1023,15 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
       __syncwarp();
       // 2. chunks: out to global memory and into the CRC; each chunk's loads
       // are issued two chunks ahead of its use (three rotating slots)
-      const uint32_t nls = min(lcarry, kEncMaxLong);
-      const uint32_t m0 = ph, m1 = ph + bsz + 1;
       uint8_t* gbase = dst - ph;
-      uint32_t u = 0, last = 0xffffffffu, k = 0;
-      uint32_t sa[4], sb[4], sc[4];
+      uint32_t u = 0, last = 0xffffffffu;
+      EncSlot sc;
       bool vb = 16 * (lane + 32) < m1;
-      if (16 * lane < m1) enc_fetch(J, W, st, nls, lane, k, sa);
-      if (vb) enc_fetch(J, W, st, nls, lane + 32, k, sb);
+      if (16 * lane < m1 && !ga) enc_fetch_stage(st, lane, sa);
+      if (vb && !gb) enc_fetch_stage(st, lane + 32, sb);
       if (bn < nb) {  // the next block's place and entries, in flight meanwhile
         nxt.dst = J.out + J.files[n_file].out_off + n_off;
-        enc_ahead_entries(J, nxt, lane);
+        enc_ahead_entries(J, W, nxt, lane);
       }
       for (uint32_t c = lane; 16 * c < m1; c += 96) {
         const bool vc = 16 * (c + 64) < m1;
@@ -944,8 +1044,21 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
         if (vc) enc_chunk_out(s_h5, gbase, 16 * (c + 64), m0, m1, sc, u, last);
         vb = ve;
       }
-      // 3. CRC, trailer, partial chunks at both ends
-      const uint32_t crc = crc_rows_finish(s_xinv, s_tab8, u, last, m1);
+      // the lines the next block's entry pass copies bytes from (its keys,
+      // its values' first and last bytes) into L2 while this block finishes
+      if (bn < nb && lane < nxt.n) {
+        cp_async_wait_all();
+        const uint32_t pkl = W.ahead[0][lane], pvl = W.ahead[2][lane];
+        const uint32_t pko = W.ahead[3][lane], pvo = W.ahead[4][lane];
+        prefetch_l2(J.keys + pko);
+        prefetch_l2(J.keys + pko + pkl - 1);
+        prefetch_l2(J.in + pvo);
+        if (pvl) prefetch_l2(J.in + pvo + pvl - 1);
+      }
+      // 3. CRC (with the initial register's share), trailer, partial chunks
+      // at both ends
+      const uint32_t full = crc_rows_raw(s_xinv, s_tab8, u, last, m1) ^ ones ^ 0xffffffffu;
+      const uint32_t crc = ((full >> 15) | (full << 17)) + 0xa282ead8u;  // crc32c::Mask
       if (lane == 0) st_le32(st + m1, crc);
       __syncwarp();
       const uint32_t cf0 = (m0 + 15) >> 4, cf1 = m1 >> 4;  // whole chunks [cf0, cf1) went out
@@ -960,7 +1073,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     }
     if (bn < nb && nxt.dst == nullptr) {  // the direct path
       nxt.dst = J.out + J.files[n_file].out_off + n_off;
-      enc_ahead_entries(J, nxt, lane);
+      enc_ahead_entries(J, W, nxt, lane);
     }
     cur = nxt;
   }
@@ -1281,14 +1394,26 @@ __global__ void __launch_bounds__(256) k_meta_crc(const JobDev* __restrict__ job
       const uint32_t m0 = (uint32_t)(reinterpret_cast<uintptr_t>(pa) & 15);
       const uint32_t m1 = m0 + (uint32_t)(e - a);
       const uint8_t* g = pa - m0;
+      // the lane's chunks of the piece, all loaded before the CRC steps
+      constexpr uint32_t kRows = (kMetaPiece + 15) / kCrcRowBytes + 1;
+      uint4 v[kRows];
+#pragma unroll
+      for (uint32_t i = 0; i < kRows; i++) {
+        const uint32_t x = 16 * lane + kCrcRowBytes * i;
+        if (x < m1) v[i] = *reinterpret_cast<const uint4*>(g + x);
+      }
       uint32_t u = 0, last = 0xffffffffu;
-      for (uint32_t x = 16 * lane; x < m1; x += kCrcRowBytes) {
-        const uint4 v = *reinterpret_cast<const uint4*>(g + x);
-        u = crc_chunk_step(s_h5, u, x, m0, m1, v.x, v.y, v.z, v.w, a == 0);
-        last = x;
+#pragma unroll
+      for (uint32_t i = 0; i < kRows; i++) {
+        const uint32_t x = 16 * lane + kCrcRowBytes * i;
+        if (x < m1) {
+          u = crc_chunk_step(s_h5, u, x, m0, m1, v[i].x, v[i].y, v[i].z, v[i].w, a == 0);
+          last = x;
+        }
       }
       const uint32_t raw = crc_rows_raw(s_xinv, s_tab8, u, last, m1);
-      if (lane == 0) atomicXor(&J.files[f].crc_acc[r], crc_shift(J, raw, len[r] + 1 - e));
+      if (lane == 0)
+        atomicXor(&J.files[f].crc_acc[r], crc_shift_tab(J, s_tab8, raw, len[r] + 1 - e));
     }
   }
 }

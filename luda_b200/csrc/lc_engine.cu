@@ -526,6 +526,8 @@ void fill_common(JobDev& J, const lc_job* j, lc_engine* e) {
   J.crc_h5 = e->crc_xpow + kCrcXpowN;
   J.crc_xinv = J.crc_h5 + kCrcH5Words;
   J.crc_byte = J.crc_xinv + kCrcXinvN;
+  J.crc_ones = J.crc_byte + 256;
+  J.crc_xpow_hi = J.crc_ones + kCrcXpowN;
   J.chunk = kChunk;
   J.chain_smem_words = 11 * 1024;  // 44 KiB (static shared memory takes the rest of 48)
 }
@@ -1770,13 +1772,17 @@ void fill_out(lc_job* j, lc_job_out* o) {
 }
 
 // The engine's CRC tables, one device array: [x^(8n) | row fields | x^(-8n) |
-// byte table].
+// byte table | all-ones shifts | long shifts].
 //  * x^(8n) mod P for n < kCrcXpowN (register shifts by n zero bytes);
 //  * for the row CRC: entry kCrcFieldEntries i + v is the register after 16
 //    bytes holding v at bits [W i, W i + W) (W = kCrcFieldBits) and zero
 //    elsewhere, then kCrcRowBytes - 16 zero bytes, from register 0;
 //  * x^(-8n) mod P for n < kCrcXinvN: the shift that undoes n zero bytes;
-//  * the byte table: the register after byte i, from 0.
+//  * the byte table: the register after byte i, from 0;
+//  * for n < kCrcXpowN, the register after n zero bytes from all ones (the
+//    CRC's initial register carried to the end of an n-byte message);
+//  * x^(8 kCrcXpowN h) mod P for h < kCrcXpowN: with the first table, any
+//    shift below kCrcXpowN^2 bytes is one product of two entries.
 // Registers are reflected (bit 31 is x^0), as in util/crc32c.cc.
 uint32_t host_crc_byte(uint32_t c, uint8_t b) {
   c ^= b;
@@ -1785,7 +1791,7 @@ uint32_t host_crc_byte(uint32_t c, uint8_t b) {
 }
 
 void host_crc_tables(std::vector<uint32_t>& t) {
-  t.assign(kCrcXpowN + kCrcH5Words + kCrcXinvN + 256, 0);
+  t.assign(kCrcXpowN + kCrcH5Words + kCrcXinvN + 256 + 2 * kCrcXpowN, 0);
   uint32_t c = 0x80000000u;  // x^0
   for (uint32_t m = 0; m < kCrcXpowN; m++) {
     t[m] = c;
@@ -1818,6 +1824,19 @@ void host_crc_tables(std::vector<uint32_t>& t) {
   }
   uint32_t* byte = xinv + kCrcXinvN;
   for (uint32_t i = 0; i < 256; i++) byte[i] = host_crc_byte(0, (uint8_t)i);
+  uint32_t* ones = byte + 256;
+  c = 0xffffffffu;
+  for (uint32_t n = 0; n < kCrcXpowN; n++) {
+    ones[n] = c;
+    c = host_crc_byte(c, 0);
+  }
+  uint32_t* hi = ones + kCrcXpowN;
+  const uint32_t step = gf2_mulmod(t[kCrcXpowN - 1], t[1]);  // x^(8 kCrcXpowN)
+  c = 0x80000000u;
+  for (uint32_t h = 0; h < kCrcXpowN; h++) {
+    hi[h] = c;
+    c = gf2_mulmod(c, step);
+  }
 }
 
 }  // namespace

@@ -258,6 +258,8 @@ struct JobDev {
   const uint32_t* crc_h5;     // kCrcH5Words: the field tables of the row CRC
   const uint32_t* crc_xinv;   // kCrcXinvN: x^(-8n) mod P, back shifts by n bytes
   const uint32_t* crc_byte;   // 256: the byte table (register after byte i, from 0)
+  const uint32_t* crc_ones;   // crc_xpow_n: the register after n zero bytes from all ones
+  const uint32_t* crc_xpow_hi; // crc_xpow_n: x^(8 crc_xpow_n h) mod P (long shifts)
 };
 
 }  // namespace lc
