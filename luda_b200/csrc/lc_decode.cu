@@ -549,7 +549,10 @@ __device__ __forceinline__ uint4 dec_record(uint32_t src, uint32_t sh, uint32_t 
 }
 
 __global__ void __launch_bounds__(256) k_decode_walk(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
+  __shared__ JobDev s_job;
+  copy_job(jobs + blockIdx.y, &s_job);
+  __syncthreads();
+  const JobDev& J = s_job;
   __shared__ uint32_t s_rb[8][kDecGroupMax + 1];  // per warp: first run of each block of its group
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (J.ctr->error) return;
@@ -702,7 +705,10 @@ __device__ __forceinline__ uint64_t dec_unit_start(const JobDev& J, uint64_t e, 
 }
 
 __global__ void __launch_bounds__(256) k_decode_keys(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
+  __shared__ JobDev s_job;
+  copy_job(jobs + blockIdx.y, &s_job);
+  __syncthreads();
+  const JobDev& J = s_job;
   __shared__ __align__(16) DecKeysSmem s_w[8];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DecKeysSmem& W = s_w[warp];

@@ -372,6 +372,17 @@ __device__ __forceinline__ void copy_small_w(uint8_t* dst, const uint8_t* src, u
   }
 }
 
+// The job descriptor into shared memory (all threads of the CTA; a
+// __syncthreads() must follow): kernels that stream large arrays through L1
+// read their descriptor's fields from there instead of reloading evicted
+// lines from L2.
+__device__ __forceinline__ void copy_job(const JobDev* __restrict__ src, JobDev* dst) {
+  static_assert(sizeof(JobDev) % 8 == 0, "JobDev is copied in 8-byte words");
+  const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
+  uint64_t* d = reinterpret_cast<uint64_t*>(dst);
+  for (uint32_t i = threadIdx.x; i < sizeof(JobDev) / 8; i += blockDim.x) d[i] = s[i];
+}
+
 // Error reporting: the first error code wins.
 __device__ __forceinline__ void set_error(Counters* c, uint32_t code, uint32_t detail) {
   if (atomicCAS(&c->error, 0u, code) == 0u) c->error_detail = detail;

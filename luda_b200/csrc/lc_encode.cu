@@ -901,15 +901,18 @@ struct RestartDiv {
 };
 
 __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
-  const JobDev& J = jobs[blockIdx.y];
   __shared__ uint32_t s_h5[kCrcH5Words];
   __shared__ uint32_t s_xinv[kCrcXinvN];
   __shared__ uint32_t s_tab8[256];
+  __shared__ JobDev s_job;  // the job's descriptor, read from here in every step
   extern __shared__ __align__(16) uint8_t enc_smem[];
-  for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = J.crc_h5[i];
-  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = J.crc_xinv[i];
-  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = J.crc_byte[i];
+  copy_job(jobs + blockIdx.y, &s_job);
+  const JobDev& G = jobs[blockIdx.y];
+  for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = G.crc_h5[i];
+  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = G.crc_xinv[i];
+  for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = G.crc_byte[i];
   __syncthreads();
+  const JobDev& J = s_job;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem)[warp];
   if (J.ctr->error) return;
