@@ -863,14 +863,14 @@ __device__ __forceinline__ void enc_chunk_out(const uint32_t* h5, uint8_t* gbase
 struct EncAhead {
   uint8_t* dst;
   uint32_t bsz, n;
-  uint64_t s;
+  uint32_t s;
 };
 
 __device__ __forceinline__ void enc_ahead_entries(const JobDev& J, EncWarp& W, const EncAhead& A,
                                                   uint32_t lane) {
   cp_async_wait_all();  // no copy into the area is still in flight
   if (lane < A.n) {
-    const uint64_t k = A.s + lane;
+    const uint32_t k = A.s + lane;
     cp_async4(&W.ahead[0][lane], J.k_klen + k);
     cp_async4(&W.ahead[1][lane], J.k_shared + k);
     cp_async4(&W.ahead[2][lane], J.k_vlen + k);
@@ -916,12 +916,12 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   EncWarp& W = reinterpret_cast<EncWarp*>(enc_smem)[warp];
   if (J.ctr->error) return;
-  const uint64_t nb = J.ctr->n_blocks_out;
+  const uint32_t nb = (uint32_t)J.ctr->n_blocks_out;  // block and survivor indices fit 32 bits
   const uint32_t R = J.restart_interval;
   const RestartDiv rd(R);
-  const uint64_t stride = (uint64_t)gridDim.x * kEncWarps;
+  const uint32_t stride = gridDim.x * kEncWarps;
   uint8_t* st = W.stage;
-  uint64_t b = (uint64_t)blockIdx.x * kEncWarps + warp;
+  uint32_t b = blockIdx.x * kEncWarps + warp;
   EncAhead cur{};
   if (b < nb) {
     cur.dst = J.out + J.files[J.b_file[b]].out_off + J.b_off[b];
@@ -932,7 +932,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
   }
   for (; b < nb; b += stride) {
     // the next block's place and range (its entries follow after step 2)
-    const uint64_t bn = b + stride;
+    const uint32_t bn = b + stride;
     EncAhead nxt{};
     uint32_t n_file = 0;
     uint64_t n_off = 0;
@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     }
     uint8_t* dst = cur.dst;
     const uint32_t bsz = cur.bsz, n = cur.n;
-    const uint64_t s = cur.s;
+    const uint32_t s = cur.s;
     const uint32_t ph = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
     if (ph + bsz + kTrailer + 16 > kEncStage) {
       enc_direct(J, s_h5, s_xinv, s_tab8, b, dst, lane);
@@ -976,7 +976,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
             kl = W.ahead[0][lane], sh = W.ahead[1][lane], vl = W.ahead[2][lane];
             koff = W.ahead[3][lane], voff = W.ahead[4][lane];
           } else {
-            const uint64_t e = s + j;
+            const uint32_t e = s + j;
             kl = J.k_klen[e], sh = J.k_shared[e], vl = J.k_vlen[e];
             koff = J.k_koff[e], voff = J.k_voff[e];
           }
