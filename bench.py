@@ -369,10 +369,17 @@ def job_leg(name, args, eng, eng_ph, flush, torch, steps, warmup, clocks=None, p
         check_outputs(case, host_res.file_bytes(), f"{name} (host buffers)")
     host_res.release()
 
+    # warm-up keeps outputs alive the way the timed loop does (a step's output
+    # is released after the next step has run), so that the engine's device
+    # memory for two outputs is taken before timing
+    last = None
     for _ in range(warmup):
-        eng.run(prep_dev).release()
+        w = eng.run_raw(prep_dev)
+        if last is not None:
+            eng.release_raw(last[0])
+        last = w
     torch.cuda.synchronize()
-    ms_steps, launches, last = [], 0, None
+    ms_steps, launches = [], 0
     if clocks:
         clocks.mark_start()
     for step in range(steps):

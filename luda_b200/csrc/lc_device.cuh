@@ -468,6 +468,11 @@ constexpr uint32_t kCrcFieldEntries = 1u << kCrcFieldBits;
 constexpr uint32_t kCrcH5Words = kCrcFields * kCrcFieldEntries;  // the row tables
 constexpr uint32_t kCrcRowBytes = 512;   // 32 lanes x 16 bytes
 constexpr uint32_t kCrcXinvN = 512;      // back shifts of 0..511 bytes
+// The back shifts' shared-memory copy skips a word after every 16 entries:
+// a warp's lanes index it 16 apart (one lane per 16-byte chunk column), which
+// in a dense copy falls on two banks.
+constexpr uint32_t kCrcXinvSmem = kCrcXinvN + kCrcXinvN / 16;
+__host__ __device__ __forceinline__ uint32_t xinv_slot(uint32_t n) { return n + (n >> 4); }
 
 // H(w0..w3) from the row tables (table i at h5[kCrcFieldEntries i], indexed
 // by bits [W i, W i + W) of the little-endian 128-bit chunk); the field's
@@ -525,12 +530,13 @@ __device__ __forceinline__ uint32_t crc_chunk_step(const uint32_t* __restrict__ 
 
 // The raw register at the message's end from the lanes' registers (lane l's
 // last chunk at grid position `last`, 0xffffffff when it had none), the same
-// in every lane.
+// in every lane.  xinv is the back shifts' padded shared-memory copy
+// (xinv_slot).
 __device__ __forceinline__ uint32_t crc_rows_raw(const uint32_t* __restrict__ xinv,
                                                  const uint32_t* __restrict__ tab8, uint32_t u,
                                                  uint32_t last, uint32_t m1) {
   uint32_t v = 0;
-  if (last != 0xffffffffu) v = gf2_mulmod_tab(tab8, u, xinv[last + kCrcRowBytes - m1]);
+  if (last != 0xffffffffu) v = gf2_mulmod_tab(tab8, u, xinv[xinv_slot(last + kCrcRowBytes - m1)]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
   return v;

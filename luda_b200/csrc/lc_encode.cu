@@ -902,14 +902,14 @@ struct RestartDiv {
 
 __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDev* __restrict__ jobs) {
   __shared__ uint32_t s_h5[kCrcH5Words];
-  __shared__ uint32_t s_xinv[kCrcXinvN];
+  __shared__ uint32_t s_xinv[kCrcXinvSmem];
   __shared__ uint32_t s_tab8[256];
   __shared__ JobDev s_job;  // the job's descriptor, read from here in every step
   extern __shared__ __align__(16) uint8_t enc_smem[];
   copy_job(jobs + blockIdx.y, &s_job);
   const JobDev& G = jobs[blockIdx.y];
   for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = G.crc_h5[i];
-  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = G.crc_xinv[i];
+  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[xinv_slot(i)] = G.crc_xinv[i];
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = G.crc_byte[i];
   __syncthreads();
   const JobDev& J = s_job;
@@ -1367,12 +1367,12 @@ __device__ __forceinline__ void meta_region(const FileOut& F, uint32_t r, uint64
 __global__ void __launch_bounds__(256) k_meta_crc(const JobDev* __restrict__ jobs) {
   const JobDev& J = jobs[blockIdx.z];
   __shared__ uint32_t s_h5[kCrcH5Words];
-  __shared__ uint32_t s_xinv[kCrcXinvN];
+  __shared__ uint32_t s_xinv[kCrcXinvSmem];
   __shared__ uint32_t s_tab8[256];
   __shared__ uint32_t s_skip;
   if (threadIdx.x == 0) s_skip = J.ctr->error || blockIdx.y >= J.ctr->n_files;
   for (uint32_t i = threadIdx.x; i < kCrcH5Words; i += blockDim.x) s_h5[i] = J.crc_h5[i];
-  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[i] = J.crc_xinv[i];
+  for (uint32_t i = threadIdx.x; i < kCrcXinvN; i += blockDim.x) s_xinv[xinv_slot(i)] = J.crc_xinv[i];
   for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) s_tab8[i] = J.crc_byte[i];
   __syncthreads();
   if (s_skip) return;
