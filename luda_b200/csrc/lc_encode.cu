@@ -1080,6 +1080,7 @@ __global__ void __launch_bounds__(kEncWarps * 32, 3) k_encode_blocks(const JobDe
     }
     cur = nxt;
   }
+  cp_async_wait_all();  // a direct-path last block never waited for its entries' copies
 }
 
 // The survivors' decoded form for later jobs (keep_decoded): key bytes at
