@@ -127,3 +127,33 @@ def test_row_crc_needs_the_initial_register(oracle_lib, tables):
     want = oracle.crc32c_mask(oracle.crc32c(block + b"\x00"))
     assert _rows_crc(tables, block, 5) == want
     assert _rows_crc((h5, xinv, [0] * len(tables[2])), block, 5) != want
+
+
+def _xpow8(n):
+    # x^(8n) mod P by square and multiply (reflected; x^8 is one zero byte from x^0)
+    r, base = 0x80000000, _byte_step(0x80000000, 0)
+    while n:
+        if n & 1:
+            r = _mulmod(r, base)
+        base = _mulmod(base, base)
+        n >>= 1
+    return r
+
+
+def test_long_shift_is_a_product_of_two_table_entries():
+    # the meta-block CRC moves each 4 KiB piece's register to its block's end
+    # by x^(8n), n = 8192 hi + lo, as xpow[lo] * xpow_hi[hi]; the engine builds
+    # xpow_hi[h] as xpow_hi[h - 1] * (xpow[8191] * xpow[1])
+    N = 8192
+    xpow = [0x80000000]
+    for _ in range(N - 1):
+        xpow.append(_byte_step(xpow[-1], 0))
+    step = _mulmod(xpow[N - 1], xpow[1])
+    assert step == _xpow8(N)
+    hi_tab = [0x80000000]
+    for _ in range(64):
+        hi_tab.append(_mulmod(hi_tab[-1], step))
+    rng = np.random.default_rng(5)
+    for n in [0, 1, N - 1, N, N + 1, 40 * N + 17] + rng.integers(0, 64 * N, 20).tolist():
+        hi, lo = divmod(int(n), N)
+        assert _mulmod(xpow[lo], hi_tab[hi]) == _xpow8(int(n)), n
