@@ -173,3 +173,26 @@ def test_oracle_tables_readable_by_reference():
         ents = oracle.read_table(d, "ref")
         assert ents[0][0] == s and ents[-1][0] == l
         assert ents == oracle.read_table(d, "oracle")
+
+
+@pytest.mark.skipif(not oracle.has_ref(), reason="reference build absent")
+def test_oracle_matches_reference_on_encoder_path_cases():
+    # the cases tests/test_gpu_encode_paths.py runs on the GPU against the
+    # restatement: here the restatement against the reference's own build
+    import test_gpu_encode_paths as paths
+    from luda_b200.job import TableOptions
+    for ri, bs, vlen, what in paths.CASES:
+        opts = TableOptions(block_size=bs, restart_interval=ri, bits_per_key=10,
+                            max_file_size=1 << 20)
+        job = workloads.l0_l1_job(900 + ri + vlen, n0=2, n1=2, entries_per_table=4000,
+                                  key_space=1 << 20, tomb_frac=0.02, value_len=vlen,
+                                  options=opts)
+        job.materialize(lambda e, o: oracle.build_table(e, o, "ref"))
+        inputs = [bytes(f.data) for f in job.files]
+        for f in job.files:
+            assert oracle.build_table(f.entries, opts, "oracle") == bytes(f.data), what
+        a = oracle.compact(job, "oracle")
+        b = oracle.compact(job, "ref")
+        assert [x[0] for x in a] == [x[0] for x in b], what
+        assert [(x[1], x[2]) for x in a] == [(x[1], x[2]) for x in b], what
+        assert inputs == [bytes(f.data) for f in job.files]
